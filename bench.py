@@ -1,0 +1,308 @@
+#!/usr/bin/env python
+"""Reads corrected per second on B200: CARE's per-anchor correction path.
+
+Workload (default): the 5 Mbp / 30x paired-end set -- seeded random genome
+with 2% of its length in 20 copies of a 5 kbp repeat at 1% divergence,
+1,000,000 interleaved 150 bp reads, fragments ~N(400, 40), substitution rate
+rising linearly 0.2% -> 1.5% along the read, Phred qualities from the rate
++ N(0, 3); options -c 30 -k 20 -h 32 -q --qualityScoreBits 2 --pairmode PE.
+
+One step = correcting every read of the set once (the reference's STEP2,
+src/dispatch_care_correct_cpu.cpp:157-168; reads/s = reads / STEP2 time).
+
+  value : device time of the pipeline with reads and tables resident in HBM
+          (CUDA events on the library's stream), L2 flushed between steps.
+  e2e   : the same through the C ABI from host buffers -- upload of the read
+          storage (care_b200_upload_reads) + correction with the results
+          copied back to host memory (care_b200_correct_range), wall clock.
+  --impl reference : the reference's care-cpu (built from its sources by
+          oracle/Makefile) on all host cores, on a bounded sample of the
+          workload (same model, 1.25 Mbp genome, 250,000 reads).
+
+Multi-GPU: one process per GPU; each rank corrects its own 1M-read set
+(independent genome partitions, no data-path collective) -> weak scaling.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import shutil
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+ARGS = "-c 30 -k 20 -h 32 -q --qualityScoreBits 2 --pairmode PE"
+METRIC = "reads corrected/s (STEP2), 5 Mbp / 30x paired-end, plain method"
+CARE_CPU = os.path.join(ROOT, "oracle", "_ref", "care-cpu")
+L2_BYTES = 126 * 1024 * 1024
+
+
+def workload(rank: int, genome_size: int):
+    from care_b200 import datagen
+    rs = datagen.paired_end_repeats(seed=2 + 1000 * rank, genome_size=genome_size)
+    return rs
+
+
+def write_fastq_fast(rs, path):
+    n, L = rs.num_reads, rs.seqs.shape[1]
+    assert (rs.lengths == L).all()
+    heads = [b"@r%d\n" % i for i in range(n)]
+    seqs = rs.seqs.tobytes()
+    quals = rs.quals.tobytes()
+    with open(path, "wb") as f:
+        chunk = 100_000
+        for b in range(0, n, chunk):
+            parts = []
+            for i in range(b, min(n, b + chunk)):
+                parts += [heads[i], seqs[i * L:(i + 1) * L], b"\n+\n", quals[i * L:(i + 1) * L], b"\n"]
+            f.write(b"".join(parts))
+
+
+def encode_quality_2bit(quals: np.ndarray) -> np.ndarray:
+    """qualityscorecompression.hpp:95-119 with 2 bits: bins Q<=4,13,20,>20."""
+    q = quals.astype(np.int32) - 33
+    code = np.where(q <= 4, 0, np.where(q <= 13, 1, np.where(q <= 20, 2, 3))).astype(np.uint32)
+    n, L = code.shape
+    per = 16
+    pitch = (2 * L + 31) // 32
+    padded = np.zeros((n, pitch * per), np.uint32)
+    padded[:, :L] = code
+    padded = padded.reshape(n, pitch, per)
+    shifts = (30 - 2 * np.arange(per, dtype=np.uint32))
+    return (padded << shifts).sum(axis=2, dtype=np.uint64).astype(np.uint32)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.out = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+
+    def __enter__(self):
+        exe = shutil.which("nvidia-smi")
+        if exe:
+            self.proc = subprocess.Popen([exe, "-i", str(self.device), f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.out, stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            self.proc.wait(timeout=10)
+
+    def summary(self):
+        self.out.flush()
+        rows = []
+        with open(self.out.name) as f:
+            for line in f:
+                p = [x.strip() for x in line.split(",")]
+                if len(p) >= 9:
+                    rows.append(p)
+        os.unlink(self.out.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i] == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def care_cpu_sample(tmpdir: str, threads: int):
+    """care-cpu on the bounded sample; returns reads/s from its STEP2 line."""
+    from care_b200 import datagen
+    path = os.path.join(tmpdir, "sample.fq")
+    if not os.path.exists(path):
+        rs = datagen.paired_end_repeats(seed=7, genome_size=1_250_000, repeat_unit=1250)
+        write_fastq_fast(rs, path)
+    r = subprocess.run([CARE_CPU, "-i", path, "-d", tmpdir, "-o", "sample_out.fq", "-t", str(threads)]
+                       + ARGS.split(), capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("care-cpu failed: " + r.stderr[-500:])
+    m = re.search(r"Correction throughput : ~([0-9.e+]+) reads/second", r.stdout)
+    return float(m.group(1))
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    cfg = {"workload": "pe_5Mbp_30x_150bp (sample: 1.25 Mbp genome, 250,000 reads, same model)",
+           "args": ARGS, "reads_per_step": 250_000, "threads": threads}
+    if not os.path.exists(CARE_CPU):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/care-cpu not built (make -C oracle ref)"}))
+        return
+    with tempfile.TemporaryDirectory() as tmp:
+        for _ in range(args.warmup):
+            care_cpu_sample(tmp, threads)
+        vals = [care_cpu_sample(tmp, threads) for _ in range(args.steps)]
+    v = float(np.mean(vals))
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "reads/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 250_000 / v * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+            "data": "synthetic (seeded)", "config": cfg,
+            "cpu_baseline": {"value": v, "unit": "reads/s", "cores": threads, "kind": "reference",
+                             "sample": cfg["workload"]},
+            "e2e": {"value": v, "unit": "reads/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="care_b200", choices=["care_b200", "reference"])
+    ap.add_argument("--genome", type=int, default=5_000_000)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import torch
+    import torch.distributed as dist
+    import care_b200
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    tmp = tempfile.mkdtemp(prefix=f"careb200_bench_{rank}_")
+    rs = workload(rank, args.genome)
+    n = rs.num_reads
+    fq = os.path.join(tmp, "reads.fq")
+    write_fastq_fast(rs, fq)
+
+    opts = care_b200.options_from_args(ARGS, device=local)
+    corr = care_b200.Corrector(opts)
+    t0 = time.perf_counter()
+    corr.load_files([fq])
+    corr.build_tables()
+    step1_s = time.perf_counter() - t0
+
+    flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device=f"cuda:{local}")
+
+    for _ in range(args.warmup):
+        corr.correct_range_device(0, n)
+    barrier()
+    with ClockSampler(local) as clk:
+        dev_ms, stage = [], np.zeros(3)
+        t_wall = 0.0
+        for _ in range(args.steps):
+            flush.fill_(1.0)
+            torch.cuda.synchronize()
+            w0 = time.perf_counter()
+            corr.correct_range_device(0, n)
+            t_wall += time.perf_counter() - w0
+            tot, st = corr.last_timing()
+            dev_ms.append(tot)
+            stage += np.array(st)
+        barrier()
+    stats = corr.last_stats()
+    ms = float(np.mean(dev_ms))
+    if world > 1:
+        t = torch.tensor([ms], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    stage /= args.steps
+    value = world * n / (ms / 1e3)
+
+    # e2e through the C ABI from host buffers
+    from care_b200 import encode_reads
+    packed = np.ascontiguousarray(encode_reads(rs.seqs, rs.lengths))
+    quals = np.ascontiguousarray(encode_quality_2bit(rs.quals))
+    lens = np.ascontiguousarray(rs.lengths.astype(np.int32))
+    h2d = packed.nbytes + quals.nbytes + lens.nbytes
+    for _ in range(max(1, args.warmup)):
+        corr.upload_reads(packed, lens, quals)
+        corr.correct_range_raw(0, n)
+    barrier()
+    e2e_s = []
+    for _ in range(args.steps):
+        w0 = time.perf_counter()
+        corr.upload_reads(packed, lens, quals)
+        raw = corr.correct_range_raw(0, n)
+        e2e_s.append(time.perf_counter() - w0)
+    barrier()
+    d2h = raw.num_anchors * (1 + 4 + raw.max_length) + int(raw.num_candidates) * (13 + raw.max_length)
+    e2e_t = float(np.mean(e2e_s))
+    if world > 1:
+        t = torch.tensor([e2e_t], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_t = float(t.item())
+
+    peaks = {}
+    pk = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(pk):
+        peaks = json.load(open(pk))
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    # MSA stage, HBM roofline: per pair 40 B packed read + 40 B 2-bit
+    # qualities + 4 B id + 13 B alignment tuple; per anchor its own row and
+    # qualities (84 B) and the corrected row (150 B)
+    msa_bytes = stats["pairs"] * 97 + n * (84 + 150)
+    msa_gbs = msa_bytes / (stage[2] / 1e3) / 1e9
+    # alignment stage: un-pruned 32-bit word compares, 1486 per pair at L=150
+    align_words = stats["pairs"] * 1486
+    line = {
+        "metric": METRIC, "value": value, "unit": "reads/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded), " + rs.name,
+        "config": {"workload": "pe_5Mbp_30x_150bp", "reads_per_gpu": n, "args": ARGS,
+                   "genome_bp": args.genome, "l2": "flushed between steps (252 MB write); working set > L2",
+                   "parallelism": f"replicas x{world} (independent read sets)",
+                   "stage_ms": {"candidates": stage[0], "align": stage[1], "msa": stage[2]},
+                   "pairs_per_step": stats["pairs"], "wall_ms_per_step": t_wall / args.steps * 1e3,
+                   "step1_s": step1_s},
+        "roofline": {"kernel": "k_msa", "bound": "hbm", "achieved": msa_gbs, "peak": hbm_peak,
+                     "unit": "GB/s", "frac": msa_gbs / hbm_peak, "traffic": None,
+                     "peak_source": "measured" if peaks else "fallback"},
+        "roofline_alignment": {"kernel": "k_align", "word_compares_per_s": align_words / (stage[1] / 1e3),
+                               "ms": stage[1]},
+        "e2e": {"value": world * n / e2e_t, "unit": "reads/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "gpu_launches": 3 * args.steps,
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and os.path.exists(CARE_CPU):
+        threads = os.cpu_count() or 1
+        v = care_cpu_sample(tmp, threads)
+        line["cpu_baseline"] = {"value": v, "unit": "reads/s", "cores": threads, "kind": "reference",
+                                "sample": "care-cpu -t all cores on 1.25 Mbp genome, 250,000 reads, same model"}
+    corr.close()
+    shutil.rmtree(tmp, ignore_errors=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line))
+
+
+if __name__ == "__main__":
+    main()

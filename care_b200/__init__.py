@@ -1,0 +1,361 @@
+"""care_b200 -- B200 (sm_100a) read-error correction, CARE's per-anchor path.
+
+Python view of the C ABI in include/care_b200.h (the library itself is C++
+and CUDA; this module only loads it with ctypes). The shared library must be
+built first (`python -m care_b200.build`); importing never falls back to any
+other implementation.
+"""
+from __future__ import annotations
+
+import ctypes
+import dataclasses
+import os
+from typing import Sequence
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libcareb200.so")
+CLI_PATH = os.path.join(HERE, "care-b200")
+
+
+class CareError(RuntimeError):
+    pass
+
+
+class Options(ctypes.Structure):
+    """care_b200_options; defaults of include/options.hpp:37-98 (reference)."""
+    _fields_ = [
+        ("kmerlength", ctypes.c_int),
+        ("num_maps", ctypes.c_int),
+        ("min_overlap", ctypes.c_int),
+        ("max_error_rate", ctypes.c_float),
+        ("min_overlap_ratio", ctypes.c_float),
+        ("estimated_errorrate", ctypes.c_float),
+        ("estimated_coverage", ctypes.c_float),
+        ("m_coverage", ctypes.c_float),
+        ("paired_filter_threshold", ctypes.c_float),
+        ("new_columns_to_correct", ctypes.c_int),
+        ("use_quality", ctypes.c_int),
+        ("quality_bits", ctypes.c_int),
+        ("exclude_ambiguous", ctypes.c_int),
+        ("correct_candidates", ctypes.c_int),
+        ("paired_end", ctypes.c_int),
+        ("correction_type", ctypes.c_int),
+        ("quality_labels", ctypes.c_int),
+        ("threads", ctypes.c_int),
+        ("device", ctypes.c_int),
+        ("batch_size", ctypes.c_int),
+    ]
+
+
+class Results(ctypes.Structure):
+    _fields_ = [
+        ("first_anchor", ctypes.c_uint32),
+        ("num_anchors", ctypes.c_uint32),
+        ("max_length", ctypes.c_int32),
+        ("anchor_status", ctypes.POINTER(ctypes.c_uint8)),
+        ("anchor_num_edits", ctypes.POINTER(ctypes.c_int32)),
+        ("anchor_sequences", ctypes.POINTER(ctypes.c_char)),
+        ("num_candidates", ctypes.c_uint64),
+        ("cand_read_ids", ctypes.POINTER(ctypes.c_uint32)),
+        ("cand_anchor_ids", ctypes.POINTER(ctypes.c_uint32)),
+        ("cand_shifts", ctypes.POINTER(ctypes.c_int32)),
+        ("cand_use_edits", ctypes.POINTER(ctypes.c_uint8)),
+        ("cand_sequences", ctypes.POINTER(ctypes.c_char)),
+    ]
+
+
+# every entry point of include/care_b200.h
+EXPORTS = [
+    "care_b200_default_options", "care_b200_create", "care_b200_destroy",
+    "care_b200_last_error", "care_b200_upload_reads", "care_b200_upload_tables",
+    "care_b200_build_tables", "care_b200_get_table", "care_b200_correct_range",
+    "care_b200_correct_range_device", "care_b200_serialize_results",
+    "care_b200_load_reads_from_files", "care_b200_write_output", "care_b200_last_timing",
+    "care_b200_last_stats", "care_b200_num_reads", "care_b200_max_length", "care_b200_num_maps",
+]
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
+    """Loads libcareb200.so; raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise CareError(f"{path} is missing: build it with `python -m care_b200.build`")
+    lib = ctypes.CDLL(path)
+    P = ctypes.POINTER
+    c_ctx = ctypes.c_void_p
+    lib.care_b200_default_options.argtypes = [P(Options)]
+    lib.care_b200_create.argtypes = [P(Options), P(c_ctx)]
+    lib.care_b200_destroy.argtypes = [c_ctx]
+    lib.care_b200_last_error.argtypes = [c_ctx]
+    lib.care_b200_last_error.restype = ctypes.c_char_p
+    lib.care_b200_upload_reads.argtypes = [c_ctx, P(ctypes.c_uint32), ctypes.c_size_t, P(ctypes.c_int32),
+                                           P(ctypes.c_uint32), ctypes.c_size_t, P(ctypes.c_uint32),
+                                           ctypes.c_size_t, ctypes.c_uint32]
+    lib.care_b200_upload_tables.argtypes = [c_ctx, ctypes.c_int, P(P(ctypes.c_uint64)), P(P(ctypes.c_uint32)),
+                                            P(P(ctypes.c_uint32)), P(ctypes.c_size_t)]
+    lib.care_b200_build_tables.argtypes = [c_ctx]
+    lib.care_b200_get_table.argtypes = [c_ctx, ctypes.c_int, P(P(ctypes.c_uint64)), P(P(ctypes.c_uint32)),
+                                        P(P(ctypes.c_uint32)), P(ctypes.c_size_t)]
+    lib.care_b200_correct_range.argtypes = [c_ctx, ctypes.c_uint32, ctypes.c_uint32, P(Results)]
+    lib.care_b200_correct_range_device.argtypes = [c_ctx, ctypes.c_uint32, ctypes.c_uint32]
+    lib.care_b200_serialize_results.argtypes = [c_ctx, P(Results), P(ctypes.c_uint8), ctypes.c_size_t,
+                                                P(ctypes.c_size_t)]
+    lib.care_b200_load_reads_from_files.argtypes = [c_ctx, P(ctypes.c_char_p), ctypes.c_int]
+    lib.care_b200_write_output.argtypes = [c_ctx, ctypes.c_char_p]
+    lib.care_b200_last_timing.argtypes = [c_ctx, P(ctypes.c_float), P(ctypes.c_float), ctypes.c_int]
+    lib.care_b200_last_stats.argtypes = [c_ctx, P(ctypes.c_uint64), ctypes.c_int]
+    lib.care_b200_num_reads.argtypes = [c_ctx]
+    lib.care_b200_num_reads.restype = ctypes.c_uint32
+    lib.care_b200_max_length.argtypes = [c_ctx]
+    lib.care_b200_num_maps.argtypes = [c_ctx]
+    _lib = lib
+    return lib
+
+
+def default_options(**kw) -> Options:
+    lib = load_library()
+    o = Options()
+    lib.care_b200_default_options(ctypes.byref(o))
+    for k, v in kw.items():
+        if not hasattr(o, k):
+            raise TypeError(f"unknown option {k}")
+        setattr(o, k, v)
+    return o
+
+
+def _ptr(a: np.ndarray, ctype):
+    return a.ctypes.data_as(ctypes.POINTER(ctype))
+
+
+@dataclasses.dataclass
+class CorrectionResults:
+    first: int
+    status: np.ndarray            # uint8 per anchor: 1 corrected, 2 hq, 4 edit list
+    num_edits: np.ndarray
+    sequences: np.ndarray         # (num_anchors, max_len) uint8 ASCII
+    cand_read_ids: np.ndarray
+    cand_anchor_ids: np.ndarray
+    cand_shifts: np.ndarray
+    cand_use_edits: np.ndarray
+    cand_sequences: np.ndarray    # (num_candidates, max_len)
+
+
+class Corrector:
+    """One device context: read storage + minhash tables + correction."""
+
+    def __init__(self, options: Options | None = None, **kw):
+        self.lib = load_library()
+        self.opts = options if options is not None else default_options(**kw)
+        self._ctx = ctypes.c_void_p()
+        rc = self.lib.care_b200_create(ctypes.byref(self.opts), ctypes.byref(self._ctx))
+        if rc != 0:
+            msg = self.lib.care_b200_last_error(self._ctx) if self._ctx else b""
+            raise CareError(f"care_b200_create failed ({rc}) {msg!r}")
+        self._keep = []
+
+    def close(self):
+        if self._ctx:
+            self.lib.care_b200_destroy(self._ctx)
+            self._ctx = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc: int, what: str):
+        if rc != 0:
+            raise CareError(f"{what} failed ({rc}): {self.lib.care_b200_last_error(self._ctx).decode()}")
+
+    # -- read storage / tables -------------------------------------------------
+    def upload_reads(self, packed: np.ndarray, lengths: np.ndarray, quals: np.ndarray | None = None,
+                     ambiguous: np.ndarray | None = None):
+        packed = np.ascontiguousarray(packed, dtype=np.uint32)
+        lengths = np.ascontiguousarray(lengths, dtype=np.int32)
+        amb = np.ascontiguousarray(ambiguous if ambiguous is not None else np.zeros(0, np.uint32), dtype=np.uint32)
+        qp = None
+        qpitch = 0
+        if quals is not None:
+            quals = np.ascontiguousarray(quals, dtype=np.uint32)
+            qp = _ptr(quals, ctypes.c_uint32)
+            qpitch = quals.shape[1]
+        self._check(self.lib.care_b200_upload_reads(
+            self._ctx, _ptr(packed, ctypes.c_uint32), packed.shape[1], _ptr(lengths, ctypes.c_int32),
+            qp, qpitch, _ptr(amb, ctypes.c_uint32), amb.shape[0], packed.shape[0]), "upload_reads")
+
+    def load_files(self, files: Sequence[str]):
+        arr = (ctypes.c_char_p * len(files))(*[f.encode() for f in files])
+        self._check(self.lib.care_b200_load_reads_from_files(self._ctx, arr, len(files)), "load_reads_from_files")
+
+    def build_tables(self):
+        self._check(self.lib.care_b200_build_tables(self._ctx), "build_tables")
+
+    def upload_tables(self, tables: Sequence[tuple[np.ndarray, np.ndarray, np.ndarray]]):
+        m = len(tables)
+        ks = [np.ascontiguousarray(t[0], dtype=np.uint64) for t in tables]
+        os_ = [np.ascontiguousarray(t[1], dtype=np.uint32) for t in tables]
+        vs = [np.ascontiguousarray(t[2], dtype=np.uint32) for t in tables]
+        P = ctypes.POINTER
+        kp = (P(ctypes.c_uint64) * m)(*[_ptr(k, ctypes.c_uint64) for k in ks])
+        op = (P(ctypes.c_uint32) * m)(*[_ptr(o, ctypes.c_uint32) for o in os_])
+        vp = (P(ctypes.c_uint32) * m)(*[_ptr(v, ctypes.c_uint32) for v in vs])
+        nk = (ctypes.c_size_t * m)(*[k.shape[0] for k in ks])
+        self._check(self.lib.care_b200_upload_tables(self._ctx, m, kp, op, vp, nk), "upload_tables")
+
+    def get_table(self, m: int):
+        P = ctypes.POINTER
+        k = P(ctypes.c_uint64)()
+        o = P(ctypes.c_uint32)()
+        v = P(ctypes.c_uint32)()
+        n = ctypes.c_size_t()
+        self._check(self.lib.care_b200_get_table(self._ctx, m, ctypes.byref(k), ctypes.byref(o),
+                                                 ctypes.byref(v), ctypes.byref(n)), "get_table")
+        nk = n.value
+        keys = np.ctypeslib.as_array(k, shape=(nk,)).copy() if nk else np.zeros(0, np.uint64)
+        offs = np.ctypeslib.as_array(o, shape=(nk + 1,)).copy()
+        nv = int(offs[-1]) if nk else 0
+        vals = np.ctypeslib.as_array(v, shape=(nv,)).copy() if nv else np.zeros(0, np.uint32)
+        return keys, offs, vals
+
+    @property
+    def num_reads(self) -> int:
+        return int(self.lib.care_b200_num_reads(self._ctx))
+
+    @property
+    def max_length(self) -> int:
+        return int(self.lib.care_b200_max_length(self._ctx))
+
+    @property
+    def num_maps(self) -> int:
+        return int(self.lib.care_b200_num_maps(self._ctx))
+
+    # -- correction ------------------------------------------------------------
+    def correct_range_raw(self, first: int, count: int) -> Results:
+        res = Results()
+        self._check(self.lib.care_b200_correct_range(self._ctx, first, count, ctypes.byref(res)), "correct_range")
+        return res
+
+    def correct_range(self, first: int = 0, count: int | None = None) -> CorrectionResults:
+        if count is None:
+            count = self.num_reads - first
+        res = self.correct_range_raw(first, count)
+        L = res.max_length
+        na = res.num_anchors
+        nc = int(res.num_candidates)
+
+        def arr(p, shape, dt):
+            if int(np.prod(shape)) == 0:
+                return np.zeros(shape, dt)
+            return np.ctypeslib.as_array(p, shape=shape).view(dt).copy()
+
+        return CorrectionResults(
+            first=res.first_anchor,
+            status=arr(res.anchor_status, (na,), np.uint8),
+            num_edits=arr(res.anchor_num_edits, (na,), np.int32),
+            sequences=arr(ctypes.cast(res.anchor_sequences, ctypes.POINTER(ctypes.c_uint8)), (na, L), np.uint8),
+            cand_read_ids=arr(res.cand_read_ids, (nc,), np.uint32),
+            cand_anchor_ids=arr(res.cand_anchor_ids, (nc,), np.uint32),
+            cand_shifts=arr(res.cand_shifts, (nc,), np.int32),
+            cand_use_edits=arr(res.cand_use_edits, (nc,), np.uint8),
+            cand_sequences=arr(ctypes.cast(res.cand_sequences, ctypes.POINTER(ctypes.c_uint8)), (nc, L), np.uint8),
+        )
+
+    def correct_range_device(self, first: int = 0, count: int | None = None):
+        if count is None:
+            count = self.num_reads - first
+        self._check(self.lib.care_b200_correct_range_device(self._ctx, first, count), "correct_range_device")
+
+    def serialize(self, res: Results) -> bytes:
+        need = ctypes.c_size_t()
+        self._check(self.lib.care_b200_serialize_results(self._ctx, ctypes.byref(res), None, 0,
+                                                         ctypes.byref(need)), "serialize")
+        buf = np.zeros(need.value, np.uint8)
+        self._check(self.lib.care_b200_serialize_results(self._ctx, ctypes.byref(res), _ptr(buf, ctypes.c_uint8),
+                                                         need.value, ctypes.byref(need)), "serialize")
+        return buf.tobytes()
+
+    def write_output(self, path: str):
+        self._check(self.lib.care_b200_write_output(self._ctx, path.encode()), "write_output")
+
+    def last_stats(self):
+        st = (ctypes.c_uint64 * 3)()
+        self._check(self.lib.care_b200_last_stats(self._ctx, st, 3), "last_stats")
+        return {"anchors": st[0], "pairs": st[1], "candidate_corrections": st[2]}
+
+    def last_timing(self):
+        t = ctypes.c_float()
+        st = (ctypes.c_float * 3)()
+        self._check(self.lib.care_b200_last_timing(self._ctx, ctypes.byref(t), st, 3), "last_timing")
+        return t.value, list(st)
+
+
+def encode_reads(seqs: np.ndarray, lengths: np.ndarray):
+    """ASCII reads (n, Lmax) -> packed 2-bit rows (n, ceil(Lmax/16)) uint32, MSB-first,
+    zero padded; non-ACGT characters become A (caller handles N rotation)."""
+    n, Lmax = seqs.shape
+    code = np.zeros((n, Lmax), np.uint32)
+    code[seqs == ord("C")] = 1
+    code[seqs == ord("G")] = 2
+    code[seqs == ord("T")] = 3
+    valid = np.arange(Lmax)[None, :] < lengths[:, None]
+    code[~valid] = 0
+    pitch = (Lmax + 15) // 16
+    padded = np.zeros((n, pitch * 16), np.uint32)
+    padded[:, :Lmax] = code
+    padded = padded.reshape(n, pitch, 16)
+    shifts = (30 - 2 * np.arange(16, dtype=np.uint32))
+    return (padded << shifts).sum(axis=2, dtype=np.uint64).astype(np.uint32)
+
+
+def options_from_args(args: str | Sequence[str], **kw) -> Options:
+    """care-cpu command-line options (src/options.cpp:54-383) -> Options."""
+    toks = args.split() if isinstance(args, str) else list(args)
+    o = default_options()
+    flags = {"-q": "use_quality", "--useQualityScores": "use_quality",
+             "--excludeAmbiguous": "exclude_ambiguous", "--candidateCorrection": "correct_candidates",
+             "--correctionQualityLabels": "quality_labels"}
+    valued = {"-c": ("estimated_coverage", float), "--coverage": ("estimated_coverage", float),
+              "-k": ("kmerlength", int), "--kmerlength": ("kmerlength", int),
+              "-h": ("num_maps", int), "--hashmaps": ("num_maps", int),
+              "-t": ("threads", int), "--threads": ("threads", int),
+              "--qualityScoreBits": ("quality_bits", int),
+              "--minalignmentoverlap": ("min_overlap", int),
+              "--maxmismatchratio": ("max_error_rate", float),
+              "--minalignmentoverlapratio": ("min_overlap_ratio", float),
+              "--errorfactortuning": ("estimated_errorrate", float),
+              "--coveragefactortuning": ("m_coverage", float),
+              "--pairedFilterThreshold": ("paired_filter_threshold", float),
+              "--candidateCorrectionNewColumns": ("new_columns_to_correct", int),
+              "--batchsize": ("batch_size", int), "-g": ("device", int), "--gpu": ("device", int),
+              "--correctionType": ("correction_type", int)}
+    i = 0
+    while i < len(toks):
+        t = toks[i]
+        if t in flags:
+            setattr(o, flags[t], 1)
+        elif t == "--pairmode":
+            o.paired_end = 1 if toks[i + 1] in ("PE", "pe") else 0
+            i += 1
+        elif t in valued:
+            name, typ = valued[t]
+            setattr(o, name, typ(toks[i + 1]))
+            i += 1
+        else:
+            raise ValueError(f"unsupported option {t}")
+        i += 1
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o

@@ -1,0 +1,729 @@
+// capi.cu -- the C ABI (include/care_b200.h): context, device-resident read
+// storage and minhash tables, the batched correction pipeline, results.
+#include "../../include/care_b200.h"
+#include "hostio.hpp"
+#include "kernels.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <numeric>
+#include <string>
+#include <thread>
+#include <vector>
+
+using namespace careb200;
+
+namespace {
+
+// Device allocation that frees itself.
+struct DBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    DBuf() = default;
+    DBuf(const DBuf&) = delete;
+    DBuf& operator=(const DBuf&) = delete;
+    ~DBuf() { release(); }
+    void release() { if (p) cudaFree(p); p = nullptr; bytes = 0; }
+    cudaError_t ensure(size_t n) {
+        if (n <= bytes && p) return cudaSuccess;
+        release();
+        const cudaError_t e = cudaMalloc(&p, n ? n : 16);
+        if (e == cudaSuccess) bytes = n;
+        return e;
+    }
+    template <class T> T* as() const { return static_cast<T*>(p); }
+};
+
+// Pinned host allocation that frees itself.
+struct HBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    HBuf() = default;
+    HBuf(const HBuf&) = delete;
+    HBuf& operator=(const HBuf&) = delete;
+    ~HBuf() { release(); }
+    void release() { if (p) cudaFreeHost(p); p = nullptr; bytes = 0; }
+    cudaError_t ensure(size_t n) {
+        if (n <= bytes && p) return cudaSuccess;
+        release();
+        const cudaError_t e = cudaMallocHost(&p, n ? n : 16);
+        if (e == cudaSuccess) bytes = n;
+        return e;
+    }
+    template <class T> T* as() const { return static_cast<T*>(p); }
+};
+
+constexpr int kCandBlock = 128;
+constexpr int kAlignBlock = 128;
+constexpr int kMsaBlock = 128;
+
+}  // namespace
+
+struct care_b200_ctx {
+    care_b200_options opt{};
+    std::string err;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    float last_ms = 0.f, stage_ms[3] = {0.f, 0.f, 0.f};
+
+    // read storage
+    uint32_t n = 0;
+    int max_len = 0, seq_pitch = 0, qual_pitch = 0;
+    bool has_qual = false;
+    DBuf d_seq, d_qual, d_len, d_ambig;
+    std::vector<uint8_t> h_ambig;
+    std::vector<int32_t> h_len;
+    HostReads reads;                  // set when loaded from files
+    bool have_records = false;
+
+    // tables
+    int num_maps = 0, threshold = 0;
+    DBuf d_slots, d_values, d_tdesc;
+    std::vector<std::vector<uint64_t>> t_keys;
+    std::vector<std::vector<uint32_t>> t_off, t_val;
+    bool tables_ready = false;
+    uint32_t tables_reads = 0;        // storage size the tables were built for
+
+    // batch scratch
+    DBuf d_seg_off, d_seg_cnt, d_cand_ids, d_cand_anchor, d_ares, d_recs, d_counters, d_status;
+    unsigned long long cand_cap = 0;
+    DBuf d_st, d_ned, d_oseq;
+    DBuf d_cid, d_canc, d_cshift, d_cue, d_cseq;
+    unsigned long long corr_cap = 0;
+    HBuf h_small;
+
+    // results of the last call (pinned host)
+    HBuf r_status, r_nedits, r_seq;
+    HBuf r_cid, r_canc, r_cshift, r_cue, r_cseq;
+    uint64_t r_ncand = 0, r_pairs = 0;
+    uint32_t r_first = 0, r_count = 0;
+    bool r_valid = false;
+};
+
+namespace {
+
+int fail(care_b200_ctx* c, int code, const std::string& msg) {
+    if (c) c->err = msg;
+    return code;
+}
+
+int cuda_fail(care_b200_ctx* c, cudaError_t e, const char* where) {
+    return fail(c, CARE_B200_ECUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+#define CK(call, where)                                             \
+    do {                                                            \
+        const cudaError_t e_ = (call);                              \
+        if (e_ != cudaSuccess) return cuda_fail(ctx, e_, where);    \
+    } while (0)
+
+DevOptions make_dev_options(const care_b200_ctx* ctx) {
+    const care_b200_options& o = ctx->opt;
+    DevOptions d{};
+    d.k = o.kmerlength;
+    d.num_maps = ctx->num_maps ? ctx->num_maps : o.num_maps;
+    d.min_overlap = o.min_overlap;
+    d.new_columns = o.new_columns_to_correct;
+    d.use_quality = o.use_quality && ctx->has_qual;
+    d.quality_bits = o.quality_bits;
+    d.exclude_ambiguous = o.exclude_ambiguous;
+    d.correct_candidates = o.correct_candidates;
+    d.paired_end = o.paired_end;
+    d.threshold = ctx->threshold;
+    d.coverage_int = (int)o.estimated_coverage;
+    d.correction_type = o.correction_type;
+    d.max_error_rate = o.max_error_rate;
+    d.min_overlap_ratio = o.min_overlap_ratio;
+    d.estimated_errorrate = o.estimated_errorrate;
+    d.estimated_coverage = o.estimated_coverage;
+    d.m_coverage = o.m_coverage;
+    d.paired_filter_threshold = o.paired_filter_threshold;
+    d.kmer_mask = ~0ull >> ((32 - o.kmerlength) * 2);
+    return d;
+}
+
+DevReads make_dev_reads(const care_b200_ctx* ctx) {
+    DevReads r{};
+    r.seq = ctx->d_seq.as<uint32_t>();
+    r.qual = ctx->has_qual ? ctx->d_qual.as<uint32_t>() : nullptr;
+    r.len = ctx->d_len.as<int32_t>();
+    r.ambig = ctx->d_ambig.as<uint8_t>();
+    r.seq_pitch = ctx->seq_pitch;
+    r.qual_pitch = ctx->qual_pitch;
+    r.max_len = ctx->max_len;
+    r.n = ctx->n;
+    return r;
+}
+
+// calculateResultsPerMapThreshold (minhasherlimit.hpp:9-15) of int(coverage)
+int results_per_map_threshold(float coverage) {
+    const int cov = (int)coverage;
+    int r = (int)(cov * 2.5f);
+    r = std::min(r, 65535);
+    return std::max(10, r);
+}
+
+uint64_t host_murmur64(uint64_t x) {
+    x ^= x >> 33;
+    x *= 0xff51afd7ed558ccdULL;
+    x ^= x >> 33;
+    x *= 0xc4ceb9fe1a85ec53ULL;
+    x ^= x >> 33;
+    return x;
+}
+
+int validate_options(care_b200_ctx* ctx, const care_b200_options& o) {
+    // ProgramOptions::isValid, src/options.cpp:387-480, plus this library's limits
+    if (o.max_error_rate < 0.f || o.max_error_rate > 1.f) return fail(ctx, CARE_B200_EINVAL, "maxmismatchratio must be in [0,1]");
+    if (o.min_overlap < 1) return fail(ctx, CARE_B200_EINVAL, "min_overlap must be > 0");
+    if (o.min_overlap_ratio < 0.f || o.min_overlap_ratio > 1.f) return fail(ctx, CARE_B200_EINVAL, "min_overlap_ratio must be in [0,1]");
+    if (!(o.estimated_coverage > 0.f)) return fail(ctx, CARE_B200_EINVAL, "estimatedCoverage must be > 0");
+    if (!(o.estimated_errorrate > 0.f)) return fail(ctx, CARE_B200_EINVAL, "estimatedErrorrate must be > 0");
+    if (o.num_maps < 1 || o.num_maps > kMaxMaps) return fail(ctx, CARE_B200_EINVAL, "number of hash maps must be in [1,48]");
+    if (o.kmerlength < 1 || o.kmerlength > 32) return fail(ctx, CARE_B200_EINVAL, "kmer length must be in [1,32]");
+    if (o.quality_bits != 1 && o.quality_bits != 2 && o.quality_bits != 8) return fail(ctx, CARE_B200_EINVAL, "qualityScoreBits must be 1, 2 or 8");
+    if (o.correction_type != 0 && o.correction_type != 1) return fail(ctx, CARE_B200_EINVAL, "correction_type must be 0 or 1");
+    return CARE_B200_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void care_b200_default_options(care_b200_options* o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->kmerlength = 20;
+    o->num_maps = 48;
+    o->min_overlap = 30;
+    o->max_error_rate = 0.2f;
+    o->min_overlap_ratio = 0.30f;
+    o->estimated_errorrate = 0.06f;
+    o->estimated_coverage = 1.0f;
+    o->m_coverage = 0.6f;
+    o->paired_filter_threshold = 0.06f;
+    o->new_columns_to_correct = 15;
+    o->quality_bits = 8;
+    o->threads = 0;
+    o->device = 0;
+}
+
+int care_b200_create(const care_b200_options* opt, care_b200_ctx** out) {
+    if (!opt || !out) return CARE_B200_EINVAL;
+    *out = nullptr;
+    auto c = std::make_unique<care_b200_ctx>();
+    care_b200_ctx* ctx = c.get();
+    ctx->opt = *opt;
+    const int v = validate_options(ctx, *opt);
+    if (v) return v;
+    int ndev = 0;
+    CK(cudaGetDeviceCount(&ndev), "cudaGetDeviceCount");
+    if (opt->device < 0 || opt->device >= ndev) return CARE_B200_EINVAL;
+    CK(cudaSetDevice(opt->device), "cudaSetDevice");
+    CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    for (auto& e : ctx->ev) CK(cudaEventCreate(&e), "cudaEventCreate");
+    float qw[256];
+    quality_weights(qw);
+    CK(cudaMemcpyToSymbol(c_qweight, qw, sizeof(qw)), "quality weights");
+    ctx->threshold = results_per_map_threshold(opt->estimated_coverage);
+    *out = c.release();
+    return CARE_B200_OK;
+}
+
+int care_b200_destroy(care_b200_ctx* ctx) {
+    if (!ctx) return CARE_B200_OK;
+    cudaSetDevice(ctx->opt.device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    for (auto& e : ctx->ev) if (e) cudaEventDestroy(e);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return CARE_B200_OK;
+}
+
+const char* care_b200_last_error(const care_b200_ctx* ctx) {
+    return ctx ? ctx->err.c_str() : "no context";
+}
+
+int care_b200_upload_reads(care_b200_ctx* ctx, const uint32_t* packed, size_t pitch_ints,
+                           const int32_t* lengths, const uint32_t* enc_quals, size_t qual_pitch_ints,
+                           const uint32_t* ambiguous_ids, size_t num_ambiguous, uint32_t num_reads) {
+    if (!ctx) return CARE_B200_EINVAL;
+    if (!packed || !lengths || num_reads == 0 || pitch_ints == 0) return fail(ctx, CARE_B200_EINVAL, "empty read storage");
+    if (ctx->opt.paired_end && (num_reads % 2)) return fail(ctx, CARE_B200_EINVAL, "paired-end storage needs an even number of reads");
+    int mx = 0;
+    for (uint32_t i = 0; i < num_reads; i++) mx = std::max(mx, (int)lengths[i]);
+    if (mx > kMaxLen) return fail(ctx, CARE_B200_ELIMIT, "reads longer than 256 bases are not supported");
+    if ((size_t)(mx + 15) / 16 > pitch_ints) return fail(ctx, CARE_B200_EINVAL, "pitch_ints too small for the longest read");
+    CK(cudaSetDevice(ctx->opt.device), "cudaSetDevice");
+    ctx->n = num_reads;
+    ctx->max_len = mx;
+    ctx->seq_pitch = (int)pitch_ints;
+    ctx->has_qual = enc_quals != nullptr && ctx->opt.use_quality;
+    ctx->qual_pitch = ctx->has_qual ? (int)qual_pitch_ints : 0;
+    if (ctx->has_qual && (size_t)quality_ints(mx, ctx->opt.quality_bits) > qual_pitch_ints)
+        return fail(ctx, CARE_B200_EINVAL, "qual_pitch_ints too small for the longest read");
+    CK(ctx->d_seq.ensure((size_t)num_reads * pitch_ints * 4), "alloc reads");
+    CK(cudaMemcpyAsync(ctx->d_seq.p, packed, (size_t)num_reads * pitch_ints * 4, cudaMemcpyHostToDevice, ctx->stream), "upload reads");
+    CK(ctx->d_len.ensure((size_t)num_reads * 4), "alloc lengths");
+    CK(cudaMemcpyAsync(ctx->d_len.p, lengths, (size_t)num_reads * 4, cudaMemcpyHostToDevice, ctx->stream), "upload lengths");
+    if (ctx->has_qual) {
+        CK(ctx->d_qual.ensure((size_t)num_reads * qual_pitch_ints * 4), "alloc qualities");
+        CK(cudaMemcpyAsync(ctx->d_qual.p, enc_quals, (size_t)num_reads * qual_pitch_ints * 4, cudaMemcpyHostToDevice, ctx->stream), "upload qualities");
+    }
+    ctx->h_len.assign(lengths, lengths + num_reads);
+    ctx->h_ambig.assign(num_reads, 0);
+    for (size_t i = 0; i < num_ambiguous; i++) {
+        if (ambiguous_ids[i] >= num_reads) return fail(ctx, CARE_B200_EINVAL, "ambiguous id out of range");
+        ctx->h_ambig[ambiguous_ids[i]] = 1;
+    }
+    CK(ctx->d_ambig.ensure(num_reads), "alloc ambiguous flags");
+    CK(cudaMemcpyAsync(ctx->d_ambig.p, ctx->h_ambig.data(), num_reads, cudaMemcpyHostToDevice, ctx->stream), "upload ambiguous flags");
+    CK(cudaStreamSynchronize(ctx->stream), "upload");
+    if (ctx->tables_ready && ctx->t_keys.size() && num_reads != ctx->tables_reads) ctx->tables_ready = false;
+    ctx->r_valid = false;
+    return CARE_B200_OK;
+}
+
+int care_b200_upload_tables(care_b200_ctx* ctx, int num_maps, const uint64_t* const* keys,
+                            const uint32_t* const* offsets, const uint32_t* const* values,
+                            const size_t* nkeys) {
+    if (!ctx) return CARE_B200_EINVAL;
+    if (num_maps < 1 || num_maps > kMaxMaps || !keys || !offsets || !values || !nkeys)
+        return fail(ctx, CARE_B200_EINVAL, "invalid tables");
+    CK(cudaSetDevice(ctx->opt.device), "cudaSetDevice");
+    // open-addressing key index per map: capacity a power of two >= 2 keys
+    std::vector<TableDesc> desc(num_maps);
+    size_t total_slots = 0, total_values = 0;
+    for (int m = 0; m < num_maps; m++) {
+        size_t cap = 16;
+        while (cap < 2 * nkeys[m]) cap <<= 1;
+        desc[m].slot_base = total_slots;
+        desc[m].value_base = total_values;
+        desc[m].mask = (uint32_t)(cap - 1);
+        total_slots += cap;
+        total_values += nkeys[m] ? offsets[m][nkeys[m]] : 0;
+    }
+    if (total_values >= 0xFFFFFFFFull) return fail(ctx, CARE_B200_ELIMIT, "tables too large");
+    std::vector<Slot> slots(total_slots, Slot{0, 0, 0});
+    std::vector<uint32_t> vals(total_values);
+    for (int m = 0; m < num_maps; m++) {
+        Slot* s = slots.data() + desc[m].slot_base;
+        const uint32_t mask = desc[m].mask;
+        for (size_t i = 0; i < nkeys[m]; i++) {
+            const uint32_t cnt = offsets[m][i + 1] - offsets[m][i];
+            if (cnt == 0) continue;
+            uint32_t pos = (uint32_t)host_murmur64(keys[m][i]) & mask;
+            while (s[pos].count != 0) pos = (pos + 1) & mask;
+            s[pos].key = keys[m][i];
+            s[pos].offset = offsets[m][i];
+            s[pos].count = cnt;
+        }
+        if (nkeys[m]) std::memcpy(vals.data() + desc[m].value_base, values[m], (size_t)offsets[m][nkeys[m]] * 4);
+    }
+    CK(ctx->d_slots.ensure(total_slots * sizeof(Slot)), "alloc slots");
+    CK(ctx->d_values.ensure(std::max<size_t>(total_values, 1) * 4), "alloc values");
+    CK(ctx->d_tdesc.ensure(num_maps * sizeof(TableDesc)), "alloc table descriptors");
+    CK(cudaMemcpy(ctx->d_slots.p, slots.data(), total_slots * sizeof(Slot), cudaMemcpyHostToDevice), "upload slots");
+    if (total_values) CK(cudaMemcpy(ctx->d_values.p, vals.data(), total_values * 4, cudaMemcpyHostToDevice), "upload values");
+    CK(cudaMemcpy(ctx->d_tdesc.p, desc.data(), num_maps * sizeof(TableDesc), cudaMemcpyHostToDevice), "upload descriptors");
+    ctx->num_maps = num_maps;
+    ctx->t_keys.assign(num_maps, {});
+    ctx->t_off.assign(num_maps, {});
+    ctx->t_val.assign(num_maps, {});
+    for (int m = 0; m < num_maps; m++) {
+        ctx->t_keys[m].assign(keys[m], keys[m] + nkeys[m]);
+        ctx->t_off[m].assign(offsets[m], offsets[m] + nkeys[m] + 1);
+        const uint32_t nv = nkeys[m] ? offsets[m][nkeys[m]] : 0;
+        ctx->t_val[m].assign(values[m], values[m] + nv);
+    }
+    ctx->tables_ready = true;
+    ctx->tables_reads = ctx->n;
+    return CARE_B200_OK;
+}
+
+int care_b200_build_tables(care_b200_ctx* ctx) {
+    if (!ctx) return CARE_B200_EINVAL;
+    if (ctx->n == 0) return fail(ctx, CARE_B200_ESTATE, "no reads uploaded");
+    CK(cudaSetDevice(ctx->opt.device), "cudaSetDevice");
+    const int h = ctx->opt.num_maps;
+    ctx->num_maps = h;
+    DevOptions o = make_dev_options(ctx);
+    DevReads r = make_dev_reads(ctx);
+    // signatures of all reads on the device (insert, ordinaryminhasher.hpp:376-426)
+    std::vector<uint64_t> sig((size_t)ctx->n * h);
+    DBuf d_sig;
+    const uint32_t chunk = 1u << 20;
+    CK(d_sig.ensure((size_t)std::min(ctx->n, chunk) * h * 8), "alloc signatures");
+    for (uint32_t b = 0; b < ctx->n; b += chunk) {
+        const uint32_t cnt = std::min(chunk, ctx->n - b);
+        const int wpb = 8;
+        k_signatures<<<(cnt + wpb - 1) / wpb, 32 * wpb, 0, ctx->stream>>>(o, r, b, cnt, d_sig.as<unsigned long long>());
+        CK(cudaGetLastError(), "k_signatures");
+        CK(cudaMemcpyAsync(sig.data() + (size_t)b * h, d_sig.p, (size_t)cnt * h * 8, cudaMemcpyDeviceToHost, ctx->stream), "signatures");
+    }
+    CK(cudaStreamSynchronize(ctx->stream), "signatures");
+    // group per map: values of one key ascending, buckets with fewer than 2
+    // or more than threshold values cleared (groupbykey.hpp:99-249)
+    const uint32_t n = ctx->n;
+    const int thr = ctx->threshold;
+    std::vector<std::vector<uint64_t>> K(h);
+    std::vector<std::vector<uint32_t>> O(h), Vv(h);
+    auto build = [&](int m0, int m1) {
+        std::vector<std::pair<uint64_t, uint32_t>> kv(n);
+        for (int m = m0; m < m1; m++) {
+            for (uint32_t i = 0; i < n; i++) kv[i] = {sig[(size_t)i * h + m], i};
+            std::sort(kv.begin(), kv.end());
+            auto& keys = K[m]; auto& off = O[m]; auto& val = Vv[m];
+            off.push_back(0);
+            for (uint32_t i = 0; i < n;) {
+                uint32_t e = i;
+                while (e < n && kv[e].first == kv[i].first) e++;
+                const uint32_t c = e - i;
+                if (c >= 2 && (int)c <= thr) {
+                    keys.push_back(kv[i].first);
+                    for (uint32_t x = i; x < e; x++) val.push_back(kv[x].second);
+                    off.push_back((uint32_t)val.size());
+                }
+                i = e;
+            }
+        }
+    };
+    unsigned nt = ctx->opt.threads > 0 ? (unsigned)ctx->opt.threads : std::thread::hardware_concurrency();
+    nt = std::max(1u, std::min<unsigned>(nt, (unsigned)h));
+    std::vector<std::thread> th;
+    for (unsigned t = 0; t < nt; t++) th.emplace_back(build, (int)(h * t / nt), (int)(h * (t + 1) / nt));
+    for (auto& x : th) x.join();
+    std::vector<const uint64_t*> kp(h);
+    std::vector<const uint32_t*> op(h), vp(h);
+    std::vector<size_t> nk(h);
+    for (int m = 0; m < h; m++) { kp[m] = K[m].data(); op[m] = O[m].data(); vp[m] = Vv[m].data(); nk[m] = K[m].size(); }
+    return care_b200_upload_tables(ctx, h, kp.data(), op.data(), vp.data(), nk.data());
+}
+
+int care_b200_get_table(care_b200_ctx* ctx, int map, const uint64_t** keys, const uint32_t** offsets,
+                        const uint32_t** values, size_t* nkeys) {
+    if (!ctx) return CARE_B200_EINVAL;
+    if (!ctx->tables_ready || map < 0 || map >= ctx->num_maps) return fail(ctx, CARE_B200_EINVAL, "no such table");
+    *keys = ctx->t_keys[map].data();
+    *offsets = ctx->t_off[map].data();
+    *values = ctx->t_val[map].data();
+    *nkeys = ctx->t_keys[map].size();
+    return CARE_B200_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+// Runs the three stages for anchors [first, first+count) into the device
+// output buffers; grows the arenas and repeats on overflow.
+int run_batch(care_b200_ctx* ctx, uint32_t first, uint32_t count, bool timed) {
+    const DevOptions o = make_dev_options(ctx);
+    const DevReads r = make_dev_reads(ctx);
+    const int h = ctx->num_maps;
+    // shared hash set for de-duplication: > num_maps * threshold entries
+    const size_t tmax = (size_t)h * ctx->threshold;
+    int set_log2 = 4;
+    while ((size_t)1 << set_log2 < (tmax * 4 + 2) / 3 + 1) set_log2++;
+    const int groups = kCandBlock / h;
+    const size_t cand_smem = CandSmem::total(ctx->max_len, groups, h, ctx->seq_pitch, 1 << set_log2);
+    if (cand_smem > 227 * 1024) return fail(ctx, CARE_B200_ELIMIT, "num_maps * threshold too large for the de-duplication set");
+    CK(cudaFuncSetAttribute(k_candidates<kCandBlock>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cand_smem), "smem attr");
+
+    CK(ctx->d_seg_off.ensure((size_t)count * 4), "alloc");
+    CK(ctx->d_seg_cnt.ensure((size_t)count * 4), "alloc");
+    CK(ctx->d_counters.ensure(64), "alloc");
+    CK(ctx->d_status.ensure(16), "alloc");
+    CK(ctx->d_st.ensure(count), "alloc");
+    CK(ctx->d_ned.ensure((size_t)count * 4), "alloc");
+    CK(ctx->d_oseq.ensure((size_t)count * ctx->max_len), "alloc");
+    CK(ctx->h_small.ensure(64), "alloc");
+    if (ctx->cand_cap < (unsigned long long)count * 96) ctx->cand_cap = (unsigned long long)count * 96;
+    if (ctx->corr_cap == 0) ctx->corr_cap = ctx->opt.correct_candidates ? (unsigned long long)count * 16 + 1024 : 1024;
+
+    for (int attempt = 0; attempt < 8; ++attempt) {
+        const unsigned long long cap = ctx->cand_cap;
+        CK(ctx->d_cand_ids.ensure(cap * 4), "alloc candidates");
+        CK(ctx->d_cand_anchor.ensure(cap * 4), "alloc candidates");
+        CK(ctx->d_ares.ensure(cap * sizeof(AlignRes)), "alloc alignments");
+        CK(ctx->d_recs.ensure(cap * sizeof(CandRec)), "alloc records");
+        const unsigned long long ccap = ctx->corr_cap;
+        CK(ctx->d_cid.ensure(ccap * 4), "alloc");
+        CK(ctx->d_canc.ensure(ccap * 4), "alloc");
+        CK(ctx->d_cshift.ensure(ccap * 4), "alloc");
+        CK(ctx->d_cue.ensure(ccap), "alloc");
+        CK(ctx->d_cseq.ensure(ccap * ctx->max_len), "alloc");
+
+        unsigned long long* counters = ctx->d_counters.as<unsigned long long>();
+        int* status = ctx->d_status.as<int>();
+        CK(cudaMemsetAsync(counters, 0, 64, ctx->stream), "memset");
+        CK(cudaMemsetAsync(status, 0, 16, ctx->stream), "memset");
+        if (timed) CK(cudaEventRecord(ctx->ev[0], ctx->stream), "event");
+        k_candidates<kCandBlock><<<count, kCandBlock, cand_smem, ctx->stream>>>(
+            o, r, ctx->d_tdesc.as<TableDesc>(), ctx->d_slots.as<Slot>(), ctx->d_values.as<uint32_t>(), first,
+            count, set_log2, ctx->d_cand_ids.as<uint32_t>(), ctx->d_cand_anchor.as<uint32_t>(),
+            ctx->d_seg_off.as<uint32_t>(), ctx->d_seg_cnt.as<uint32_t>(), counters, cap, status);
+        CK(cudaGetLastError(), "k_candidates");
+        if (timed) CK(cudaEventRecord(ctx->ev[1], ctx->stream), "event");
+        const unsigned long long ablocks = (cap + kAlignBlock - 1) / kAlignBlock;
+        k_align<kAlignBlock><<<(unsigned)ablocks, kAlignBlock, 0, ctx->stream>>>(
+            o, r, first, ctx->d_cand_ids.as<uint32_t>(), ctx->d_cand_anchor.as<uint32_t>(),
+            ctx->d_seg_off.as<uint32_t>(), ctx->d_seg_cnt.as<uint32_t>(), counters, cap, status,
+            ctx->d_ares.as<AlignRes>());
+        CK(cudaGetLastError(), "k_align");
+        if (timed) CK(cudaEventRecord(ctx->ev[2], ctx->stream), "event");
+        MsaOut mo;
+        mo.status = ctx->d_st.as<uint8_t>();
+        mo.nedits = ctx->d_ned.as<int32_t>();
+        mo.seq = ctx->d_oseq.as<char>();
+        mo.corr_id = ctx->d_cid.as<uint32_t>();
+        mo.corr_anchor = ctx->d_canc.as<uint32_t>();
+        mo.corr_shift = ctx->d_cshift.as<int32_t>();
+        mo.corr_use_edits = ctx->d_cue.as<uint8_t>();
+        mo.corr_seq = ctx->d_cseq.as<char>();
+        mo.corr_count = counters + 1;
+        mo.corr_cap = ccap;
+        const int maxcols = 3 * ctx->max_len;
+        if (maxcols <= kMsaBlock * 3)
+            k_msa<kMsaBlock, 3><<<count, kMsaBlock, 0, ctx->stream>>>(
+                o, r, first, count, nullptr, ctx->d_cand_ids.as<uint32_t>(), ctx->d_seg_off.as<uint32_t>(),
+                ctx->d_seg_cnt.as<uint32_t>(), ctx->d_ares.as<AlignRes>(), ctx->d_recs.as<CandRec>(), mo, status);
+        else
+            k_msa<kMsaBlock, 6><<<count, kMsaBlock, 0, ctx->stream>>>(
+                o, r, first, count, nullptr, ctx->d_cand_ids.as<uint32_t>(), ctx->d_seg_off.as<uint32_t>(),
+                ctx->d_seg_cnt.as<uint32_t>(), ctx->d_ares.as<AlignRes>(), ctx->d_recs.as<CandRec>(), mo, status);
+        CK(cudaGetLastError(), "k_msa");
+        if (timed) CK(cudaEventRecord(ctx->ev[3], ctx->stream), "event");
+        CK(cudaMemcpyAsync(ctx->h_small.p, counters, 16, cudaMemcpyDeviceToHost, ctx->stream), "counters");
+        CK(cudaMemcpyAsync(ctx->h_small.as<char>() + 16, status, 4, cudaMemcpyDeviceToHost, ctx->stream), "status");
+        CK(cudaStreamSynchronize(ctx->stream), "batch");
+        const unsigned long long used = ctx->h_small.as<unsigned long long>()[0];
+        const unsigned long long corr = ctx->h_small.as<unsigned long long>()[1];
+        const int st = *(int*)(ctx->h_small.as<char>() + 16);
+        if (st & kStatusColumns) return fail(ctx, CARE_B200_ELIMIT, "MSA wider than the kernel's column capacity");
+        bool again = false;
+        if ((st & kStatusCandOverflow) || used > cap) { ctx->cand_cap = used + used / 8 + 1024; again = true; }
+        if ((st & kStatusCorrOverflow) || corr > ccap) { ctx->corr_cap = corr + corr / 8 + 1024; again = true; }
+        if (again) continue;
+        if (timed) {
+            float a = 0, b = 0, c = 0;
+            cudaEventElapsedTime(&a, ctx->ev[0], ctx->ev[1]);
+            cudaEventElapsedTime(&b, ctx->ev[1], ctx->ev[2]);
+            cudaEventElapsedTime(&c, ctx->ev[2], ctx->ev[3]);
+            ctx->stage_ms[0] += a; ctx->stage_ms[1] += b; ctx->stage_ms[2] += c;
+            ctx->last_ms += a + b + c;
+        }
+        ctx->r_ncand += corr;
+        ctx->r_pairs += used;
+        return (int)std::min<unsigned long long>(corr, 0x7fffffff);
+    }
+    return fail(ctx, CARE_B200_ENOMEM, "arena growth did not converge");
+}
+
+int correct_impl(care_b200_ctx* ctx, uint32_t first, uint32_t count, care_b200_results* res, bool copy) {
+    if (!ctx) return CARE_B200_EINVAL;
+    if (ctx->n == 0) return fail(ctx, CARE_B200_ESTATE, "no reads uploaded");
+    if (!ctx->tables_ready) return fail(ctx, CARE_B200_ESTATE, "no tables uploaded or built");
+    if ((uint64_t)first + count > ctx->n) return fail(ctx, CARE_B200_EINVAL, "anchor range beyond the read storage");
+    if (ctx->opt.paired_end && ((first | count) & 1)) return fail(ctx, CARE_B200_EINVAL, "paired-end ranges must be pair aligned");
+    CK(cudaSetDevice(ctx->opt.device), "cudaSetDevice");
+    uint32_t B = ctx->opt.batch_size > 0 ? (uint32_t)ctx->opt.batch_size : (1u << 21);
+    if (ctx->opt.paired_end) B &= ~1u;
+    if (B == 0) B = 2;
+    ctx->last_ms = 0.f;
+    ctx->stage_ms[0] = ctx->stage_ms[1] = ctx->stage_ms[2] = 0.f;
+    ctx->r_ncand = 0;
+    ctx->r_pairs = 0;
+    ctx->r_valid = false;
+    const int L = ctx->max_len;
+    if (copy) {
+        CK(ctx->r_status.ensure(std::max<size_t>(count, 1)), "alloc results");
+        CK(ctx->r_nedits.ensure((size_t)std::max<size_t>(count, 1) * 4), "alloc results");
+        CK(ctx->r_seq.ensure((size_t)std::max<size_t>(count, 1) * L), "alloc results");
+    }
+    std::vector<uint64_t> corr_counts;
+    uint64_t corr_total = 0;
+    for (uint32_t b = 0; b < count; b += B) {
+        const uint32_t cnt = std::min(B, count - b);
+        const uint64_t before = ctx->r_ncand;
+        const int rc = run_batch(ctx, first + b, cnt, true);
+        if (rc < 0) return rc;
+        const uint64_t nc = ctx->r_ncand - before;
+        if (copy) {
+            CK(cudaMemcpyAsync(ctx->r_status.as<uint8_t>() + b, ctx->d_st.p, cnt, cudaMemcpyDeviceToHost, ctx->stream), "results");
+            CK(cudaMemcpyAsync(ctx->r_nedits.as<int32_t>() + b, ctx->d_ned.p, (size_t)cnt * 4, cudaMemcpyDeviceToHost, ctx->stream), "results");
+            CK(cudaMemcpyAsync(ctx->r_seq.as<char>() + (size_t)b * L, ctx->d_oseq.p, (size_t)cnt * L, cudaMemcpyDeviceToHost, ctx->stream), "results");
+            if (nc) {
+                const uint64_t need = corr_total + nc;
+                // grow the pinned candidate arrays, keeping earlier batches
+                auto grow = [&](HBuf& hb, size_t elem) -> cudaError_t {
+                    if (hb.bytes >= need * elem) return cudaSuccess;
+                    HBuf nb;
+                    const cudaError_t e = nb.ensure(std::max<size_t>(need * elem * 3 / 2, 64));
+                    if (e != cudaSuccess) return e;
+                    if (hb.p && corr_total) std::memcpy(nb.p, hb.p, corr_total * elem);
+                    std::swap(hb.p, nb.p); std::swap(hb.bytes, nb.bytes);
+                    return cudaSuccess;
+                };
+                CK(cudaStreamSynchronize(ctx->stream), "results");
+                CK(grow(ctx->r_cid, 4), "alloc"); CK(grow(ctx->r_canc, 4), "alloc"); CK(grow(ctx->r_cshift, 4), "alloc");
+                CK(grow(ctx->r_cue, 1), "alloc"); CK(grow(ctx->r_cseq, (size_t)L), "alloc");
+                CK(cudaMemcpyAsync(ctx->r_cid.as<uint32_t>() + corr_total, ctx->d_cid.p, nc * 4, cudaMemcpyDeviceToHost, ctx->stream), "results");
+                CK(cudaMemcpyAsync(ctx->r_canc.as<uint32_t>() + corr_total, ctx->d_canc.p, nc * 4, cudaMemcpyDeviceToHost, ctx->stream), "results");
+                CK(cudaMemcpyAsync(ctx->r_cshift.as<int32_t>() + corr_total, ctx->d_cshift.p, nc * 4, cudaMemcpyDeviceToHost, ctx->stream), "results");
+                CK(cudaMemcpyAsync(ctx->r_cue.as<uint8_t>() + corr_total, ctx->d_cue.p, nc, cudaMemcpyDeviceToHost, ctx->stream), "results");
+                CK(cudaMemcpyAsync(ctx->r_cseq.as<char>() + corr_total * L, ctx->d_cseq.p, nc * L, cudaMemcpyDeviceToHost, ctx->stream), "results");
+            }
+            CK(cudaStreamSynchronize(ctx->stream), "results");
+        }
+        corr_total += nc;
+    }
+    ctx->r_ncand = corr_total;
+    ctx->r_first = first;
+    ctx->r_count = count;
+    ctx->r_valid = copy;
+    if (res) {
+        std::memset(res, 0, sizeof(*res));
+        res->first_anchor = first;
+        res->num_anchors = count;
+        res->max_length = L;
+        if (copy) {
+            res->anchor_status = ctx->r_status.as<uint8_t>();
+            res->anchor_num_edits = ctx->r_nedits.as<int32_t>();
+            res->anchor_sequences = ctx->r_seq.as<char>();
+            res->num_candidates = corr_total;
+            res->cand_read_ids = ctx->r_cid.as<uint32_t>();
+            res->cand_anchor_ids = ctx->r_canc.as<uint32_t>();
+            res->cand_shifts = ctx->r_cshift.as<int32_t>();
+            res->cand_use_edits = ctx->r_cue.as<uint8_t>();
+            res->cand_sequences = ctx->r_cseq.as<char>();
+        }
+    }
+    return CARE_B200_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int care_b200_correct_range(care_b200_ctx* ctx, uint32_t first, uint32_t count, care_b200_results* res) {
+    return correct_impl(ctx, first, count, res, true);
+}
+
+int care_b200_correct_range_device(care_b200_ctx* ctx, uint32_t first, uint32_t count) {
+    return correct_impl(ctx, first, count, nullptr, false);
+}
+
+int care_b200_serialize_results(care_b200_ctx* ctx, const care_b200_results* res, uint8_t* out,
+                                size_t capacity, size_t* needed) {
+    if (!ctx || !res || !needed) return CARE_B200_EINVAL;
+    size_t pos = 0;
+    const int L = res->max_length;
+    auto put = [&](const void* p, size_t nb) {
+        if (out && pos + nb <= capacity) std::memcpy(out + pos, p, nb);
+        pos += nb;
+    };
+    std::vector<char> dec((size_t)L + 1);
+    auto decode = [&](uint32_t id, int len) {
+        std::vector<uint32_t> row(ctx->seq_pitch);
+        cudaMemcpy(row.data(), ctx->d_seq.as<uint32_t>() + (size_t)id * ctx->seq_pitch, ctx->seq_pitch * 4, cudaMemcpyDeviceToHost);
+        for (int p = 0; p < len; p++) dec[p] = "ACGT"[(row[p >> 4] >> (30 - 2 * (p & 15))) & 3u];
+    };
+    // EncodedTempCorrectedSequence::encodeDataIntoEncodedCorrectedSequence,
+    // correctedsequence.hpp:262-336
+    auto record = [&](uint32_t id, bool hq, bool useEdits, int type, int shift, const char* seq, int len) {
+        std::vector<int> epos;
+        std::vector<char> ebase;
+        if (useEdits) {
+            decode(id, len);
+            for (int p = 0; p < len; p++) if (seq[p] != dec[p]) { epos.push_back(p); ebase.push_back(seq[p]); }
+        }
+        uint32_t nbytes = useEdits ? (uint32_t)(4 + epos.size() * 5) : (uint32_t)(4 + len);
+        if (type == 1) nbytes += 4;
+        const uint32_t flags = ((uint32_t)hq << 31) | ((uint32_t)useEdits << 30) | ((uint32_t)type << 29) | nbytes;
+        put(&id, 4);
+        put(&flags, 4);
+        if (useEdits) {
+            const int ne = (int)epos.size();
+            put(&ne, 4);
+            for (int p : epos) put(&p, 4);
+            for (char c : ebase) put(&c, 1);
+        } else {
+            put(&len, 4);
+            put(seq, (size_t)len);
+        }
+        if (type == 1) put(&shift, 4);
+    };
+    for (uint32_t k = 0; k < res->num_anchors; k++) {
+        const uint8_t st = res->anchor_status[k];
+        if (!(st & 1)) continue;
+        const bool hq = st & 2, ue = st & 4;
+        if (hq && ue && res->anchor_num_edits[k] == 0) continue;   // correct_cpu.cpp:263-264
+        const uint32_t id = res->first_anchor + k;
+        record(id, hq, ue, 0, 0, res->anchor_sequences + (size_t)k * L, ctx->h_len[id]);
+    }
+    for (uint64_t i = 0; i < res->num_candidates; i++) {
+        const uint32_t id = res->cand_read_ids[i];
+        record(id, false, res->cand_use_edits[i], 1, res->cand_shifts[i], res->cand_sequences + i * L, ctx->h_len[id]);
+    }
+    *needed = pos;
+    if (out && pos > capacity) return fail(ctx, CARE_B200_EINVAL, "serialization buffer too small");
+    return CARE_B200_OK;
+}
+
+int care_b200_load_reads_from_files(care_b200_ctx* ctx, const char* const* files, int num_files) {
+    if (!ctx || !files || num_files < 1 || num_files > 2) return CARE_B200_EINVAL;
+    std::vector<std::string> fs;
+    for (int i = 0; i < num_files; i++) fs.emplace_back(files[i]);
+    const std::string e = load_reads(fs, ctx->opt.paired_end, ctx->opt.use_quality, ctx->opt.quality_bits, ctx->reads);
+    if (!e.empty()) return fail(ctx, CARE_B200_EIO, e);
+    HostReads& h = ctx->reads;
+    if (h.n == 0) return fail(ctx, CARE_B200_EINVAL, "no reads in input");
+    ctx->have_records = true;
+    return care_b200_upload_reads(ctx, h.seq.data(), h.seq_pitch, h.len.data(),
+                                  h.has_quality ? h.qual.data() : nullptr, h.qual_pitch,
+                                  h.ambiguous_ids.data(), h.ambiguous_ids.size(), h.n);
+}
+
+int care_b200_write_output(care_b200_ctx* ctx, const char* outfile) {
+    if (!ctx || !outfile) return CARE_B200_EINVAL;
+    if (!ctx->have_records) return fail(ctx, CARE_B200_ESTATE, "reads were not loaded from files");
+    if (!ctx->r_valid) return fail(ctx, CARE_B200_ESTATE, "no correction results");
+    HostCorrections c;
+    c.first = ctx->r_first;
+    c.count = ctx->r_count;
+    c.max_len = ctx->max_len;
+    c.status = ctx->r_status.as<uint8_t>();
+    c.nedits = ctx->r_nedits.as<int32_t>();
+    c.seq = ctx->r_seq.as<char>();
+    c.ncand = ctx->r_ncand;
+    c.cand_id = ctx->r_cid.as<uint32_t>();
+    c.cand_use_edits = ctx->r_cue.as<uint8_t>();
+    c.cand_seq = ctx->r_cseq.as<char>();
+    const std::string e = write_corrected(ctx->reads, c, ctx->opt.quality_labels, outfile);
+    if (!e.empty()) return fail(ctx, CARE_B200_EIO, e);
+    return CARE_B200_OK;
+}
+
+int care_b200_last_timing(const care_b200_ctx* ctx, float* total_ms, float* stage_ms, int nstages) {
+    if (!ctx) return CARE_B200_EINVAL;
+    if (total_ms) *total_ms = ctx->last_ms;
+    for (int i = 0; i < nstages && i < 3 && stage_ms; i++) stage_ms[i] = ctx->stage_ms[i];
+    return CARE_B200_OK;
+}
+
+int care_b200_last_stats(const care_b200_ctx* ctx, uint64_t* stats, int nstats) {
+    if (!ctx || !stats) return CARE_B200_EINVAL;
+    const uint64_t v[3] = {ctx->r_count, ctx->r_pairs, ctx->r_ncand};
+    for (int i = 0; i < nstats && i < 3; i++) stats[i] = v[i];
+    return CARE_B200_OK;
+}
+
+uint32_t care_b200_num_reads(const care_b200_ctx* ctx) { return ctx ? ctx->n : 0; }
+int care_b200_max_length(const care_b200_ctx* ctx) { return ctx ? ctx->max_len : 0; }
+int care_b200_num_maps(const care_b200_ctx* ctx) { return ctx ? ctx->num_maps : 0; }
+
+}  // extern "C"

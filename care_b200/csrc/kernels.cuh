@@ -1,0 +1,763 @@
+// kernels.cuh -- the three device stages of one correction batch.
+//
+//   k_candidates : minhash signature + table lookup + de-duplication
+//                  (one CTA per anchor)
+//   k_align      : shifted Hamming distance, both strands, orientation,
+//                  pair flag (one thread per (anchor, candidate) pair)
+//   k_msa        : alignment filters, MSA build/refine, consensus
+//                  correction of anchor and candidates (one CTA per anchor)
+#pragma once
+#include "device.cuh"
+
+namespace careb200 {
+
+__constant__ float c_qweight[256];    // QualityScoreConversion table (qualityscoreweights.hpp:16-31)
+
+// ---------------------------------------------------------------------------
+// Stage 1: candidate read ids per anchor.
+//   CPUSequenceHasher::hashInto       include/cpusequencehasher.hpp:88-125
+//   forEachEncodedCanonicalKmer...    include/sequencehelpers.hpp:844-926
+//   OrdinaryCpuMinhasher::determineNumValues/retrieveValues/queryMap
+//                                     include/ordinaryminhasher.hpp:135-221,437-449
+//   determineCandidateReadIds         include/corrector.hpp:571-650
+// The table-major concatenation is followed by sort+unique in the reference;
+// here a shared-memory hash set removes duplicates and a bitonic sort orders
+// the (few) unique ids: same set, same ascending order.
+// ---------------------------------------------------------------------------
+constexpr uint32_t kEmpty = 0xFFFFFFFFu;
+
+struct CandSmem {
+    // dynamic shared memory layout, all offsets in bytes
+    static __host__ __device__ size_t canon(int) { return 0; }
+    static __host__ __device__ size_t partial(int maxlen) { return (size_t)(maxlen + 8) * 8; }
+    static __host__ __device__ size_t seq(int maxlen, int groups, int maps) {
+        return partial(maxlen) + (size_t)groups * maps * 8;
+    }
+    static __host__ __device__ size_t qinfo(int maxlen, int groups, int maps, int pitch) {
+        return seq(maxlen, groups, maps) + (size_t)(pitch + 4) * 4;
+    }
+    static __host__ __device__ size_t set(int maxlen, int groups, int maps, int pitch) {
+        return qinfo(maxlen, groups, maps, pitch) + (size_t)(3 * kMaxMaps + 8) * 4;
+    }
+    static __host__ __device__ size_t total(int maxlen, int groups, int maps, int pitch, int setcap) {
+        return set(maxlen, groups, maps, pitch) + (size_t)setcap * 4 * 2;
+    }
+};
+
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK)
+k_candidates(DevOptions o, DevReads r, const TableDesc* __restrict__ td, const Slot* __restrict__ slots,
+             const uint32_t* __restrict__ values, uint32_t first, uint32_t count, int set_log2,
+             uint32_t* __restrict__ cand_ids, uint32_t* __restrict__ cand_anchor,
+             uint32_t* __restrict__ seg_off, uint32_t* __restrict__ seg_cnt,
+             unsigned long long* __restrict__ arena_count, unsigned long long arena_cap,
+             int* __restrict__ status) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int tid = threadIdx.x;
+    const uint32_t ai = blockIdx.x;
+    if (ai >= count) return;
+    const uint32_t a = first + ai;
+    const int h = o.num_maps;
+    const int groups = BLOCK / h;
+    const int setcap = 1 << set_log2;
+    unsigned long long* canon = (unsigned long long*)(smem + CandSmem::canon(r.max_len));
+    unsigned long long* partial = (unsigned long long*)(smem + CandSmem::partial(r.max_len));
+    uint32_t* sseq = (uint32_t*)(smem + CandSmem::seq(r.max_len, groups, h));
+    uint32_t* qoff = (uint32_t*)(smem + CandSmem::qinfo(r.max_len, groups, h, r.seq_pitch));
+    uint32_t* qcnt = qoff + kMaxMaps;
+    uint32_t* qpre = qcnt + kMaxMaps;              // kMaxMaps + 1 entries
+    uint32_t* set = (uint32_t*)(smem + CandSmem::set(r.max_len, groups, h, r.seq_pitch));
+    uint32_t* list = set + setcap;
+    __shared__ uint32_t s_unique;
+    __shared__ unsigned long long s_base;
+
+    const int L = r.len[a];
+    const bool skip = (o.exclude_ambiguous && r.ambig[a]) || L < o.k;
+    if (skip) {
+        if (tid == 0) { seg_off[ai] = 0; seg_cnt[ai] = 0; }
+        return;
+    }
+    // anchor row into shared memory, two zero words of padding for kmer_at
+    const uint32_t* arow = r.seq + (size_t)a * r.seq_pitch;
+    for (int i = tid; i < r.seq_pitch + 2; i += BLOCK) sseq[i] = i < r.seq_pitch ? __ldg(arow + i) : 0u;
+    __syncthreads();
+
+    // canonical k-mers
+    const int npos = L - o.k + 1;
+    const int rcshift = 64 - 2 * o.k;
+    for (int p = tid; p < npos; p += BLOCK) {
+        const unsigned long long fw = kmer_at(sseq, o.k, p);
+        const unsigned long long rv = revcomp64(fw) >> rcshift;
+        canon[p] = fw < rv ? fw : rv;
+    }
+    __syncthreads();
+
+    // per map: min over k-mers of murmur64(kmer + map)
+    {
+        const int m = tid % h, g = tid / h;
+        if (g < groups) {
+            unsigned long long mn = ~0ull;
+            for (int p = g; p < npos; p += groups) {
+                const unsigned long long v = murmur64(canon[p] + (unsigned long long)m);
+                mn = v < mn ? v : mn;
+            }
+            partial[g * h + m] = mn;
+        }
+    }
+    __syncthreads();
+
+    // table lookup (linear probing from murmur64(key))
+    if (tid < h) {
+        unsigned long long key = ~0ull;
+        for (int g = 0; g < groups; ++g) { const unsigned long long v = partial[g * h + tid]; key = v < key ? v : key; }
+        key &= o.kmer_mask;
+        const TableDesc d = td[tid];
+        uint32_t pos = (uint32_t)murmur64(key) & d.mask;
+        uint32_t off = 0, cnt = 0;
+        for (uint32_t probe = 0; probe <= d.mask; ++probe) {
+            const Slot sl = slots[d.slot_base + pos];
+            if (sl.count == 0) break;
+            if (sl.key == key) { off = sl.offset; cnt = sl.count; break; }
+            pos = (pos + 1) & d.mask;
+        }
+        if ((int)cnt > o.threshold) cnt = 0;      // queryMap :443-446
+        qoff[tid] = (uint32_t)d.value_base + off;
+        qcnt[tid] = cnt;
+    }
+    for (int i = tid; i < setcap; i += BLOCK) set[i] = kEmpty;
+    if (tid == 0) s_unique = 0;
+    __syncthreads();
+    if (tid == 0) {
+        uint32_t acc = 0;
+        for (int m = 0; m < h; ++m) { qpre[m] = acc; acc += qcnt[m]; }
+        qpre[h] = acc;
+    }
+    __syncthreads();
+
+    // insert all retrieved ids into the shared hash set
+    const uint32_t T = qpre[h];
+    for (uint32_t e = tid; e < T; e += BLOCK) {
+        int lo = 0, hi = h - 1;                     // map of element e
+        while (lo < hi) { const int mid = (lo + hi + 1) >> 1; if (qpre[mid] <= e) lo = mid; else hi = mid - 1; }
+        const uint32_t id = __ldg(values + qoff[lo] + (e - qpre[lo]));
+        uint32_t pos = (id * 2654435761u) >> (32 - set_log2);
+        for (int probe = 0; probe < setcap; ++probe) {
+            const uint32_t prev = atomicCAS(&set[pos], kEmpty, id);
+            if (prev == kEmpty || prev == id) break;
+            pos = (pos + 1) & (setcap - 1);
+        }
+    }
+    __syncthreads();
+
+    // unique ids minus the anchor itself and (optionally) ambiguous reads
+    for (int i = tid; i < setcap; i += BLOCK) {
+        const uint32_t v = set[i];
+        if (v != kEmpty && v != a && !(o.exclude_ambiguous && r.ambig[v])) list[atomicAdd(&s_unique, 1u)] = v;
+    }
+    __syncthreads();
+    const uint32_t U = s_unique;
+    uint32_t P = 1;
+    while (P < U) P <<= 1;
+    for (uint32_t i = U + tid; i < P; i += BLOCK) list[i] = kEmpty;
+    __syncthreads();
+    // bitonic sort of list[0..P)
+    for (uint32_t kk = 2; kk <= P; kk <<= 1) {
+        for (uint32_t j = kk >> 1; j > 0; j >>= 1) {
+            for (uint32_t i = tid; i < P; i += BLOCK) {
+                const uint32_t ixj = i ^ j;
+                if (ixj > i) {
+                    const uint32_t x = list[i], y = list[ixj];
+                    const bool up = (i & kk) == 0;
+                    if ((x > y) == up) { list[i] = y; list[ixj] = x; }
+                }
+            }
+            __syncthreads();
+        }
+    }
+    if (tid == 0) s_base = atomicAdd(arena_count, (unsigned long long)U);
+    __syncthreads();
+    const unsigned long long base = s_base;
+    if (tid == 0) { seg_off[ai] = (uint32_t)base; seg_cnt[ai] = U; }
+    if (base + U > arena_cap) {
+        if (tid == 0) atomicOr(status, kStatusCandOverflow);
+        return;
+    }
+    for (uint32_t i = tid; i < U; i += BLOCK) { cand_ids[base + i] = list[i]; cand_anchor[base + i] = ai; }
+}
+
+// ---------------------------------------------------------------------------
+// Stage 2: alignment of every (anchor, candidate) pair, both strands.
+//   getCandidateAlignments            include/corrector.hpp:925-979
+//   cpuShiftedHammingDistance...      src/cpu_alignment.cpp:32-323
+//   chooseBestAlignmentOrientation    include/alignmentorientation.hpp:72-92
+//   computePairFlags                  include/corrector.hpp:763-807 (PE)
+// ---------------------------------------------------------------------------
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK)
+k_align(DevOptions o, DevReads r, uint32_t first, const uint32_t* __restrict__ cand_ids,
+        const uint32_t* __restrict__ cand_anchor, const uint32_t* __restrict__ seg_off,
+        const uint32_t* __restrict__ seg_cnt, const unsigned long long* __restrict__ total_ptr,
+        unsigned long long arena_cap, const int* __restrict__ status, AlignRes* __restrict__ out) {
+    // an overflowed candidate arena holds unwritten entries: the batch is
+    // repeated with a larger arena, nothing here may read them
+    if (*status & kStatusCandOverflow) return;
+    const unsigned long long i = (unsigned long long)blockIdx.x * BLOCK + threadIdx.x;
+    const unsigned long long total = *total_ptr;
+    if (total > arena_cap || i >= total) return;
+    constexpr int W = kPlaneWords;
+    const uint32_t ai = cand_anchor[i];
+    const uint32_t a = first + ai;
+    const uint32_t c = cand_ids[i];
+    const int La = r.len[a], Lc = r.len[c];
+    unsigned long long Ahi[W + 1], Alo[W + 1], Chi[W + 1], Clo[W + 1];
+    load_planes<W>(r.seq + (size_t)a * r.seq_pitch, La, Ahi, Alo);
+    load_planes<W>(r.seq + (size_t)c * r.seq_pitch, Lc, Chi, Clo);
+    const int lo = __float2int_rz(__fmul_rn((float)La, o.min_overlap_ratio));
+    const int minov = o.min_overlap > lo ? o.min_overlap : lo;
+    const ShdResult f = shifted_hamming<W>(Ahi, Alo, La, Chi, Clo, Lc, minov, o.max_error_rate);
+    unsigned long long Rhi[W + 1], Rlo[W + 1];
+    revcomp_planes<W>(Chi, Clo, Lc, Rhi, Rlo);
+    const ShdResult rc = shifted_hamming<W>(Ahi, Alo, La, Rhi, Rlo, Lc, minov, o.max_error_rate);
+    const int orient = choose_orientation(f, rc, La, o.min_overlap_ratio, o.min_overlap,
+                                          __fmul_rn(o.estimated_errorrate, 4.0f));
+    AlignRes res;
+    const ShdResult& b = orient == 2 ? rc : f;
+    res.shift = (int16_t)b.shift;
+    res.overlap = (int16_t)b.overlap;
+    res.nops = (int16_t)b.nops;
+    res.orient = (uint8_t)orient;
+    res.paired = 0;
+    if (o.paired_end) {
+        // candidate c is paired iff c's mate is a candidate of the anchor's mate
+        // (equivalent to flagPairedCandidates, include/util.hpp:1016-1197)
+        const uint32_t mi = ai ^ 1u;
+        const uint32_t moff = seg_off[mi], mcnt = seg_cnt[mi];
+        const uint32_t target = c ^ 1u;
+        uint32_t lo2 = 0, hi2 = mcnt;
+        while (lo2 < hi2) {
+            const uint32_t mid = (lo2 + hi2) >> 1;
+            if (cand_ids[moff + mid] < target) lo2 = mid + 1; else hi2 = mid;
+        }
+        res.paired = (lo2 < mcnt && cand_ids[moff + lo2] == target) ? 1 : 0;
+    }
+    out[i] = res;
+}
+
+// ---------------------------------------------------------------------------
+// Stage 3: filters, MSA, refinement, correction.
+//   filterCandidatesByAlignmentFlag / ...MismatchRatio(WithPairFlags)
+//                                     include/corrector.hpp:982-1211
+//   alignmentsComputeWeightsAndAoStoSoA :1260-1280, calculateOverlapWeight
+//                                     include/hostdevicefunctions.cuh:93-97
+//   MultipleSequenceAlignment::build/addSequence/findConsensus/
+//   findOrigWeightAndCoverage         src/msa.cpp:9-173
+//   refineMSA                         include/corrector.hpp:1307-1421
+//   findCandidatesOfDifferentRegion   src/msa.cpp:532-734
+//   getMSAProperties                  src/msa.cpp:304-376
+//   getCorrectedAnchor                src/msa.cpp:379-453
+//   getCorrectedCandidates            src/msa.cpp:457-522
+//   makeOutputOfTask (edits)          include/corrector.hpp:1639-1761
+// Column sums are accumulated by the thread that owns the column, anchor
+// first and then candidates in list order, with separate IEEE multiply and
+// add (no FMA) -- the reference's exact order and rounding.
+// ---------------------------------------------------------------------------
+struct MsaOut {
+    uint8_t* status;
+    int32_t* nedits;
+    char* seq;                        // count * max_len
+    uint32_t* corr_id;
+    uint32_t* corr_anchor;
+    int32_t* corr_shift;
+    uint8_t* corr_use_edits;
+    char* corr_seq;                   // corr_cap * max_len
+    unsigned long long* corr_count;
+    unsigned long long corr_cap;
+};
+
+constexpr int kStage = 32;            // candidates staged in shared memory at a time
+
+template <int BLOCK, int COLS>
+__global__ void __launch_bounds__(BLOCK)
+k_msa(DevOptions o, DevReads r, uint32_t first, uint32_t count, const uint32_t* __restrict__ order,
+      const uint32_t* __restrict__ cand_ids, const uint32_t* __restrict__ seg_off,
+      const uint32_t* __restrict__ seg_cnt, const AlignRes* __restrict__ ares,
+      CandRec* __restrict__ recs, MsaOut out, int* __restrict__ status) {
+    constexpr int MAXCOLS = BLOCK * COLS;
+    constexpr int NW = BLOCK / 32;
+    __shared__ uint8_t s_cons[MAXCOLS];
+    __shared__ float s_support[MAXCOLS];
+    __shared__ uint16_t s_cov[MAXCOLS];
+    __shared__ uint16_t s_cnt[MAXCOLS][4];
+    __shared__ uint32_t s_aseq[kMaxLen / 16 + 2];
+    __shared__ uint32_t s_aqual[kMaxLen / 4 + 2];
+    __shared__ uint32_t s_cseq[kStage][kMaxLen / 16];
+    __shared__ uint32_t s_cqual[kStage][kMaxLen / 4];
+    __shared__ int s_cbeg[kStage], s_clen[kStage];
+    __shared__ float s_cw[kStage];
+    __shared__ int s_cfwd[kStage];
+    __shared__ int s_red[NW][4];
+    __shared__ int s_vals[8];
+    __shared__ float s_fvals[4];
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (blockIdx.x >= count) return;
+    if (*status & kStatusCandOverflow) return;   // batch is repeated with a larger arena
+    const uint32_t ai = order ? order[blockIdx.x] : blockIdx.x;
+    const uint32_t a = first + ai;
+    const uint32_t off = seg_off[ai], cnt = seg_cnt[ai];
+    const int La = r.len[a];
+    const int mlen = r.max_len;
+    const bool useQ = o.use_quality && r.qual != nullptr;
+    char* aout = out.seq + (size_t)ai * mlen;
+
+    if (cnt == 0) {
+        if (tid == 0) { out.status[ai] = 0; out.nedits[ai] = 0; }
+        return;
+    }
+
+    auto block_sum4 = [&](int v0, int v1, int v2, int v3, int* res) {
+#pragma unroll
+        for (int d = 16; d > 0; d >>= 1) {
+            v0 += __shfl_xor_sync(0xffffffffu, v0, d);
+            v1 += __shfl_xor_sync(0xffffffffu, v1, d);
+            v2 += __shfl_xor_sync(0xffffffffu, v2, d);
+            v3 += __shfl_xor_sync(0xffffffffu, v3, d);
+        }
+        __syncthreads();
+        if (lane == 0) { s_red[warp][0] = v0; s_red[warp][1] = v1; s_red[warp][2] = v2; s_red[warp][3] = v3; }
+        __syncthreads();
+        int t0 = 0, t1 = 0, t2 = 0, t3 = 0;
+#pragma unroll
+        for (int w = 0; w < NW; ++w) { t0 += s_red[w][0]; t1 += s_red[w][1]; t2 += s_red[w][2]; t3 += s_red[w][3]; }
+        res[0] = t0; res[1] = t1; res[2] = t2; res[3] = t3;
+    };
+    // block-wide exclusive scan of one flag per thread; returns the prefix, *tot the sum
+    auto block_scan = [&](int v, int* tot) {
+        int x = v;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, x, d);
+            if (lane >= d) x += y;
+        }
+        __syncthreads();
+        if (lane == 31) s_red[warp][0] = x;
+        __syncthreads();
+        int pre = 0, all = 0;
+#pragma unroll
+        for (int w = 0; w < NW; ++w) { const int s = s_red[w][0]; if (w < warp) pre += s; all += s; }
+        *tot = all;
+        return pre + x - v;
+    };
+
+    // ---- alignment filters (corrector.hpp:982-1211), ordered compaction ----
+    const float base = __fmul_rn(o.estimated_errorrate, 1.0f);
+    int c0 = 0, c1 = 0, c2 = 0, n1 = 0;
+    for (uint32_t i = tid; i < cnt; i += BLOCK) {
+        const AlignRes ar = ares[off + i];
+        if (ar.orient != 3) {
+            n1++;
+            const float mr = __fdiv_rn((float)ar.nops, (float)ar.overlap);
+            c0 += mr < __fmul_rn(2.0f, base);
+            c1 += mr < __fmul_rn(3.0f, base);
+            c2 += mr < __fmul_rn(4.0f, base);
+        }
+    }
+    int red[4];
+    block_sum4(c0, c1, c2, n1, red);
+    if (red[3] == 0) {
+        if (tid == 0) { out.status[ai] = 0; out.nedits[ai] = 0; }
+        return;
+    }
+    float thr = -3.402823466e+38f;
+    {
+        const float good = __fmul_rn(o.estimated_coverage, o.m_coverage);
+        if (red[0] > 0 || red[1] > 0 || red[2] > 0) {
+            if ((float)red[0] >= good) thr = __fmul_rn(2.0f, base);
+            else if ((float)red[1] >= good) thr = __fmul_rn(3.0f, base);
+            else if ((float)red[2] >= good) thr = __fmul_rn(4.0f, base);
+        }
+    }
+    int V = 0;
+    for (uint32_t c = 0; c < cnt; c += BLOCK) {
+        const uint32_t i = c + tid;
+        int keep = 0;
+        AlignRes ar;
+        if (i < cnt) {
+            ar = ares[off + i];
+            if (ar.orient != 3) {
+                const float mr = __fdiv_rn((float)ar.nops, (float)ar.overlap);
+                keep = o.paired_end ? (ar.paired || mr < o.paired_filter_threshold) : (mr < thr);
+            }
+        }
+        int tot;
+        const int pre = block_scan(keep, &tot);
+        if (keep) {
+            CandRec rec;
+            rec.id = cand_ids[off + i];
+            rec.shift = ar.shift;
+            rec.len = (uint16_t)r.len[rec.id];
+            // calculateOverlapWeight: 1 - sqrtf(nOps / (overlap * maxMismatchRatio))
+            rec.weight = __fsub_rn(1.0f, __fsqrt_rn(__fdiv_rn((float)ar.nops,
+                                                          __fmul_rn((float)ar.overlap, o.max_error_rate))));
+            rec.orient = ar.orient;
+            recs[off + V + pre] = rec;
+        }
+        V += tot;
+    }
+    if (V == 0) {
+        if (tid == 0) { out.status[ai] = 0; out.nedits[ai] = 0; }
+        return;
+    }
+    __syncthreads();
+
+    // ---- anchor row and qualities ----
+    for (int i = tid; i < r.seq_pitch; i += BLOCK) s_aseq[i] = __ldg(r.seq + (size_t)a * r.seq_pitch + i);
+    if (useQ) for (int i = tid; i < r.qual_pitch; i += BLOCK) s_aqual[i] = __ldg(r.qual + (size_t)a * r.qual_pitch + i);
+    __syncthreads();
+
+    const int qbits = o.quality_bits;
+    auto qual_weight = [&](const uint32_t* row, int p) -> float {
+        uint32_t ch;
+        if (qbits == 8) ch = (row[p >> 2] >> (8 * (p & 3))) & 0xFFu;
+        else if (qbits == 2) {
+            const uint32_t b = (row[p >> 4] >> (30 - 2 * (p & 15))) & 3u;
+            ch = b == 0 ? '$' : b == 1 ? '(' : b == 2 ? '1' : '9';
+        } else {
+            const uint32_t b = (row[p >> 5] >> (31 - (p & 31))) & 1u;
+            ch = b == 0 ? '(' : '5';
+        }
+        return c_qweight[ch];
+    };
+
+    int abegin = 0, aend = 0, ncols = 0;
+    bool allGood = false, hq = false;
+
+    for (int iter = 0;; ++iter) {
+        // ---- MSA geometry ----
+        int mn = 0, mx = La;
+        for (int k = tid; k < V; k += BLOCK) {
+            const CandRec rc = recs[off + k];
+            mn = min(mn, (int)rc.shift);
+            mx = max(mx, (int)rc.shift + (int)rc.len);
+        }
+#pragma unroll
+        for (int d = 16; d > 0; d >>= 1) {
+            mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, d));
+            mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, d));
+        }
+        __syncthreads();
+        if (lane == 0) { s_red[warp][0] = mn; s_red[warp][1] = mx; }
+        __syncthreads();
+        mn = 0; mx = La;
+        for (int w = 0; w < NW; ++w) { mn = min(mn, s_red[w][0]); mx = max(mx, s_red[w][1]); }
+        ncols = mx - mn;
+        abegin = -mn;
+        aend = abegin + La;
+        if (ncols > MAXCOLS) {
+            if (tid == 0) { atomicOr(status, kStatusColumns); out.status[ai] = 0; out.nedits[ai] = 0; }
+            return;
+        }
+
+        // ---- column accumulation: anchor, then candidates in order ----
+        int cA[COLS], cC[COLS], cG[COLS], cT[COLS];
+        float wA[COLS], wC[COLS], wG[COLS], wT[COLS];
+#pragma unroll
+        for (int j = 0; j < COLS; ++j) {
+            cA[j] = cC[j] = cG[j] = cT[j] = 0;
+            wA[j] = wC[j] = wG[j] = wT[j] = 0.0f;
+            const int col = tid + j * BLOCK;
+            if (col >= abegin && col < aend) {
+                const int p = col - abegin;
+                const uint32_t b = base_at(s_aseq, p);
+                const float w = useQ ? __fmul_rn(1.0f, qual_weight(s_aqual, p)) : 1.0f;
+                if (b == 0) { cA[j] = 1; wA[j] = w; } else if (b == 1) { cC[j] = 1; wC[j] = w; }
+                else if (b == 2) { cG[j] = 1; wG[j] = w; } else { cT[j] = 1; wT[j] = w; }
+            }
+        }
+        for (int c = 0; c < V; c += kStage) {
+            const int nst = min(kStage, V - c);
+            __syncthreads();
+            // stage rows of nst candidates
+            const int sp = r.seq_pitch, qp = r.qual_pitch;
+            for (int e = tid; e < nst * sp; e += BLOCK) {
+                const int k = e / sp, w = e - k * sp;
+                s_cseq[k][w] = __ldg(r.seq + (size_t)recs[off + c + k].id * sp + w);
+            }
+            if (useQ)
+                for (int e = tid; e < nst * qp; e += BLOCK) {
+                    const int k = e / qp, w = e - k * qp;
+                    s_cqual[k][w] = __ldg(r.qual + (size_t)recs[off + c + k].id * qp + w);
+                }
+            if (tid < nst) {
+                const CandRec rc = recs[off + c + tid];
+                s_cbeg[tid] = abegin + rc.shift;
+                s_clen[tid] = rc.len;
+                s_cw[tid] = rc.weight;
+                s_cfwd[tid] = rc.orient == 1;
+            }
+            __syncthreads();
+            for (int k = 0; k < nst; ++k) {
+                const int cb = s_cbeg[k], cl = s_clen[k];
+                const float fw = s_cw[k];
+                const bool fwd = s_cfwd[k];
+#pragma unroll
+                for (int j = 0; j < COLS; ++j) {
+                    const int col = tid + j * BLOCK;
+                    const int p = col - cb;
+                    if (p >= 0 && p < cl) {
+                        uint32_t b = fwd ? base_at(s_cseq[k], p) : (base_at(s_cseq[k], cl - 1 - p) ^ 3u);
+                        // reverse-complement candidates read their qualities
+                        // reversed over the whole quality pitch
+                        // (reverseQualitiesOfRCAlignments, corrector.hpp:1227-1239)
+                        const float w = useQ ? __fmul_rn(fw, qual_weight(s_cqual[k], fwd ? p : mlen - 1 - p))
+                                             : __fmul_rn(fw, 1.0f);
+                        if (b == 0) { cA[j]++; wA[j] = __fadd_rn(wA[j], w); }
+                        else if (b == 1) { cC[j]++; wC[j] = __fadd_rn(wC[j], w); }
+                        else if (b == 2) { cG[j]++; wG[j] = __fadd_rn(wG[j], w); }
+                        else { cT[j]++; wT[j] = __fadd_rn(wT[j], w); }
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        // ---- consensus and support (findConsensus) ----
+#pragma unroll
+        for (int j = 0; j < COLS; ++j) {
+            const int col = tid + j * BLOCK;
+            if (col < ncols) {
+                uint8_t cs = 0; float cw = wA[j];
+                if (wC[j] > cw) { cs = 1; cw = wC[j]; }
+                if (wG[j] > cw) { cs = 2; cw = wG[j]; }
+                if (wT[j] > cw) { cs = 3; cw = wT[j]; }
+                const float colw = __fadd_rn(__fadd_rn(__fadd_rn(wA[j], wC[j]), wG[j]), wT[j]);
+                s_cons[col] = cs;
+                s_support[col] = __fdiv_rn(cw, colw);
+                s_cov[col] = (uint16_t)(cA[j] + cC[j] + cG[j] + cT[j]);
+                s_cnt[col][0] = (uint16_t)cA[j]; s_cnt[col][1] = (uint16_t)cC[j];
+                s_cnt[col][2] = (uint16_t)cG[j]; s_cnt[col][3] = (uint16_t)cT[j];
+            }
+        }
+        __syncthreads();
+
+        if (iter >= 5) break;
+        // ---- refinement: findCandidatesOfDifferentRegion ----
+        if (tid == 0) { s_vals[0] = 0; s_vals[1] = 0x7fffffff; s_vals[2] = 0; s_vals[3] = 0; }
+        __syncthreads();
+        int mism = 0;
+        for (int p = tid; p < La; p += BLOCK) mism |= base_at(s_aseq, p) != s_cons[abegin + p];
+        if (__syncthreads_or(mism) == 0) break;
+        const int sigThr = __float2int_rz(__fmul_rn((float)o.coverage_int, 0.3f));
+        for (int p = tid; p < La; p += BLOCK) {
+            const int col = abegin + p;
+            const int cs = s_cons[col];
+            int sig = -1;
+#pragma unroll
+            for (int b = 0; b < 4; ++b) if (b != cs && sigThr <= (int)s_cnt[col][b]) sig = b;
+            if (sig >= 0) atomicMin(&s_vals[1], col);
+        }
+        __syncthreads();
+        const int col = s_vals[1];
+        if (col == 0x7fffffff) break;
+        int foundBase = -1;
+        {
+            const int cs = s_cons[col];
+            for (int b = 0; b < 4; ++b) if (b != cs && sigThr <= (int)s_cnt[col][b]) foundBase = b;
+        }
+        const int orig = base_at(s_aseq, col - abegin);
+        const bool keepMatching = orig == foundBase;
+        int nrem = 0, veto = 0;
+        for (int k = tid; k < V; k += BLOCK) {
+            const CandRec rc = recs[off + k];
+            const int rb = abegin + rc.shift, re = rb + rc.len;
+            int rem = 0;
+            if (!(col < rb || re <= col)) {
+                const int p = col - rb;
+                const uint32_t* row = r.seq + (size_t)rc.id * r.seq_pitch;
+                const int b = rc.orient == 1 ? (int)base_at(row, p) : (int)(base_at(row, rc.len - 1 - p) ^ 3u);
+                rem = keepMatching ? (b != foundBase) : (b == foundBase);
+            }
+            nrem += rem;
+            veto |= rem && rc.weight >= 0.90f;
+        }
+        const int anyVeto = __syncthreads_or(veto);
+        const int anyRem = __syncthreads_or(nrem);
+        if (anyVeto || !anyRem) break;
+        // ordered compaction of the survivors (recs read before rewrite)
+        int newV = 0;
+        for (int c = 0; c < V; c += BLOCK) {
+            const int k = c + tid;
+            CandRec rc;
+            int keep = 0;
+            if (k < V) {
+                rc = recs[off + k];
+                const int rb = abegin + rc.shift, re = rb + rc.len;
+                keep = 1;
+                if (!(col < rb || re <= col)) {
+                    const int p = col - rb;
+                    const uint32_t* row = r.seq + (size_t)rc.id * r.seq_pitch;
+                    const int b = rc.orient == 1 ? (int)base_at(row, p) : (int)(base_at(row, rc.len - 1 - p) ^ 3u);
+                    keep = !(keepMatching ? (b != foundBase) : (b == foundBase));
+                }
+            }
+            int tot;
+            const int pre = block_scan(keep, &tot);
+            __syncthreads();
+            if (keep) recs[off + newV + pre] = rc;
+            newV += tot;
+            __syncthreads();
+        }
+        V = newV;
+        __syncthreads();
+    }
+
+    // ---- MSA properties (getMSAProperties) ----
+    {
+        float mnS = 3.402823466e+38f;
+        int mnC = 0x7fffffff;
+        for (int p = tid; p < La; p += BLOCK) {
+            mnS = fminf(mnS, s_support[abegin + p]);
+            mnC = min(mnC, (int)s_cov[abegin + p]);
+        }
+#pragma unroll
+        for (int d = 16; d > 0; d >>= 1) {
+            mnS = fminf(mnS, __shfl_xor_sync(0xffffffffu, mnS, d));
+            mnC = min(mnC, __shfl_xor_sync(0xffffffffu, mnC, d));
+        }
+        __syncthreads();
+        if (lane == 0) { s_red[warp][0] = __float_as_int(mnS); s_red[warp][1] = mnC; }
+        __syncthreads();
+        if (tid == 0) {
+            float minSup = 3.402823466e+38f;
+            int minCov = 0x7fffffff;
+            for (int w = 0; w < NW; ++w) { minSup = fminf(minSup, __int_as_float(s_red[w][0])); minCov = min(minCov, s_red[w][1]); }
+            float sum = 0.0f;
+            for (int p = 0; p < La; ++p) sum = __fadd_rn(sum, s_support[abegin + p]);
+            const float avgSup = __fdiv_rn(sum, (float)La);
+            const float e = o.estimated_errorrate;
+            const float avgThr = __fsub_rn(1.0f, __fmul_rn(1.0f, e));
+            const float minThr = __fsub_rn(1.0f, __fmul_rn(3.0f, e));
+            const float covThr = __fmul_rn(__fdiv_rn(o.m_coverage, 6.0f), o.estimated_coverage);
+            const bool good = fgeq(avgSup, avgThr) && fgeq(minSup, minThr) && fgeq((float)minCov, covThr);
+            bool isHQ = false;
+            if (good) {
+                int smallest = 100;
+                const int pct = (int)ceilf(__fmul_rn(e, 100.0f));
+                for (int pc = pct; pc >= 0; --pc) {
+                    const float fac = __fdiv_rn((float)pc, 100.0f);
+                    const float at = __fsub_rn(1.0f, __fmul_rn(1.0f, fac));
+                    const float mt = __fsub_rn(1.0f, __fmul_rn(3.0f, fac));
+                    if (fgeq(avgSup, at) && fgeq(minSup, mt)) smallest = pc;
+                }
+                isHQ = fgeq((float)minCov, covThr) && fleq((float)smallest, __fmul_rn((float)pct, 0.5f));
+            }
+            s_vals[4] = good;
+            s_vals[5] = isHQ;
+        }
+        __syncthreads();
+        allGood = s_vals[4];
+        hq = s_vals[5];
+    }
+
+    // ---- anchor correction (getCorrectedAnchor) ----
+    if (V == 0) {
+        if (tid == 0) { out.status[ai] = 0; out.nedits[ai] = 0; }
+        return;   // nCandidates == 0: not corrected; no candidate corrections either
+    }
+    int diffs = 0;
+    for (int p = tid; p < La; p += BLOCK) {
+        const int col = abegin + p;
+        const uint32_t ob = base_at(s_aseq, p);
+        uint32_t cb;
+        if (allGood) cb = s_cons[col];
+        else {
+            const int oc = s_cnt[col][ob];    // origCoverages: count of the anchor's base
+            cb = (s_support[col] > 0.90f && oc <= 2) ? s_cons[col] : ob;
+        }
+        aout[p] = "ACGT"[cb];
+        diffs += cb != ob;
+    }
+    int rr[4];
+    block_sum4(diffs, 0, 0, 0, rr);
+    if (tid == 0) {
+        const int nd = rr[0];
+        const bool useEdits = !r.ambig[a] && nd <= La / 7;
+        out.status[ai] = (uint8_t)(1 | (hq ? 2 : 0) | (useEdits ? 4 : 0));
+        out.nedits[ai] = useEdits ? nd : 0;
+    }
+
+    // ---- candidate correction (getCorrectedCandidates) ----
+    if (hq && o.correct_candidates) {
+        const int ncc = o.new_columns;
+        for (int k = tid; k < V; k += BLOCK) {
+            const CandRec rc = recs[off + k];
+            const int qb = abegin + rc.shift;
+            const int qe = qb + rc.len;
+            if (!(abegin - ncc <= qb && qb <= abegin + ncc && qe <= aend + ncc)) continue;
+            const unsigned long long slot = atomicAdd(out.corr_count, 1ull);
+            if (slot >= out.corr_cap) { atomicOr(status, kStatusCorrOverflow); continue; }
+            char* dst = out.corr_seq + slot * mlen;
+            const uint32_t* row = r.seq + (size_t)rc.id * r.seq_pitch;
+            int nd = 0;
+            const int L = rc.len;
+            for (int p = 0; p < L; ++p) {
+                // forward orientation of the corrected candidate
+                if (rc.orient == 1) {
+                    const uint32_t cs = s_cons[qb + p];
+                    dst[p] = "ACGT"[cs];
+                    nd += cs != base_at(row, p);
+                } else {
+                    const uint32_t cs = s_cons[qb + L - 1 - p] ^ 3u;
+                    dst[p] = "ACGT"[cs];
+                    nd += cs != base_at(row, p);
+                }
+            }
+            out.corr_id[slot] = rc.id;
+            out.corr_anchor[slot] = a;
+            out.corr_shift[slot] = rc.shift;
+            out.corr_use_edits[slot] = (!r.ambig[rc.id] && nd <= L / 7) ? 1 : 0;
+        }
+    }
+}
+
+// Signatures of all reads (for table construction): one warp per read.
+__global__ void k_signatures(DevOptions o, DevReads r, uint32_t first, uint32_t count,
+                             unsigned long long* __restrict__ sig) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t ri = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+    if (ri >= count) return;
+    const uint32_t id = first + ri;
+    const int L = r.len[id];
+    const int h = o.num_maps;
+    const uint32_t* row = r.seq + (size_t)id * r.seq_pitch;
+    unsigned long long mine[2] = {~0ull, ~0ull};  // maps lane and lane+32
+    if (L >= o.k) {
+        const int npos = L - o.k + 1;
+        const int rcshift = 64 - 2 * o.k;
+        for (int p0 = 0; p0 < npos; p0 += 32) {
+            // each lane builds one canonical k-mer, then all lanes hash all 32
+            unsigned long long cn = 0;
+            const int p = p0 + lane;
+            if (p < npos) {
+                const int w = p >> 4, of = p & 15;
+                const uint32_t s0 = __ldg(row + w);
+                const uint32_t s1 = (w + 1 < r.seq_pitch) ? __ldg(row + w + 1) : 0u;
+                const uint32_t s2 = (w + 2 < r.seq_pitch) ? __ldg(row + w + 2) : 0u;
+                const unsigned long long hi = ((unsigned long long)s0 << 32) | s1;
+                const unsigned long long top = of ? (hi << (2 * of)) | ((unsigned long long)s2 >> (32 - 2 * of)) : hi;
+                const unsigned long long fw = top >> (64 - 2 * o.k);
+                const unsigned long long rv = revcomp64(fw) >> rcshift;
+                cn = fw < rv ? fw : rv;
+            }
+            const int nv = min(32, npos - p0);
+            for (int q = 0; q < nv; ++q) {
+                const unsigned long long km = __shfl_sync(0xffffffffu, cn, q);
+                if (lane < h) { const unsigned long long v = murmur64(km + lane); mine[0] = v < mine[0] ? v : mine[0]; }
+                if (lane + 32 < h) { const unsigned long long v = murmur64(km + lane + 32); mine[1] = v < mine[1] ? v : mine[1]; }
+            }
+        }
+    }
+    if (lane < h) sig[(size_t)ri * h + lane] = mine[0] & o.kmer_mask;
+    if (lane + 32 < h) sig[(size_t)ri * h + lane + 32] = mine[1] & o.kmer_mask;
+}
+
+}  // namespace careb200

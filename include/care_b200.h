@@ -1,0 +1,169 @@
+/*
+ * care_b200.h -- C ABI of the B200 (sm_100a) read-correction library.
+ *
+ * This is the drop-in boundary for CARE's per-anchor correction path
+ * (yanlifeng/CARE). Each entry point names the reference interface it
+ * replaces. All functions return 0 on success and a negative
+ * CARE_B200_E* code on failure; care_b200_last_error() returns a message.
+ * No exception crosses this boundary. One context per host thread; calls on
+ * one context are serial. The caller owns every host array it passes in;
+ * the context owns all device memory and the result buffers it returns.
+ */
+#ifndef CARE_B200_H
+#define CARE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CARE_B200_OK            0
+#define CARE_B200_EINVAL       -1   /* invalid argument / option */
+#define CARE_B200_ECUDA        -2   /* CUDA runtime error */
+#define CARE_B200_ENOMEM       -3   /* device or host allocation failed */
+#define CARE_B200_ESTATE       -4   /* call out of order (e.g. no reads uploaded) */
+#define CARE_B200_EIO          -5   /* file read / write error */
+#define CARE_B200_ELIMIT       -6   /* input beyond a documented limit */
+
+/* The ProgramOptions fields read on the correction path
+ * (include/options.hpp:36-123 of the reference; defaults :37-98). */
+typedef struct care_b200_options {
+    int   kmerlength;               /* -k, default 20 */
+    int   num_maps;                 /* -h, default 48 (<= 48) */
+    int   min_overlap;              /* --minalignmentoverlap, 30 */
+    float max_error_rate;           /* --maxmismatchratio, 0.2 */
+    float min_overlap_ratio;        /* --minalignmentoverlapratio, 0.30 */
+    float estimated_errorrate;      /* --errorfactortuning, 0.06 */
+    float estimated_coverage;       /* -c, mandatory */
+    float m_coverage;               /* --coveragefactortuning, 0.6 */
+    float paired_filter_threshold;  /* --pairedFilterThreshold, 0.06 */
+    int   new_columns_to_correct;   /* --candidateCorrectionNewColumns, 15 */
+    int   use_quality;              /* -q */
+    int   quality_bits;             /* --qualityScoreBits: 1, 2 or 8 */
+    int   exclude_ambiguous;        /* --excludeAmbiguous */
+    int   correct_candidates;       /* --candidateCorrection */
+    int   paired_end;               /* --pairmode PE */
+    int   correction_type;          /* 0 classic consensus rule, 1 learned (MLP) */
+    int   quality_labels;           /* --correctionQualityLabels */
+    int   threads;                  /* host threads for STEP1/STEP3 helpers */
+    int   device;                   /* CUDA device ordinal */
+    int   batch_size;               /* anchors per device batch, 0 = automatic */
+} care_b200_options;
+
+typedef struct care_b200_ctx care_b200_ctx;
+
+/* Result view of the last correction call. Buffers are owned by the context
+ * and stay valid until the next correction call or care_b200_destroy().
+ * anchor_status bits: 1 = corrected, 2 = high quality (HQ) MSA,
+ * 4 = store as edit list (the reference's useEdits, corrector.hpp:1648-1675).
+ * Candidate corrections are in forward read orientation
+ * (corrector.hpp:1679-1757). Sequences are max_length bytes per row. */
+typedef struct care_b200_results {
+    uint32_t        first_anchor;
+    uint32_t        num_anchors;
+    int32_t         max_length;
+    const uint8_t*  anchor_status;
+    const int32_t*  anchor_num_edits;
+    const char*     anchor_sequences;
+    uint64_t        num_candidates;
+    const uint32_t* cand_read_ids;
+    const uint32_t* cand_anchor_ids;
+    const int32_t*  cand_shifts;
+    const uint8_t*  cand_use_edits;
+    const char*     cand_sequences;
+} care_b200_results;
+
+void        care_b200_default_options(care_b200_options* opt);
+
+/* Creates a context on opt->device. Replaces the CpuErrorCorrector
+ * constructor (include/corrector.hpp:118-139): options, pitches and handles
+ * are bound once; the read storage and minhasher follow by upload/build. */
+int         care_b200_create(const care_b200_options* opt, care_b200_ctx** ctx);
+int         care_b200_destroy(care_b200_ctx* ctx);
+const char* care_b200_last_error(const care_b200_ctx* ctx);
+
+/* Read-storage handle: replaces CpuReadStorage (include/cpureadstorage.hpp:
+ * 11-84, gathers chunkedreadstorage.hpp:403-607). packed: num_reads rows of
+ * pitch_ints uint32, 2-bit MSB-first (A=0,C=1,G=2,T=3, sequencehelpers.hpp:
+ * 152-187); enc_quals: num_reads rows of qual_pitch_ints uint32 in the
+ * reference's qualityScoreBits encoding (qualityscorecompression.hpp:90-119),
+ * or NULL; ambiguous_ids: reads that contained non-ACGT bases. Data is
+ * copied into HBM once. Read length limit: 256 bases. Re-uploading the same
+ * number of reads keeps the tables (they index reads by id); a different
+ * number drops them. */
+int care_b200_upload_reads(care_b200_ctx* ctx, const uint32_t* packed, size_t pitch_ints,
+                           const int32_t* lengths, const uint32_t* enc_quals,
+                           size_t qual_pitch_ints, const uint32_t* ambiguous_ids,
+                           size_t num_ambiguous, uint32_t num_reads);
+
+/* Minhasher handle, host-built tables: replaces OrdinaryCpuMinhasher's
+ * tables (ordinaryminhasher.hpp:98-221; content groupbykey.hpp:99-249).
+ * For map m: keys[m][0..nkeys[m]) ascending, values of key i are
+ * values[m][offsets[m][i] .. offsets[m][i+1]) ascending read ids. */
+int care_b200_upload_tables(care_b200_ctx* ctx, int num_maps, const uint64_t* const* keys,
+                            const uint32_t* const* offsets, const uint32_t* const* values,
+                            const size_t* nkeys);
+
+/* Builds the minhash tables from the uploaded reads: signatures on the GPU,
+ * grouping with the reference's bucket rules (size < 2 or > threshold
+ * cleared). Replaces constructCpuMinhasherFromReadStorage
+ * (src/cpuminhasherconstruction.cpp:27-165). */
+int care_b200_build_tables(care_b200_ctx* ctx);
+
+/* Copies the device tables back in the upload_tables layout (for
+ * inspection and tests). Arrays are owned by the context. */
+int care_b200_get_table(care_b200_ctx* ctx, int map, const uint64_t** keys,
+                        const uint32_t** offsets, const uint32_t** values, size_t* nkeys);
+
+/* The hot path: corrects anchors [first_anchor, first_anchor+num_anchors).
+ * Replaces CpuErrorCorrector::process / processMulti
+ * (include/corrector.hpp:145-312, :325-513) over the correct_cpu loop
+ * (src/correct_cpu.cpp:134-301). Paired-end ranges must be pair aligned
+ * (even first and count, corrector.hpp:328). */
+int care_b200_correct_range(care_b200_ctx* ctx, uint32_t first_anchor, uint32_t num_anchors,
+                            care_b200_results* results);
+
+/* Same work without the device->host copy of results: the results stay in
+ * HBM (used to time the device pipeline alone). */
+int care_b200_correct_range_device(care_b200_ctx* ctx, uint32_t first_anchor,
+                                   uint32_t num_anchors);
+
+/* Serialises the results as the reference's EncodedTempCorrectedSequence
+ * byte records (correctedsequence.hpp:148-340: readId u32, flags u32 with
+ * bit31 hq, bit30 useEdits, bit29 type, low 29 bits payload size, payload),
+ * applying the save filter of src/correct_cpu.cpp:255-273. With out == NULL
+ * only *needed is set. */
+int care_b200_serialize_results(care_b200_ctx* ctx, const care_b200_results* results,
+                                uint8_t* out, size_t capacity, size_t* needed);
+
+/* ---- whole-file driver (STEP1 + STEP2 + STEP3 of care-cpu,
+ *      src/dispatch_care_correct_cpu.cpp:51-251) ---- */
+
+/* Parses FASTQ/FASTA (one file, or two files of mates for PE), applies the
+ * reference's read preprocessing (chunkedreadstorageconstruction.hpp:67-92)
+ * and uploads the read storage. */
+int care_b200_load_reads_from_files(care_b200_ctx* ctx, const char* const* files, int num_files);
+
+/* Merges all corrections of the last full-range call with the input reads
+ * and writes the output file (correctionresultoutput.cpp:30-440, 730-1020). */
+int care_b200_write_output(care_b200_ctx* ctx, const char* outfile);
+
+/* Statistics of the last correction call: device milliseconds of the
+ * pipeline and per-stage kernel times (signature+query, alignment, MSA). */
+int care_b200_last_timing(const care_b200_ctx* ctx, float* total_ms, float* stage_ms, int nstages);
+
+/* Counters of the last correction call: stats[0] anchors, stats[1]
+ * (anchor, candidate) pairs aligned, stats[2] candidate corrections. */
+int care_b200_last_stats(const care_b200_ctx* ctx, uint64_t* stats, int nstats);
+
+/* Read-storage facts after upload. */
+uint32_t care_b200_num_reads(const care_b200_ctx* ctx);
+int      care_b200_max_length(const care_b200_ctx* ctx);
+int      care_b200_num_maps(const care_b200_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

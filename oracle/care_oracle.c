@@ -1278,6 +1278,23 @@ int co_write_output(const co_reads* r, const co_results* res, const co_opts* o, 
     char* m0 = xmalloc((size_t)dp + 1);
     char* m1 = xmalloc((size_t)dp + 1);
     char* outseq = xmalloc((size_t)dp + 1);
+    /* mergeSerializedResultsWithOriginalReads_multithreaded (:30-440) calls the
+     * combiner -- and appends a quality label -- only for reads up to the last
+     * read id that has a stored result; later reads are copied unchanged.
+     * Stored: anchor results passing the save filter, and candidate results
+     * for reads that are not HQ anchors (a candidate result for an HQ anchor is
+     * dropped once that anchor's flag is set, corrector.hpp:1682-1684). */
+    int64_t last = -1;
+    for (uint32_t k = 0; k < res->count; k++) {
+        const co_anchor_result* A = &res->anchors[k];
+        if (A->status == 1 && !(A->hq && A->use_edits && A->num_edits == 0)) last = (int64_t)(res->first + k) > last ? (int64_t)(res->first + k) : last;
+    }
+    for (size_t k = 0; k < nc; k++) {
+        const uint32_t id = res->cands[k].read_id;
+        const int hqAnchor = id >= res->first && id < res->first + res->count &&
+                             res->anchors[id - res->first].status == 1 && res->anchors[id - res->first].hq;
+        if (!hqAnchor && (int64_t)id > last) last = id;
+    }
     size_t ci = 0;
     for (uint32_t i = 0; i < r->n; i++) {
         const char* h = r->text + r->rec_off[i];
@@ -1320,7 +1337,7 @@ int co_write_output(const co_reads* r, const co_results* res, const co_opts* o, 
         }
         fputc(r->fasta ? '>' : '@', fp);
         fputs(h, fp);
-        if (o->quality_labels) fprintf(fp, " care:q=%d", corrected ? label : 0);
+        if (o->quality_labels && (int64_t)i <= last) fprintf(fp, " care:q=%d", corrected ? label : 0);
         fputc('\n', fp);
         fwrite(outseq, 1, (size_t)L, fp);
         fputc('\n', fp);

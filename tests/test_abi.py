@@ -1,0 +1,47 @@
+"""The C-ABI library loads and exports every entry point include/care_b200.h
+declares (no compute without a GPU)."""
+import os
+import re
+import subprocess
+
+import care_b200
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared():
+    text = open(os.path.join(ROOT, "include", "care_b200.h")).read()
+    return sorted(set(re.findall(r"\b(care_b200_\w+)\s*\(", text)))
+
+
+def test_header_matches_python_binding():
+    assert declared() == sorted(care_b200.EXPORTS)
+
+
+def test_library_exports_every_declared_symbol():
+    lib = care_b200.load_library()
+    for name in declared():
+        assert hasattr(lib, name), name
+    out = subprocess.run(["nm", "-D", "--defined-only", care_b200.LIB_PATH], capture_output=True, text=True).stdout
+    exported = set(re.findall(r" T (care_b200_\w+)", out))
+    assert set(declared()) <= exported
+
+
+def test_default_options_match_reference_defaults():
+    o = care_b200.default_options()
+    assert (o.kmerlength, o.num_maps, o.min_overlap, o.new_columns_to_correct, o.quality_bits) == (20, 48, 30, 15, 8)
+    assert abs(o.max_error_rate - 0.2) < 1e-7 and abs(o.min_overlap_ratio - 0.3) < 1e-7
+    assert abs(o.estimated_errorrate - 0.06) < 1e-7 and abs(o.m_coverage - 0.6) < 1e-7
+    assert abs(o.paired_filter_threshold - 0.06) < 1e-7
+
+
+def test_create_without_gpu_fails_cleanly():
+    import torch
+    if torch.cuda.is_available():
+        return
+    try:
+        care_b200.Corrector(estimated_coverage=30.0)
+    except care_b200.CareError as e:
+        assert "create" in str(e)
+    else:
+        raise AssertionError("context creation must fail loudly without a GPU")
