@@ -461,6 +461,8 @@ int run_batch(care_b200_ctx* ctx, uint32_t first, uint32_t count, bool timed) {
         int* status = ctx->d_status.as<int>();
         CK(cudaMemsetAsync(counters, 0, 64, ctx->stream), "memset");
         CK(cudaMemsetAsync(status, 0, 16, ctx->stream), "memset");
+        // rows of anchors that are not corrected read as zero bytes
+        CK(cudaMemsetAsync(ctx->d_oseq.p, 0, (size_t)count * ctx->max_len, ctx->stream), "memset");
         if (timed) CK(cudaEventRecord(ctx->ev[0], ctx->stream), "event");
         k_candidates<kCandBlock><<<count, kCandBlock, cand_smem, ctx->stream>>>(
             o, r, ctx->d_tdesc.as<TableDesc>(), ctx->d_slots.as<Slot>(), ctx->d_values.as<uint32_t>(), first,
@@ -469,10 +471,18 @@ int run_batch(care_b200_ctx* ctx, uint32_t first, uint32_t count, bool timed) {
         CK(cudaGetLastError(), "k_candidates");
         if (timed) CK(cudaEventRecord(ctx->ev[1], ctx->stream), "event");
         const unsigned long long ablocks = (cap + kAlignBlock - 1) / kAlignBlock;
-        k_align<kAlignBlock><<<(unsigned)ablocks, kAlignBlock, 0, ctx->stream>>>(
-            o, r, first, ctx->d_cand_ids.as<uint32_t>(), ctx->d_cand_anchor.as<uint32_t>(),
-            ctx->d_seg_off.as<uint32_t>(), ctx->d_seg_cnt.as<uint32_t>(), counters, cap, status,
-            ctx->d_ares.as<AlignRes>());
+#define LAUNCH_ALIGN(NW)                                                                          \
+    k_align<kAlignBlock, NW><<<(unsigned)ablocks, kAlignBlock, 0, ctx->stream>>>(                 \
+        o, r, first, ctx->d_cand_ids.as<uint32_t>(), ctx->d_cand_anchor.as<uint32_t>(),           \
+        ctx->d_seg_off.as<uint32_t>(), ctx->d_seg_cnt.as<uint32_t>(), counters, cap, status,      \
+        ctx->d_ares.as<AlignRes>())
+        // bit-plane width: 32-base words covering the longest read
+        const int nw = (ctx->max_len + 31) / 32;
+        if (nw <= 4) LAUNCH_ALIGN(4);
+        else if (nw <= 5) LAUNCH_ALIGN(5);
+        else if (nw <= 6) LAUNCH_ALIGN(6);
+        else LAUNCH_ALIGN(8);
+#undef LAUNCH_ALIGN
         CK(cudaGetLastError(), "k_align");
         if (timed) CK(cudaEventRecord(ctx->ev[2], ctx->stream), "event");
         MsaOut mo;
@@ -486,15 +496,31 @@ int run_batch(care_b200_ctx* ctx, uint32_t first, uint32_t count, bool timed) {
         mo.corr_seq = ctx->d_cseq.as<char>();
         mo.corr_count = counters + 1;
         mo.corr_cap = ccap;
-        const int maxcols = 3 * ctx->max_len;
-        if (maxcols <= kMsaBlock * 3)
-            k_msa<kMsaBlock, 3><<<count, kMsaBlock, 0, ctx->stream>>>(
-                o, r, first, count, nullptr, ctx->d_cand_ids.as<uint32_t>(), ctx->d_seg_off.as<uint32_t>(),
-                ctx->d_seg_cnt.as<uint32_t>(), ctx->d_ares.as<AlignRes>(), ctx->d_recs.as<CandRec>(), mo, status);
-        else
-            k_msa<kMsaBlock, 6><<<count, kMsaBlock, 0, ctx->stream>>>(
-                o, r, first, count, nullptr, ctx->d_cand_ids.as<uint32_t>(), ctx->d_seg_off.as<uint32_t>(),
-                ctx->d_seg_cnt.as<uint32_t>(), ctx->d_ares.as<AlignRes>(), ctx->d_recs.as<CandRec>(), mo, status);
+        // widest possible MSA: La + 2*Lmax - 2*minoverlap(La), maximised over La
+        int maxcols = 1;
+        for (int la = 1; la <= ctx->max_len; ++la) {
+            const int lo = (int)((float)la * ctx->opt.min_overlap_ratio);
+            const int mo = std::max(ctx->opt.min_overlap, lo);
+            maxcols = std::max(maxcols, la + 2 * ctx->max_len - 2 * std::min(mo, ctx->max_len));
+        }
+        const int jb = (maxcols + 32 * (kMsaBlock / 32) - 1) / (32 * (kMsaBlock / 32));
+        const size_t msmem = msa_smem_bytes(ctx->max_len, ctx->seq_pitch, ctx->has_qual ? ctx->qual_pitch : 0);
+#define LAUNCH_MSA(JB)                                                                                  \
+    do {                                                                                                \
+        CK(cudaFuncSetAttribute(k_msa<kMsaBlock, JB>, cudaFuncAttributeMaxDynamicSharedMemorySize,       \
+                                (int)msmem), "smem attr");                                              \
+        k_msa<kMsaBlock, JB><<<count, kMsaBlock, msmem, ctx->stream>>>(                                 \
+            o, r, first, count, nullptr, ctx->d_cand_ids.as<uint32_t>(), ctx->d_seg_off.as<uint32_t>(), \
+            ctx->d_seg_cnt.as<uint32_t>(), ctx->d_ares.as<AlignRes>(), ctx->d_recs.as<CandRec>(), mo,   \
+            status);                                                                                    \
+    } while (0)
+        if (jb <= 1) LAUNCH_MSA(1);
+        else if (jb <= 2) LAUNCH_MSA(2);
+        else if (jb <= 3) LAUNCH_MSA(3);
+        else if (jb <= 4) LAUNCH_MSA(4);
+        else if (jb <= 5) LAUNCH_MSA(5);
+        else LAUNCH_MSA(6);
+#undef LAUNCH_MSA
         CK(cudaGetLastError(), "k_msa");
         if (timed) CK(cudaEventRecord(ctx->ev[3], ctx->stream), "event");
         CK(cudaMemcpyAsync(ctx->h_small.p, counters, 16, cudaMemcpyDeviceToHost, ctx->stream), "counters");

@@ -2,18 +2,85 @@
 //
 // Sequences: 2-bit codes A=0,C=1,G=2,T=3 packed 16 per uint32, MSB-first
 // (the reference's layout, include/sequencehelpers.hpp:152-187). The aligner
-// works on "hi/lo bit planes" held in 64-bit words: plane bit i (MSB-first)
+// works on "hi/lo bit planes" held in 32-bit words: plane bit i (MSB-first)
 // is the high / low bit of base i (the HiLo layout of
-// sequencehelpers.hpp:645-697, widened from 32- to 64-bit words).
+// sequencehelpers.hpp:645-697).
+//
+// The per-thread helpers are __host__ __device__ so that a host build can
+// check them against the CPU oracle; the few intrinsics have host shims.
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
 
 namespace careb200 {
 
+#define CB_HD __host__ __device__ __forceinline__
+
+CB_HD uint32_t funnel_l(uint32_t lo, uint32_t hi, int r) {   // high word of (hi:lo) << r
+#ifdef __CUDA_ARCH__
+    return __funnelshift_l(lo, hi, r);
+#else
+    return (uint32_t)(((((unsigned long long)hi) << 32) | lo) << (r & 31) >> 32);
+#endif
+}
+CB_HD int popc32(uint32_t x) {
+#ifdef __CUDA_ARCH__
+    return __popc(x);
+#else
+    return __builtin_popcount(x);
+#endif
+}
+CB_HD uint32_t brev32(uint32_t x) {
+#ifdef __CUDA_ARCH__
+    return __brev(x);
+#else
+    x = ((x >> 1) & 0x55555555u) | ((x & 0x55555555u) << 1);
+    x = ((x >> 2) & 0x33333333u) | ((x & 0x33333333u) << 2);
+    x = ((x >> 4) & 0x0F0F0F0Fu) | ((x & 0x0F0F0F0Fu) << 4);
+    x = ((x >> 8) & 0x00FF00FFu) | ((x & 0x00FF00FFu) << 8);
+    return (x >> 16) | (x << 16);
+#endif
+}
+CB_HD uint32_t ldg32(const uint32_t* p) {
+#ifdef __CUDA_ARCH__
+    return __ldg(p);
+#else
+    return *p;
+#endif
+}
+// IEEE single operations without contraction (host side is built with
+// -ffp-contract=off)
+CB_HD float fmul_rn(float a, float b) {
+#ifdef __CUDA_ARCH__
+    return __fmul_rn(a, b);
+#else
+    return a * b;
+#endif
+}
+CB_HD float fdiv_rn(float a, float b) {
+#ifdef __CUDA_ARCH__
+    return __fdiv_rn(a, b);
+#else
+    return a / b;
+#endif
+}
+CB_HD float fsub_rn(float a, float b) {
+#ifdef __CUDA_ARCH__
+    return __fsub_rn(a, b);
+#else
+    return a - b;
+#endif
+}
+CB_HD int f2i_rz(float x) {
+#ifdef __CUDA_ARCH__
+    return __float2int_rz(x);
+#else
+    return (int)x;
+#endif
+}
+
 constexpr int kMaxLen = 256;          // longest read the kernels accept
 constexpr int kMaxMaps = 48;          // maximum_number_of_maps, include/config.hpp:31
-constexpr int kPlaneWords = 4;        // 64-bit words per bit plane (kMaxLen / 64)
 
 // Per-launch view of the options (include/options.hpp:36-98).
 struct DevOptions {
@@ -93,7 +160,7 @@ enum : int {
 
 // MurmurHash3 64-bit finalizer (the published fmix64), as used by the
 // reference's minhasher (hpc_helpers hashers.cuh:85-139).
-__device__ __forceinline__ unsigned long long murmur64(unsigned long long x) {
+CB_HD unsigned long long murmur64(unsigned long long x) {
     x ^= x >> 33;
     x *= 0xff51afd7ed558ccdULL;
     x ^= x >> 33;
@@ -104,7 +171,7 @@ __device__ __forceinline__ unsigned long long murmur64(unsigned long long x) {
 
 // Reverse complement of a 32-base 2-bit word (reverse the 2-bit groups,
 // complement each code).
-__device__ __forceinline__ unsigned long long revcomp64(unsigned long long n) {
+CB_HD unsigned long long revcomp64(unsigned long long n) {
     n = ((n >> 2) & 0x3333333333333333ull) | ((n & 0x3333333333333333ull) << 2);
     n = ((n >> 4) & 0x0F0F0F0F0F0F0F0Full) | ((n & 0x0F0F0F0F0F0F0F0Full) << 4);
     n = ((n >> 8) & 0x00FF00FF00FF00FFull) | ((n & 0x00FF00FF00FF00FFull) << 8);
@@ -114,7 +181,7 @@ __device__ __forceinline__ unsigned long long revcomp64(unsigned long long n) {
 }
 
 // k-mer of k bases starting at base pos of a packed sequence (k <= 32).
-__device__ __forceinline__ unsigned long long kmer_at(const uint32_t* s, int k, int pos) {
+CB_HD unsigned long long kmer_at(const uint32_t* s, int k, int pos) {
     const int w = pos >> 4, o = pos & 15;
     // up to three 32-bit words cover 32 bases at any offset
     const unsigned long long hi = ((unsigned long long)s[w] << 32) | (unsigned long long)s[w + 1];
@@ -125,12 +192,12 @@ __device__ __forceinline__ unsigned long long kmer_at(const uint32_t* s, int k, 
 }
 
 // 2-bit code of base p of a packed row.
-__device__ __forceinline__ uint32_t base_at(const uint32_t* s, int p) {
+CB_HD uint32_t base_at(const uint32_t* s, int p) {
     return (s[p >> 4] >> (30 - 2 * (p & 15))) & 3u;
 }
 
 // Compress the even bits (0,2,...,30) of x into the low 16 bits, order kept.
-__device__ __forceinline__ uint32_t even_bits(uint32_t x) {
+CB_HD uint32_t even_bits(uint32_t x) {
     x &= 0x55555555u;
     x = (x | (x >> 1)) & 0x33333333u;
     x = (x | (x >> 2)) & 0x0F0F0F0Fu;
@@ -139,67 +206,53 @@ __device__ __forceinline__ uint32_t even_bits(uint32_t x) {
     return x;
 }
 
-// The 2-bit row of a read -> hi/lo planes of W 64-bit words (+1 zero word).
-template <int W>
-__device__ __forceinline__ void load_planes(const uint32_t* __restrict__ s, int L,
-                                            unsigned long long (&hi)[W + 1],
-                                            unsigned long long (&lo)[W + 1]) {
+// The 2-bit row of a read -> hi/lo bit planes of NW 32-bit words (32 bases
+// per word, MSB-first; the reference's HiLo layout, sequencehelpers.hpp:
+// 645-697), plus two zero words so that windows may read past the end.
+template <int NW>
+CB_HD void load_planes(const uint32_t* __restrict__ s, int L,
+                                            uint32_t (&hi)[NW + 2], uint32_t (&lo)[NW + 2]) {
     const int nints = (L + 15) >> 4;
 #pragma unroll
-    for (int w = 0; w <= W; ++w) { hi[w] = 0; lo[w] = 0; }
-#pragma unroll
-    for (int w = 0; w < W; ++w) {
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const int idx = 4 * w + q;
-            if (idx < nints) {
-                const uint32_t x = __ldg(s + idx);
-                hi[w] |= (unsigned long long)even_bits(x >> 1) << (48 - 16 * q);
-                lo[w] |= (unsigned long long)even_bits(x) << (48 - 16 * q);
-            }
-        }
-        const int valid = L - 64 * w;
-        if (valid <= 0) { hi[w] = 0; lo[w] = 0; }
-        else if (valid < 64) {
-            const unsigned long long m = ~(~0ull >> valid);
-            hi[w] &= m; lo[w] &= m;
-        }
+    for (int w = 0; w < NW; ++w) {
+        const uint32_t x0 = 2 * w < nints ? ldg32(s + 2 * w) : 0u;
+        const uint32_t x1 = 2 * w + 1 < nints ? ldg32(s + 2 * w + 1) : 0u;
+        uint32_t h = (even_bits(x0 >> 1) << 16) | even_bits(x1 >> 1);
+        uint32_t l = (even_bits(x0) << 16) | even_bits(x1);
+        const int valid = L - 32 * w;
+        const uint32_t m = valid >= 32 ? 0xFFFFFFFFu : (valid <= 0 ? 0u : ~(0xFFFFFFFFu >> valid));
+        hi[w] = h & m;
+        lo[w] = l & m;
     }
+    hi[NW] = hi[NW + 1] = 0u;
+    lo[NW] = lo[NW + 1] = 0u;
 }
 
-// Planes of the reverse complement of a read of length L given its planes.
-template <int W>
-__device__ __forceinline__ void revcomp_planes(const unsigned long long (&hi)[W + 1],
-                                               const unsigned long long (&lo)[W + 1], int L,
-                                               unsigned long long (&rhi)[W + 1],
-                                               unsigned long long (&rlo)[W + 1]) {
-    // reverse the 64W-bit string word by word
+// Planes of the reverse complement of a read of length L: base i of the
+// result is the complement of base L-1-i (complement flips both bits).
+template <int NW>
+CB_HD void revcomp_planes(const uint32_t (&hi)[NW + 2], const uint32_t (&lo)[NW + 2],
+                                               int L, uint32_t (&rhi)[NW + 2], uint32_t (&rlo)[NW + 2]) {
 #pragma unroll
-    for (int j = 0; j < W; ++j) { rhi[j] = __brevll(hi[W - 1 - j]); rlo[j] = __brevll(lo[W - 1 - j]); }
-    rhi[W] = 0; rlo[W] = 0;
-    // drop the 64W-L leading bits that came from the padding
-    const int d = 64 * W - L;
-    const int dq = d >> 6, dr = d & 63;
+    for (int j = 0; j < NW; ++j) { rhi[j] = brev32(hi[NW - 1 - j]); rlo[j] = brev32(lo[NW - 1 - j]); }
+    rhi[NW] = rhi[NW + 1] = 0u;
+    rlo[NW] = rlo[NW + 1] = 0u;
+    const int d = 32 * NW - L;            // leading bits that came from padding
+    const int dq = d >> 5, dr = d & 31;
 #pragma unroll
-    for (int step = 0; step < W; ++step) {
+    for (int step = 0; step < NW; ++step) {
         if (step < dq) {
 #pragma unroll
-            for (int j = 0; j < W; ++j) { rhi[j] = rhi[j + 1]; rlo[j] = rlo[j + 1]; }
-            rhi[W] = 0; rlo[W] = 0;
+            for (int j = 0; j < NW; ++j) { rhi[j] = rhi[j + 1]; rlo[j] = rlo[j + 1]; }
+            rhi[NW] = 0u; rlo[NW] = 0u;
         }
     }
-    if (dr) {
 #pragma unroll
-        for (int j = 0; j < W; ++j) {
-            rhi[j] = (rhi[j] << dr) | (rhi[j + 1] >> (64 - dr));
-            rlo[j] = (rlo[j] << dr) | (rlo[j + 1] >> (64 - dr));
-        }
-    }
-    // complement the L valid bases, keep zeros beyond
-#pragma unroll
-    for (int j = 0; j < W; ++j) {
-        const int valid = L - 64 * j;
-        unsigned long long m = valid >= 64 ? ~0ull : (valid <= 0 ? 0ull : ~(~0ull >> valid));
+    for (int j = 0; j < NW; ++j) {
+        rhi[j] = funnel_l(rhi[j + 1], rhi[j], dr);
+        rlo[j] = funnel_l(rlo[j + 1], rlo[j], dr);
+        const int valid = L - 32 * j;
+        const uint32_t m = valid >= 32 ? 0xFFFFFFFFu : (valid <= 0 ? 0u : ~(0xFFFFFFFFu >> valid));
         rhi[j] = (~rhi[j]) & m;
         rlo[j] = (~rlo[j]) & m;
     }
@@ -209,112 +262,121 @@ struct ShdResult {
     int score, overlap, shift, nops, valid;
 };
 
+// Keeps the `valid` leading bits of a 32-bit word (valid in 0..32).
+CB_HD uint32_t lead_mask(int valid) {
+    return valid >= 32 ? 0xFFFFFFFFu : (valid <= 0 ? 0u : ~(0xFFFFFFFFu >> valid));
+}
+
 // One scan direction of the shifted Hamming distance. The "shifted" planes S
-// are slid by t = t0..t1 bases against the "other" planes O, exactly in the
-// reference's order with its pruning (src/cpu_alignment.cpp:247-316):
-// max_errors_excl = min(int(ov*maxErrorRate), best - total + 2*ov); a shift
-// with max_errors_excl <= 0 ends the direction; mismatches < max_errors_excl
-// and score < best replaces the best (first best kept).
-template <int W>
-__device__ __forceinline__ void shd_scan(unsigned long long (&Shi)[W + 1], unsigned long long (&Slo)[W + 1],
-                                         const unsigned long long (&Ohi)[W + 1],
-                                         const unsigned long long (&Olo)[W + 1], int t0, int t1,
-                                         int sign, int La, int Lc, int total, float mer, int& best,
-                                         int& bestShift) {
+// slide by t = t0..t1 bases against the "other" planes O, in the reference's
+// order and with its pruning (src/cpu_alignment.cpp:247-316):
+//   max_errors_excl = min(int(ov * maxErrorRate), best - total + 2*ov);
+//   max_errors_excl <= 0 ends the direction; a shift whose mismatch count is
+//   below it replaces the best when its score is strictly smaller.
+// Mismatches are counted 64 bases at a time (two funnel-shifted 32-bit words
+// per plane); further words are only read while the count stays below the
+// limit, which decides the same comparisons as the reference's early exit.
+// mextab[ov] holds int(float(ov) * maxErrorRate).
+template <int NW>
+CB_HD void shd_scan(uint32_t (&Sh)[NW + 2], uint32_t (&Sl)[NW + 2],
+                                         const uint32_t (&Oh)[NW + 2], const uint32_t (&Ol)[NW + 2],
+                                         int t0, int t1, int sign, int La, int Lc, int total,
+                                         const int* __restrict__ mextab, int& best, int& bestShift) {
     if (t1 < t0) return;
     bool stop = false;
 #pragma unroll 1
-    for (int q = 0; q <= (t1 >> 6) && !stop; ++q) {
-        const int rb = (q == (t0 >> 6)) ? (t0 & 63) : 0;
-        const int re = (q == (t1 >> 6)) ? (t1 & 63) : 63;
-        if (q >= (t0 >> 6)) {
+    for (int w = 0; w <= (t1 >> 5) && !stop; ++w) {
+        const int rb = (w == (t0 >> 5)) ? (t0 & 31) : 0;
+        const int re = (w == (t1 >> 5)) ? (t1 & 31) : 31;
 #pragma unroll 1
-            for (int rr = rb; rr <= re; ++rr) {
-                const int t = 64 * q + rr;
-                const int ov = sign > 0 ? min(La - t, Lc) : min(La, Lc - t);
-                int mex = __float2int_rz(__fmul_rn((float)ov, mer));
-                mex = min(mex, best - total + 2 * ov);
-                if (mex <= 0) { stop = true; break; }
-                const int nw = (ov + 63) >> 6;
-                int mm = 0;
+        for (int r = rb; r <= re; ++r) {
+            const int t = 32 * w + r;
+            const int ov = sign > 0 ? min(La - t, Lc) : min(La, Lc - t);
+            const int mex = min(mextab[ov], best - total + 2 * ov);
+            if (mex <= 0) { stop = true; break; }
+            uint32_t d0 = (funnel_l(Sh[1], Sh[0], r) ^ Oh[0]) | (funnel_l(Sl[1], Sl[0], r) ^ Ol[0]);
+            uint32_t d1 = (funnel_l(Sh[2], Sh[1], r) ^ Oh[1]) | (funnel_l(Sl[2], Sl[1], r) ^ Ol[1]);
+            if (ov < 64) { d0 &= lead_mask(ov); d1 &= lead_mask(ov - 32); }
+            int mm = popc32(d0) + popc32(d1);
+            if (mm < mex && ov > 64) {
 #pragma unroll
-                for (int j = 0; j < W; ++j) {
-                    if (j < nw && mm < mex) {
-                        const unsigned long long xh = rr ? (Shi[j] << rr) | (Shi[j + 1] >> (64 - rr)) : Shi[j];
-                        const unsigned long long xl = rr ? (Slo[j] << rr) | (Slo[j + 1] >> (64 - rr)) : Slo[j];
-                        unsigned long long dbits = (xh ^ Ohi[j]) | (xl ^ Olo[j]);
-                        const int valid = ov - 64 * j;
-                        if (valid < 64) dbits &= ~(~0ull >> valid);
-                        mm += __popcll(dbits);
+                for (int j = 2; j < NW; ++j) {
+                    if (32 * j < ov && mm < mex) {
+                        uint32_t dj = (funnel_l(Sh[j + 1], Sh[j], r) ^ Oh[j]) |
+                                      (funnel_l(Sl[j + 1], Sl[j], r) ^ Ol[j]);
+                        dj &= lead_mask(ov - 32 * j);
+                        mm += popc32(dj);
                     }
                 }
-                if (mm < mex) {
-                    const int sc = mm + total - 2 * ov;
-                    if (sc < best) { best = sc; bestShift = sign * t; }
-                }
+            }
+            if (mm < mex) {
+                const int sc = mm + total - 2 * ov;
+                if (sc < best) { best = sc; bestShift = sign * t; }
             }
         }
-        // slide the shifted planes by one 64-base word
+        // slide the shifted planes by one 32-base word
 #pragma unroll
-        for (int j = 0; j < W; ++j) { Shi[j] = Shi[j + 1]; Slo[j] = Slo[j + 1]; }
-        Shi[W] = 0; Slo[W] = 0;
+        for (int j = 0; j < NW + 1; ++j) { Sh[j] = Sh[j + 1]; Sl[j] = Sl[j + 1]; }
+        Sh[NW + 1] = 0u; Sl[NW + 1] = 0u;
     }
 }
 
-// cpuShiftedHammingDistancePopcount2BitHiLo (src/cpu_alignment.cpp:32-323).
-template <int W>
-__device__ __forceinline__ ShdResult shifted_hamming(const unsigned long long (&Ahi)[W + 1],
-                                                     const unsigned long long (&Alo)[W + 1], int La,
-                                                     const unsigned long long (&Chi)[W + 1],
-                                                     const unsigned long long (&Clo)[W + 1], int Lc,
-                                                     int minov, float mer) {
+// cpuShiftedHammingDistancePopcount2BitHiLo (src/cpu_alignment.cpp:32-323):
+// shifts 0..La-minov (anchor slid against the candidate), then -1..-(Lc-minov)
+// (candidate slid against the anchor).
+template <int NW>
+CB_HD ShdResult shifted_hamming(const uint32_t (&Ah)[NW + 2], const uint32_t (&Al)[NW + 2],
+                                                     int La, const uint32_t (&Ch)[NW + 2],
+                                                     const uint32_t (&Cl)[NW + 2], int Lc, int minov,
+                                                     const int* __restrict__ mextab) {
     const int total = La + Lc;
     int best = total, bestShift = -Lc;
-    unsigned long long Shi[W + 1], Slo[W + 1];
+    uint32_t Sh[NW + 2], Sl[NW + 2];
+#pragma unroll 1
+    for (int dir = 0; dir < 2; ++dir) {
 #pragma unroll
-    for (int j = 0; j <= W; ++j) { Shi[j] = Ahi[j]; Slo[j] = Alo[j]; }
-    shd_scan<W>(Shi, Slo, Chi, Clo, 0, La - minov, +1, La, Lc, total, mer, best, bestShift);
-#pragma unroll
-    for (int j = 0; j <= W; ++j) { Shi[j] = Chi[j]; Slo[j] = Clo[j]; }
-    shd_scan<W>(Shi, Slo, Ahi, Alo, 1, Lc - minov, -1, La, Lc, total, mer, best, bestShift);
-    ShdResult r;
-    r.valid = bestShift != -Lc;
+        for (int j = 0; j < NW + 2; ++j) { Sh[j] = dir ? Ch[j] : Ah[j]; Sl[j] = dir ? Cl[j] : Al[j]; }
+        if (dir == 0) shd_scan<NW>(Sh, Sl, Ch, Cl, 0, La - minov, +1, La, Lc, total, mextab, best, bestShift);
+        else shd_scan<NW>(Sh, Sl, Ah, Al, 1, Lc - minov, -1, La, Lc, total, mextab, best, bestShift);
+    }
+    ShdResult res;
+    res.valid = bestShift != -Lc;
     const int cb = max(-bestShift, 0);
     const int ce = min(Lc, La - bestShift);
-    r.overlap = ce - cb;
-    r.score = best;
-    r.shift = bestShift;
-    r.nops = best - total + 2 * r.overlap;
-    return r;
+    res.overlap = ce - cb;
+    res.score = best;
+    res.shift = bestShift;
+    res.nops = best - total + 2 * res.overlap;
+    return res;
 }
 
 // chooseBestAlignmentOrientation (include/alignmentorientation.hpp:12-92).
-__device__ __forceinline__ int choose_orientation(const ShdResult& f, const ShdResult& r, int La,
+CB_HD int choose_orientation(const ShdResult& f, const ShdResult& r, int La,
                                                   float min_overlap_ratio, int min_overlap,
                                                   float maxErrorRate) {
     int ret = 3;
-    const int lo = __float2int_rz(__fmul_rn((float)La, min_overlap_ratio));
+    const int lo = f2i_rz(fmul_rn((float)La, min_overlap_ratio));
     const int mo = lo > min_overlap ? lo : min_overlap;
     if (f.valid && f.overlap >= mo) {
         if (r.valid && r.overlap >= mo) {
-            const float ratio = __fdiv_rn((float)f.nops, (float)f.overlap);
-            const float rratio = __fdiv_rn((float)r.nops, (float)r.overlap);
+            const float ratio = fdiv_rn((float)f.nops, (float)f.overlap);
+            const float rratio = fdiv_rn((float)r.nops, (float)r.overlap);
             if (ratio < rratio) { if (ratio < maxErrorRate) ret = 1; }
             else if (rratio < ratio) { if (rratio < maxErrorRate) ret = 2; }
             else if (ratio < maxErrorRate) ret = f.overlap > r.overlap ? 1 : 2;
-        } else if (__fdiv_rn((float)f.nops, (float)f.overlap) < maxErrorRate) ret = 1;
+        } else if (fdiv_rn((float)f.nops, (float)f.overlap) < maxErrorRate) ret = 1;
     } else if (r.valid && r.overlap >= mo) {
-        if (__fdiv_rn((float)r.nops, (float)r.overlap) < maxErrorRate) ret = 2;
+        if (fdiv_rn((float)r.nops, (float)r.overlap) < maxErrorRate) ret = 2;
     }
     return ret;
 }
 
 // feq / fleq / fgeq (include/hostdevicefunctions.cuh:9-29).
-__device__ __forceinline__ bool feq(float l, float r) {
-    const float d = __fsub_rn(l, r);
+CB_HD bool feq(float l, float r) {
+    const float d = fsub_rn(l, r);
     return (d < 0 ? -d : d) < 1e-5f;
 }
-__device__ __forceinline__ bool fleq(float l, float r) { return (l < r) || feq(l, r); }
-__device__ __forceinline__ bool fgeq(float l, float r) { return (l > r) || feq(l, r); }
+CB_HD bool fleq(float l, float r) { return (l < r) || feq(l, r); }
+CB_HD bool fgeq(float l, float r) { return (l > r) || feq(l, r); }
 
 }  // namespace careb200

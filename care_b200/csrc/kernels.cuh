@@ -192,32 +192,35 @@ k_candidates(DevOptions o, DevReads r, const TableDesc* __restrict__ td, const S
 //   chooseBestAlignmentOrientation    include/alignmentorientation.hpp:72-92
 //   computePairFlags                  include/corrector.hpp:763-807 (PE)
 // ---------------------------------------------------------------------------
-template <int BLOCK>
+template <int BLOCK, int NW>
 __global__ void __launch_bounds__(BLOCK)
 k_align(DevOptions o, DevReads r, uint32_t first, const uint32_t* __restrict__ cand_ids,
         const uint32_t* __restrict__ cand_anchor, const uint32_t* __restrict__ seg_off,
         const uint32_t* __restrict__ seg_cnt, const unsigned long long* __restrict__ total_ptr,
         unsigned long long arena_cap, const int* __restrict__ status, AlignRes* __restrict__ out) {
+    __shared__ int s_mex[kMaxLen + 1];
+    // int(float(ov) * maxErrorRate), the first term of max_errors_excl
+    for (int i = threadIdx.x; i <= kMaxLen; i += BLOCK) s_mex[i] = __float2int_rz(__fmul_rn((float)i, o.max_error_rate));
+    __syncthreads();
     // an overflowed candidate arena holds unwritten entries: the batch is
     // repeated with a larger arena, nothing here may read them
     if (*status & kStatusCandOverflow) return;
     const unsigned long long i = (unsigned long long)blockIdx.x * BLOCK + threadIdx.x;
     const unsigned long long total = *total_ptr;
     if (total > arena_cap || i >= total) return;
-    constexpr int W = kPlaneWords;
     const uint32_t ai = cand_anchor[i];
     const uint32_t a = first + ai;
     const uint32_t c = cand_ids[i];
     const int La = r.len[a], Lc = r.len[c];
-    unsigned long long Ahi[W + 1], Alo[W + 1], Chi[W + 1], Clo[W + 1];
-    load_planes<W>(r.seq + (size_t)a * r.seq_pitch, La, Ahi, Alo);
-    load_planes<W>(r.seq + (size_t)c * r.seq_pitch, Lc, Chi, Clo);
+    uint32_t Ah[NW + 2], Al[NW + 2], Ch[NW + 2], Cl[NW + 2];
+    load_planes<NW>(r.seq + (size_t)a * r.seq_pitch, La, Ah, Al);
+    load_planes<NW>(r.seq + (size_t)c * r.seq_pitch, Lc, Ch, Cl);
     const int lo = __float2int_rz(__fmul_rn((float)La, o.min_overlap_ratio));
     const int minov = o.min_overlap > lo ? o.min_overlap : lo;
-    const ShdResult f = shifted_hamming<W>(Ahi, Alo, La, Chi, Clo, Lc, minov, o.max_error_rate);
-    unsigned long long Rhi[W + 1], Rlo[W + 1];
-    revcomp_planes<W>(Chi, Clo, Lc, Rhi, Rlo);
-    const ShdResult rc = shifted_hamming<W>(Ahi, Alo, La, Rhi, Rlo, Lc, minov, o.max_error_rate);
+    const ShdResult f = shifted_hamming<NW>(Ah, Al, La, Ch, Cl, Lc, minov, s_mex);
+    uint32_t Rh[NW + 2], Rl[NW + 2];
+    revcomp_planes<NW>(Ch, Cl, Lc, Rh, Rl);
+    const ShdResult rc = shifted_hamming<NW>(Ah, Al, La, Rh, Rl, Lc, minov, s_mex);
     const int orient = choose_orientation(f, rc, La, o.min_overlap_ratio, o.min_overlap,
                                           __fmul_rn(o.estimated_errorrate, 4.0f));
     AlignRes res;
@@ -257,9 +260,15 @@ k_align(DevOptions o, DevReads r, uint32_t first, const uint32_t* __restrict__ c
 //   getCorrectedAnchor                src/msa.cpp:379-453
 //   getCorrectedCandidates            src/msa.cpp:457-522
 //   makeOutputOfTask (edits)          include/corrector.hpp:1639-1761
-// Column sums are accumulated by the thread that owns the column, anchor
+//
+// Layout: warp w owns the 32-column blocks w, w+NWARP, ...; lane l owns
+// column 32*block + l. A column's sums are accumulated by its owner, anchor
 // first and then candidates in list order, with separate IEEE multiply and
-// add (no FMA) -- the reference's exact order and rounding.
+// add (no FMA) -- the reference's order and rounding, so the sums are
+// bit-identical. A warp skips a candidate that covers none of a block's
+// columns (a warp-uniform test). Candidate rows are decoded once into 16-bit
+// elements (2-bit base | quality character << 2) in shared memory and kept
+// across refinement rebuilds when the candidate list fits (kStage rows).
 // ---------------------------------------------------------------------------
 struct MsaOut {
     uint8_t* status;
@@ -274,30 +283,36 @@ struct MsaOut {
     unsigned long long corr_cap;
 };
 
-constexpr int kStage = 32;            // candidates staged in shared memory at a time
+constexpr int kStage = 64;            // candidate rows held in shared memory
 
-template <int BLOCK, int COLS>
+// dynamic shared memory of k_msa: decoded rows (kStage + anchor) and raw rows
+__host__ __device__ inline size_t msa_smem_bytes(int max_len, int seq_pitch, int qual_pitch) {
+    const size_t elem = (size_t)(kStage + 1) * max_len * 2;
+    const size_t raw = (size_t)kStage * (seq_pitch + qual_pitch) * 4;
+    return ((elem + 15) & ~(size_t)15) + raw;
+}
+
+template <int BLOCK, int JB>
 __global__ void __launch_bounds__(BLOCK)
 k_msa(DevOptions o, DevReads r, uint32_t first, uint32_t count, const uint32_t* __restrict__ order,
       const uint32_t* __restrict__ cand_ids, const uint32_t* __restrict__ seg_off,
       const uint32_t* __restrict__ seg_cnt, const AlignRes* __restrict__ ares,
       CandRec* __restrict__ recs, MsaOut out, int* __restrict__ status) {
-    constexpr int MAXCOLS = BLOCK * COLS;
-    constexpr int NW = BLOCK / 32;
+    constexpr int NWARP = BLOCK / 32;
+    constexpr int MAXCOLS = 32 * JB * NWARP;
+    extern __shared__ __align__(16) unsigned char dsm[];
     __shared__ uint8_t s_cons[MAXCOLS];
     __shared__ float s_support[MAXCOLS];
     __shared__ uint16_t s_cov[MAXCOLS];
     __shared__ uint16_t s_cnt[MAXCOLS][4];
-    __shared__ uint32_t s_aseq[kMaxLen / 16 + 2];
-    __shared__ uint32_t s_aqual[kMaxLen / 4 + 2];
-    __shared__ uint32_t s_cseq[kStage][kMaxLen / 16];
-    __shared__ uint32_t s_cqual[kStage][kMaxLen / 4];
-    __shared__ int s_cbeg[kStage], s_clen[kStage];
-    __shared__ float s_cw[kStage];
-    __shared__ int s_cfwd[kStage];
-    __shared__ int s_red[NW][4];
+    __shared__ float s_qw[256];
+    __shared__ int s_beg[kStage], s_len[kStage];
+    __shared__ float s_w[kStage];
+    __shared__ uint32_t s_id[kStage];
+    __shared__ uint8_t s_fwd[kStage];
+    __shared__ uint8_t s_alive[kStage];
+    __shared__ int s_red[NWARP][4];
     __shared__ int s_vals[8];
-    __shared__ float s_fvals[4];
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     if (blockIdx.x >= count) return;
@@ -309,6 +324,10 @@ k_msa(DevOptions o, DevReads r, uint32_t first, uint32_t count, const uint32_t* 
     const int mlen = r.max_len;
     const bool useQ = o.use_quality && r.qual != nullptr;
     char* aout = out.seq + (size_t)ai * mlen;
+    uint16_t* s_elem = (uint16_t*)dsm;                       // [kStage][mlen]
+    uint16_t* s_aelem = s_elem + (size_t)kStage * mlen;      // anchor row
+    uint32_t* s_rseq = (uint32_t*)(dsm + (((size_t)(kStage + 1) * mlen * 2 + 15) & ~(size_t)15));
+    uint32_t* s_rqual = s_rseq + (size_t)kStage * r.seq_pitch;
 
     if (cnt == 0) {
         if (tid == 0) { out.status[ai] = 0; out.nedits[ai] = 0; }
@@ -328,10 +347,10 @@ k_msa(DevOptions o, DevReads r, uint32_t first, uint32_t count, const uint32_t* 
         __syncthreads();
         int t0 = 0, t1 = 0, t2 = 0, t3 = 0;
 #pragma unroll
-        for (int w = 0; w < NW; ++w) { t0 += s_red[w][0]; t1 += s_red[w][1]; t2 += s_red[w][2]; t3 += s_red[w][3]; }
+        for (int w = 0; w < NWARP; ++w) { t0 += s_red[w][0]; t1 += s_red[w][1]; t2 += s_red[w][2]; t3 += s_red[w][3]; }
         res[0] = t0; res[1] = t1; res[2] = t2; res[3] = t3;
     };
-    // block-wide exclusive scan of one flag per thread; returns the prefix, *tot the sum
+    // block-wide exclusive scan of one value per thread; *tot gets the sum
     auto block_scan = [&](int v, int* tot) {
         int x = v;
 #pragma unroll
@@ -344,22 +363,22 @@ k_msa(DevOptions o, DevReads r, uint32_t first, uint32_t count, const uint32_t* 
         __syncthreads();
         int pre = 0, all = 0;
 #pragma unroll
-        for (int w = 0; w < NW; ++w) { const int s = s_red[w][0]; if (w < warp) pre += s; all += s; }
+        for (int w = 0; w < NWARP; ++w) { const int sv = s_red[w][0]; if (w < warp) pre += sv; all += sv; }
         *tot = all;
         return pre + x - v;
     };
 
     // ---- alignment filters (corrector.hpp:982-1211), ordered compaction ----
-    const float base = __fmul_rn(o.estimated_errorrate, 1.0f);
+    const float base = fmul_rn(o.estimated_errorrate, 1.0f);
     int c0 = 0, c1 = 0, c2 = 0, n1 = 0;
     for (uint32_t i = tid; i < cnt; i += BLOCK) {
         const AlignRes ar = ares[off + i];
         if (ar.orient != 3) {
             n1++;
-            const float mr = __fdiv_rn((float)ar.nops, (float)ar.overlap);
-            c0 += mr < __fmul_rn(2.0f, base);
-            c1 += mr < __fmul_rn(3.0f, base);
-            c2 += mr < __fmul_rn(4.0f, base);
+            const float mr = fdiv_rn((float)ar.nops, (float)ar.overlap);
+            c0 += mr < fmul_rn(2.0f, base);
+            c1 += mr < fmul_rn(3.0f, base);
+            c2 += mr < fmul_rn(4.0f, base);
         }
     }
     int red[4];
@@ -370,11 +389,11 @@ k_msa(DevOptions o, DevReads r, uint32_t first, uint32_t count, const uint32_t* 
     }
     float thr = -3.402823466e+38f;
     {
-        const float good = __fmul_rn(o.estimated_coverage, o.m_coverage);
+        const float good = fmul_rn(o.estimated_coverage, o.m_coverage);
         if (red[0] > 0 || red[1] > 0 || red[2] > 0) {
-            if ((float)red[0] >= good) thr = __fmul_rn(2.0f, base);
-            else if ((float)red[1] >= good) thr = __fmul_rn(3.0f, base);
-            else if ((float)red[2] >= good) thr = __fmul_rn(4.0f, base);
+            if ((float)red[0] >= good) thr = fmul_rn(2.0f, base);
+            else if ((float)red[1] >= good) thr = fmul_rn(3.0f, base);
+            else if ((float)red[2] >= good) thr = fmul_rn(4.0f, base);
         }
     }
     int V = 0;
@@ -385,7 +404,7 @@ k_msa(DevOptions o, DevReads r, uint32_t first, uint32_t count, const uint32_t* 
         if (i < cnt) {
             ar = ares[off + i];
             if (ar.orient != 3) {
-                const float mr = __fdiv_rn((float)ar.nops, (float)ar.overlap);
+                const float mr = fdiv_rn((float)ar.nops, (float)ar.overlap);
                 keep = o.paired_end ? (ar.paired || mr < o.paired_filter_threshold) : (mr < thr);
             }
         }
@@ -397,8 +416,7 @@ k_msa(DevOptions o, DevReads r, uint32_t first, uint32_t count, const uint32_t* 
             rec.shift = ar.shift;
             rec.len = (uint16_t)r.len[rec.id];
             // calculateOverlapWeight: 1 - sqrtf(nOps / (overlap * maxMismatchRatio))
-            rec.weight = __fsub_rn(1.0f, __fsqrt_rn(__fdiv_rn((float)ar.nops,
-                                                          __fmul_rn((float)ar.overlap, o.max_error_rate))));
+            rec.weight = fsub_rn(1.0f, __fsqrt_rn(fdiv_rn((float)ar.nops, fmul_rn((float)ar.overlap, o.max_error_rate))));
             rec.orient = ar.orient;
             recs[off + V + pre] = rec;
         }
@@ -410,35 +428,92 @@ k_msa(DevOptions o, DevReads r, uint32_t first, uint32_t count, const uint32_t* 
     }
     __syncthreads();
 
-    // ---- anchor row and qualities ----
-    for (int i = tid; i < r.seq_pitch; i += BLOCK) s_aseq[i] = __ldg(r.seq + (size_t)a * r.seq_pitch + i);
-    if (useQ) for (int i = tid; i < r.qual_pitch; i += BLOCK) s_aqual[i] = __ldg(r.qual + (size_t)a * r.qual_pitch + i);
-    __syncthreads();
-
+    // ---- quality weights, anchor row ----
+    for (int i = tid; i < 256; i += BLOCK) s_qw[i] = c_qweight[i];
     const int qbits = o.quality_bits;
-    auto qual_weight = [&](const uint32_t* row, int p) -> float {
-        uint32_t ch;
-        if (qbits == 8) ch = (row[p >> 2] >> (8 * (p & 3))) & 0xFFu;
-        else if (qbits == 2) {
-            const uint32_t b = (row[p >> 4] >> (30 - 2 * (p & 15))) & 3u;
-            ch = b == 0 ? '$' : b == 1 ? '(' : b == 2 ? '1' : '9';
-        } else {
-            const uint32_t b = (row[p >> 5] >> (31 - (p & 31))) & 1u;
-            ch = b == 0 ? '(' : '5';
+    const int sp = r.seq_pitch, qp = r.qual_pitch;
+    // quality character at position q of an encoded row (qualityscorecompression.hpp:121-145)
+    auto qual_char = [&](const uint32_t* row, int q) -> uint32_t {
+        if (qbits == 8) return (row[q >> 2] >> (8 * (q & 3))) & 0xFFu;
+        if (qbits == 2) {
+            const uint32_t b = (row[q >> 4] >> (30 - 2 * (q & 15))) & 3u;
+            return b == 0 ? '$' : b == 1 ? '(' : b == 2 ? '1' : '9';
         }
-        return c_qweight[ch];
+        return ((row[q >> 5] >> (31 - (q & 31))) & 1u) ? '5' : '(';
     };
+    {
+        const uint32_t* arow = r.seq + (size_t)a * sp;
+        const uint32_t* aq = useQ ? r.qual + (size_t)a * qp : nullptr;
+        for (int p = tid; p < La; p += BLOCK) {
+            const uint32_t b = base_at(arow, p);
+            const uint32_t q = useQ ? qual_char(aq, p) : 0u;
+            s_aelem[p] = (uint16_t)(b | (q << 2));
+        }
+    }
+
+    // stage candidate rows [c, c+n) of recs into slots 0..n-1
+    auto stage = [&](int c, int n) {
+        __syncthreads();
+        for (int e = tid; e < n * sp; e += BLOCK) {
+            const int k = e / sp, w = e - k * sp;
+            s_rseq[k * sp + w] = __ldg(r.seq + (size_t)recs[off + c + k].id * sp + w);
+        }
+        if (useQ)
+            for (int e = tid; e < n * qp; e += BLOCK) {
+                const int k = e / qp, w = e - k * qp;
+                s_rqual[k * qp + w] = __ldg(r.qual + (size_t)recs[off + c + k].id * qp + w);
+            }
+        if (tid < n) {
+            const CandRec rc = recs[off + c + tid];
+            s_beg[tid] = rc.shift;          // relative to the anchor; abegin added per build
+            s_len[tid] = rc.len;
+            s_w[tid] = rc.weight;
+            s_fwd[tid] = rc.orient == 1;
+            s_id[tid] = rc.id;
+        }
+        __syncthreads();
+        for (int e = tid; e < n * mlen; e += BLOCK) {
+            const int k = e / mlen, p = e - k * mlen;
+            const int L = s_len[k];
+            if (p < L) {
+                const bool fwd = s_fwd[k];
+                const uint32_t b = fwd ? base_at(s_rseq + k * sp, p) : (base_at(s_rseq + k * sp, L - 1 - p) ^ 3u);
+                // reverse-complement candidates read their qualities reversed
+                // over the whole quality pitch (reverseQualitiesOfRCAlignments,
+                // corrector.hpp:1227-1239)
+                const uint32_t q = useQ ? qual_char(s_rqual + k * qp, fwd ? p : mlen - 1 - p) : 0u;
+                s_elem[k * mlen + p] = (uint16_t)(b | (q << 2));
+            }
+        }
+        __syncthreads();
+    };
+
+    const bool persistent = V <= kStage;      // all rows stay staged across rebuilds
+    int nalive = V;
+    if (persistent) {
+        stage(0, V);
+        for (int k = tid; k < V; k += BLOCK) s_alive[k] = (uint8_t)k;
+    }
+    __syncthreads();
 
     int abegin = 0, aend = 0, ncols = 0;
     bool allGood = false, hq = false;
 
     for (int iter = 0;; ++iter) {
-        // ---- MSA geometry ----
+        // ---- MSA geometry (build, msa.cpp:17-33) ----
         int mn = 0, mx = La;
-        for (int k = tid; k < V; k += BLOCK) {
-            const CandRec rc = recs[off + k];
-            mn = min(mn, (int)rc.shift);
-            mx = max(mx, (int)rc.shift + (int)rc.len);
+        if (persistent) {
+            for (int i = tid; i < nalive; i += BLOCK) {
+                const int k = s_alive[i];
+                mn = min(mn, s_beg[k]);
+                mx = max(mx, s_beg[k] + s_len[k]);
+            }
+        } else {
+            for (int k = tid; k < nalive; k += BLOCK) {
+                const CandRec rc = recs[off + k];
+                mn = min(mn, (int)rc.shift);
+                mx = max(mx, (int)rc.shift + (int)rc.len);
+            }
         }
 #pragma unroll
         for (int d = 16; d > 0; d >>= 1) {
@@ -449,7 +524,7 @@ k_msa(DevOptions o, DevReads r, uint32_t first, uint32_t count, const uint32_t* 
         if (lane == 0) { s_red[warp][0] = mn; s_red[warp][1] = mx; }
         __syncthreads();
         mn = 0; mx = La;
-        for (int w = 0; w < NW; ++w) { mn = min(mn, s_red[w][0]); mx = max(mx, s_red[w][1]); }
+        for (int w = 0; w < NWARP; ++w) { mn = min(mn, s_red[w][0]); mx = max(mx, s_red[w][1]); }
         ncols = mx - mn;
         abegin = -mn;
         aend = abegin + La;
@@ -458,72 +533,59 @@ k_msa(DevOptions o, DevReads r, uint32_t first, uint32_t count, const uint32_t* 
             return;
         }
 
-        // ---- column accumulation: anchor, then candidates in order ----
-        int cA[COLS], cC[COLS], cG[COLS], cT[COLS];
-        float wA[COLS], wC[COLS], wG[COLS], wT[COLS];
+        // ---- column sums: anchor, then candidates in list order ----
+        unsigned long long cntp[JB];         // four 16-bit counts per column
+        float wA[JB], wC[JB], wG[JB], wT[JB];
 #pragma unroll
-        for (int j = 0; j < COLS; ++j) {
-            cA[j] = cC[j] = cG[j] = cT[j] = 0;
+        for (int j = 0; j < JB; ++j) {
+            cntp[j] = 0ull;
             wA[j] = wC[j] = wG[j] = wT[j] = 0.0f;
-            const int col = tid + j * BLOCK;
-            if (col >= abegin && col < aend) {
-                const int p = col - abegin;
-                const uint32_t b = base_at(s_aseq, p);
-                const float w = useQ ? __fmul_rn(1.0f, qual_weight(s_aqual, p)) : 1.0f;
-                if (b == 0) { cA[j] = 1; wA[j] = w; } else if (b == 1) { cC[j] = 1; wC[j] = w; }
-                else if (b == 2) { cG[j] = 1; wG[j] = w; } else { cT[j] = 1; wT[j] = w; }
+            const int col = 32 * (warp + NWARP * j) + lane;
+            const int p = col - abegin;
+            if (p >= 0 && p < La) {
+                const uint32_t e = s_aelem[p];
+                const uint32_t b = e & 3u;
+                const float w = useQ ? s_qw[e >> 2] : 1.0f;   // factor 1.0f
+                cntp[j] = 1ull << (16 * b);
+                if (b == 0) wA[j] = w; else if (b == 1) wC[j] = w; else if (b == 2) wG[j] = w; else wT[j] = w;
             }
         }
-        for (int c = 0; c < V; c += kStage) {
-            const int nst = min(kStage, V - c);
-            __syncthreads();
-            // stage rows of nst candidates
-            const int sp = r.seq_pitch, qp = r.qual_pitch;
-            for (int e = tid; e < nst * sp; e += BLOCK) {
-                const int k = e / sp, w = e - k * sp;
-                s_cseq[k][w] = __ldg(r.seq + (size_t)recs[off + c + k].id * sp + w);
-            }
-            if (useQ)
-                for (int e = tid; e < nst * qp; e += BLOCK) {
-                    const int k = e / qp, w = e - k * qp;
-                    s_cqual[k][w] = __ldg(r.qual + (size_t)recs[off + c + k].id * qp + w);
-                }
-            if (tid < nst) {
-                const CandRec rc = recs[off + c + tid];
-                s_cbeg[tid] = abegin + rc.shift;
-                s_clen[tid] = rc.len;
-                s_cw[tid] = rc.weight;
-                s_cfwd[tid] = rc.orient == 1;
-            }
-            __syncthreads();
-            for (int k = 0; k < nst; ++k) {
-                const int cb = s_cbeg[k], cl = s_clen[k];
-                const float fw = s_cw[k];
-                const bool fwd = s_cfwd[k];
+        auto accumulate = [&](int k) {
+            const int cb = abegin + s_beg[k];
+            const int L = s_len[k];
+            const float fk = s_w[k];
+            const uint16_t* row = s_elem + k * mlen;
 #pragma unroll
-                for (int j = 0; j < COLS; ++j) {
-                    const int col = tid + j * BLOCK;
-                    const int p = col - cb;
-                    if (p >= 0 && p < cl) {
-                        uint32_t b = fwd ? base_at(s_cseq[k], p) : (base_at(s_cseq[k], cl - 1 - p) ^ 3u);
-                        // reverse-complement candidates read their qualities
-                        // reversed over the whole quality pitch
-                        // (reverseQualitiesOfRCAlignments, corrector.hpp:1227-1239)
-                        const float w = useQ ? __fmul_rn(fw, qual_weight(s_cqual[k], fwd ? p : mlen - 1 - p))
-                                             : __fmul_rn(fw, 1.0f);
-                        if (b == 0) { cA[j]++; wA[j] = __fadd_rn(wA[j], w); }
-                        else if (b == 1) { cC[j]++; wC[j] = __fadd_rn(wC[j], w); }
-                        else if (b == 2) { cG[j]++; wG[j] = __fadd_rn(wG[j], w); }
-                        else { cT[j]++; wT[j] = __fadd_rn(wT[j], w); }
+            for (int j = 0; j < JB; ++j) {
+                const int c0 = 32 * (warp + NWARP * j);
+                if (c0 < cb + L && c0 + 32 > cb) {           // warp-uniform
+                    const int p = c0 + lane - cb;
+                    if (p >= 0 && p < L) {
+                        const uint32_t e = row[p];
+                        const uint32_t b = e & 3u;
+                        const float w = useQ ? fmul_rn(fk, s_qw[e >> 2]) : fk;
+                        cntp[j] += 1ull << (16 * b);
+                        if (b == 0) wA[j] = __fadd_rn(wA[j], w);
+                        if (b == 1) wC[j] = __fadd_rn(wC[j], w);
+                        if (b == 2) wG[j] = __fadd_rn(wG[j], w);
+                        if (b == 3) wT[j] = __fadd_rn(wT[j], w);
                     }
                 }
             }
+        };
+        if (persistent) {
+            for (int i = 0; i < nalive; ++i) accumulate(s_alive[i]);
+        } else {
+            for (int c = 0; c < nalive; c += kStage) {
+                const int n = min(kStage, nalive - c);
+                stage(c, n);
+                for (int k = 0; k < n; ++k) accumulate(k);
+            }
         }
-        __syncthreads();
-        // ---- consensus and support (findConsensus) ----
+        // ---- consensus and support (findConsensus, msa.cpp:135-157) ----
 #pragma unroll
-        for (int j = 0; j < COLS; ++j) {
-            const int col = tid + j * BLOCK;
+        for (int j = 0; j < JB; ++j) {
+            const int col = 32 * (warp + NWARP * j) + lane;
             if (col < ncols) {
                 uint8_t cs = 0; float cw = wA[j];
                 if (wC[j] > cw) { cs = 1; cw = wC[j]; }
@@ -531,86 +593,107 @@ k_msa(DevOptions o, DevReads r, uint32_t first, uint32_t count, const uint32_t* 
                 if (wT[j] > cw) { cs = 3; cw = wT[j]; }
                 const float colw = __fadd_rn(__fadd_rn(__fadd_rn(wA[j], wC[j]), wG[j]), wT[j]);
                 s_cons[col] = cs;
-                s_support[col] = __fdiv_rn(cw, colw);
-                s_cov[col] = (uint16_t)(cA[j] + cC[j] + cG[j] + cT[j]);
-                s_cnt[col][0] = (uint16_t)cA[j]; s_cnt[col][1] = (uint16_t)cC[j];
-                s_cnt[col][2] = (uint16_t)cG[j]; s_cnt[col][3] = (uint16_t)cT[j];
+                s_support[col] = fdiv_rn(cw, colw);
+                const uint32_t nA = (uint32_t)(cntp[j] & 0xFFFFu), nC = (uint32_t)((cntp[j] >> 16) & 0xFFFFu);
+                const uint32_t nG = (uint32_t)((cntp[j] >> 32) & 0xFFFFu), nT = (uint32_t)(cntp[j] >> 48);
+                s_cov[col] = (uint16_t)(nA + nC + nG + nT);
+                s_cnt[col][0] = (uint16_t)nA; s_cnt[col][1] = (uint16_t)nC;
+                s_cnt[col][2] = (uint16_t)nG; s_cnt[col][3] = (uint16_t)nT;
             }
         }
         __syncthreads();
 
         if (iter >= 5) break;
-        // ---- refinement: findCandidatesOfDifferentRegion ----
-        if (tid == 0) { s_vals[0] = 0; s_vals[1] = 0x7fffffff; s_vals[2] = 0; s_vals[3] = 0; }
-        __syncthreads();
+        // ---- refinement: findCandidatesOfDifferentRegion (msa.cpp:532-734) ----
+        if (tid == 0) s_vals[1] = 0x7fffffff;
         int mism = 0;
-        for (int p = tid; p < La; p += BLOCK) mism |= base_at(s_aseq, p) != s_cons[abegin + p];
+        for (int p = tid; p < La; p += BLOCK) mism |= (s_aelem[p] & 3u) != s_cons[abegin + p];
         if (__syncthreads_or(mism) == 0) break;
-        const int sigThr = __float2int_rz(__fmul_rn((float)o.coverage_int, 0.3f));
+        const int sigThr = f2i_rz(fmul_rn((float)o.coverage_int, 0.3f));
         for (int p = tid; p < La; p += BLOCK) {
             const int col = abegin + p;
             const int cs = s_cons[col];
-            int sig = -1;
+            bool sig = false;
 #pragma unroll
-            for (int b = 0; b < 4; ++b) if (b != cs && sigThr <= (int)s_cnt[col][b]) sig = b;
-            if (sig >= 0) atomicMin(&s_vals[1], col);
+            for (int b = 0; b < 4; ++b) sig |= (b != cs && sigThr <= (int)s_cnt[col][b]);
+            if (sig) atomicMin(&s_vals[1], col);
         }
         __syncthreads();
         const int col = s_vals[1];
         if (col == 0x7fffffff) break;
-        int foundBase = -1;
+        int foundBase = -1;                   // the last qualifying base index wins (:591-601)
         {
             const int cs = s_cons[col];
             for (int b = 0; b < 4; ++b) if (b != cs && sigThr <= (int)s_cnt[col][b]) foundBase = b;
         }
-        const int orig = base_at(s_aseq, col - abegin);
+        const int orig = s_aelem[col - abegin] & 3u;
         const bool keepMatching = orig == foundBase;
+        // per candidate: remove? (discard_rows :622-665); veto by weight >= 0.90 (:672-689)
+        auto removes = [&](int b) { return keepMatching ? (b != foundBase) : (b == foundBase); };
         int nrem = 0, veto = 0;
-        for (int k = tid; k < V; k += BLOCK) {
-            const CandRec rc = recs[off + k];
-            const int rb = abegin + rc.shift, re = rb + rc.len;
-            int rem = 0;
-            if (!(col < rb || re <= col)) {
-                const int p = col - rb;
-                const uint32_t* row = r.seq + (size_t)rc.id * r.seq_pitch;
-                const int b = rc.orient == 1 ? (int)base_at(row, p) : (int)(base_at(row, rc.len - 1 - p) ^ 3u);
-                rem = keepMatching ? (b != foundBase) : (b == foundBase);
+        if (persistent) {
+            for (int i = tid; i < nalive; i += BLOCK) {
+                const int k = s_alive[i];
+                const int rb = abegin + s_beg[k], re = rb + s_len[k];
+                const int rem = (col >= rb && col < re) ? removes(s_elem[k * mlen + col - rb] & 3) : 0;
+                nrem += rem;
+                veto |= rem && s_w[k] >= 0.90f;
             }
-            nrem += rem;
-            veto |= rem && rc.weight >= 0.90f;
+        } else {
+            for (int k = tid; k < nalive; k += BLOCK) {
+                const CandRec rc = recs[off + k];
+                const int rb = abegin + rc.shift, re = rb + rc.len;
+                int rem = 0;
+                if (col >= rb && col < re) {
+                    const int p = col - rb;
+                    const uint32_t* row = r.seq + (size_t)rc.id * sp;
+                    rem = removes(rc.orient == 1 ? (int)base_at(row, p) : (int)(base_at(row, rc.len - 1 - p) ^ 3u));
+                }
+                nrem += rem;
+                veto |= rem && rc.weight >= 0.90f;
+            }
         }
         const int anyVeto = __syncthreads_or(veto);
         const int anyRem = __syncthreads_or(nrem);
-        if (anyVeto || !anyRem) break;
-        // ordered compaction of the survivors (recs read before rewrite)
+        if (anyVeto || !anyRem) break;        // nothing removed: the rebuilt MSA would be identical
+        // ordered compaction of the survivors
         int newV = 0;
-        for (int c = 0; c < V; c += BLOCK) {
-            const int k = c + tid;
+        for (int c = 0; c < nalive; c += BLOCK) {
+            const int i = c + tid;
+            int keep = 0, k = 0;
             CandRec rc;
-            int keep = 0;
-            if (k < V) {
-                rc = recs[off + k];
-                const int rb = abegin + rc.shift, re = rb + rc.len;
-                keep = 1;
-                if (!(col < rb || re <= col)) {
-                    const int p = col - rb;
-                    const uint32_t* row = r.seq + (size_t)rc.id * r.seq_pitch;
-                    const int b = rc.orient == 1 ? (int)base_at(row, p) : (int)(base_at(row, rc.len - 1 - p) ^ 3u);
-                    keep = !(keepMatching ? (b != foundBase) : (b == foundBase));
+            if (i < nalive) {
+                if (persistent) {
+                    k = s_alive[i];
+                    const int rb = abegin + s_beg[k], re = rb + s_len[k];
+                    keep = !((col >= rb && col < re) && removes(s_elem[k * mlen + col - rb] & 3));
+                } else {
+                    rc = recs[off + i];
+                    const int rb = abegin + rc.shift, re = rb + rc.len;
+                    keep = 1;
+                    if (col >= rb && col < re) {
+                        const int p = col - rb;
+                        const uint32_t* row = r.seq + (size_t)rc.id * sp;
+                        keep = !removes(rc.orient == 1 ? (int)base_at(row, p) : (int)(base_at(row, rc.len - 1 - p) ^ 3u));
+                    }
                 }
             }
             int tot;
             const int pre = block_scan(keep, &tot);
             __syncthreads();
-            if (keep) recs[off + newV + pre] = rc;
+            if (keep) {
+                if (persistent) s_alive[newV + pre] = (uint8_t)k;
+                else recs[off + newV + pre] = rc;
+            }
             newV += tot;
             __syncthreads();
         }
-        V = newV;
+        nalive = newV;
         __syncthreads();
     }
+    V = nalive;
 
-    // ---- MSA properties (getMSAProperties) ----
+    // ---- MSA properties (getMSAProperties, msa.cpp:304-376) ----
     {
         float mnS = 3.402823466e+38f;
         int mnC = 0x7fffffff;
@@ -629,26 +712,26 @@ k_msa(DevOptions o, DevReads r, uint32_t first, uint32_t count, const uint32_t* 
         if (tid == 0) {
             float minSup = 3.402823466e+38f;
             int minCov = 0x7fffffff;
-            for (int w = 0; w < NW; ++w) { minSup = fminf(minSup, __int_as_float(s_red[w][0])); minCov = min(minCov, s_red[w][1]); }
-            float sum = 0.0f;
+            for (int w = 0; w < NWARP; ++w) { minSup = fminf(minSup, __int_as_float(s_red[w][0])); minCov = min(minCov, s_red[w][1]); }
+            float sum = 0.0f;                 // std::accumulate order
             for (int p = 0; p < La; ++p) sum = __fadd_rn(sum, s_support[abegin + p]);
-            const float avgSup = __fdiv_rn(sum, (float)La);
+            const float avgSup = fdiv_rn(sum, (float)La);
             const float e = o.estimated_errorrate;
-            const float avgThr = __fsub_rn(1.0f, __fmul_rn(1.0f, e));
-            const float minThr = __fsub_rn(1.0f, __fmul_rn(3.0f, e));
-            const float covThr = __fmul_rn(__fdiv_rn(o.m_coverage, 6.0f), o.estimated_coverage);
+            const float avgThr = fsub_rn(1.0f, fmul_rn(1.0f, e));
+            const float minThr = fsub_rn(1.0f, fmul_rn(3.0f, e));
+            const float covThr = fmul_rn(fdiv_rn(o.m_coverage, 6.0f), o.estimated_coverage);
             const bool good = fgeq(avgSup, avgThr) && fgeq(minSup, minThr) && fgeq((float)minCov, covThr);
             bool isHQ = false;
             if (good) {
                 int smallest = 100;
-                const int pct = (int)ceilf(__fmul_rn(e, 100.0f));
+                const int pct = (int)ceilf(fmul_rn(e, 100.0f));
                 for (int pc = pct; pc >= 0; --pc) {
-                    const float fac = __fdiv_rn((float)pc, 100.0f);
-                    const float at = __fsub_rn(1.0f, __fmul_rn(1.0f, fac));
-                    const float mt = __fsub_rn(1.0f, __fmul_rn(3.0f, fac));
+                    const float fac = fdiv_rn((float)pc, 100.0f);
+                    const float at = fsub_rn(1.0f, fmul_rn(1.0f, fac));
+                    const float mt = fsub_rn(1.0f, fmul_rn(3.0f, fac));
                     if (fgeq(avgSup, at) && fgeq(minSup, mt)) smallest = pc;
                 }
-                isHQ = fgeq((float)minCov, covThr) && fleq((float)smallest, __fmul_rn((float)pct, 0.5f));
+                isHQ = fgeq((float)minCov, covThr) && fleq((float)smallest, fmul_rn((float)pct, 0.5f));
             }
             s_vals[4] = good;
             s_vals[5] = isHQ;
@@ -658,7 +741,7 @@ k_msa(DevOptions o, DevReads r, uint32_t first, uint32_t count, const uint32_t* 
         hq = s_vals[5];
     }
 
-    // ---- anchor correction (getCorrectedAnchor) ----
+    // ---- anchor correction (getCorrectedAnchor, msa.cpp:379-453) ----
     if (V == 0) {
         if (tid == 0) { out.status[ai] = 0; out.nedits[ai] = 0; }
         return;   // nCandidates == 0: not corrected; no candidate corrections either
@@ -666,7 +749,7 @@ k_msa(DevOptions o, DevReads r, uint32_t first, uint32_t count, const uint32_t* 
     int diffs = 0;
     for (int p = tid; p < La; p += BLOCK) {
         const int col = abegin + p;
-        const uint32_t ob = base_at(s_aseq, p);
+        const uint32_t ob = s_aelem[p] & 3u;
         uint32_t cb;
         if (allGood) cb = s_cons[col];
         else {
@@ -685,36 +768,36 @@ k_msa(DevOptions o, DevReads r, uint32_t first, uint32_t count, const uint32_t* 
         out.nedits[ai] = useEdits ? nd : 0;
     }
 
-    // ---- candidate correction (getCorrectedCandidates) ----
+    // ---- candidate correction (getCorrectedCandidates, msa.cpp:457-522) ----
     if (hq && o.correct_candidates) {
         const int ncc = o.new_columns;
-        for (int k = tid; k < V; k += BLOCK) {
-            const CandRec rc = recs[off + k];
-            const int qb = abegin + rc.shift;
-            const int qe = qb + rc.len;
+        for (int i = tid; i < V; i += BLOCK) {
+            uint32_t id; int shift, L; bool fwd;
+            if (persistent) {
+                const int k = s_alive[i];
+                id = s_id[k]; shift = s_beg[k]; L = s_len[k]; fwd = s_fwd[k];
+            } else {
+                const CandRec rc = recs[off + i];
+                id = rc.id; shift = rc.shift; L = rc.len; fwd = rc.orient == 1;
+            }
+            const int qb = abegin + shift;
+            const int qe = qb + L;
             if (!(abegin - ncc <= qb && qb <= abegin + ncc && qe <= aend + ncc)) continue;
             const unsigned long long slot = atomicAdd(out.corr_count, 1ull);
             if (slot >= out.corr_cap) { atomicOr(status, kStatusCorrOverflow); continue; }
             char* dst = out.corr_seq + slot * mlen;
-            const uint32_t* row = r.seq + (size_t)rc.id * r.seq_pitch;
+            const uint32_t* row = r.seq + (size_t)id * sp;
             int nd = 0;
-            const int L = rc.len;
             for (int p = 0; p < L; ++p) {
                 // forward orientation of the corrected candidate
-                if (rc.orient == 1) {
-                    const uint32_t cs = s_cons[qb + p];
-                    dst[p] = "ACGT"[cs];
-                    nd += cs != base_at(row, p);
-                } else {
-                    const uint32_t cs = s_cons[qb + L - 1 - p] ^ 3u;
-                    dst[p] = "ACGT"[cs];
-                    nd += cs != base_at(row, p);
-                }
+                const uint32_t cs = fwd ? s_cons[qb + p] : (s_cons[qb + L - 1 - p] ^ 3u);
+                dst[p] = "ACGT"[cs];
+                nd += cs != base_at(row, p);
             }
-            out.corr_id[slot] = rc.id;
+            out.corr_id[slot] = id;
             out.corr_anchor[slot] = a;
-            out.corr_shift[slot] = rc.shift;
-            out.corr_use_edits[slot] = (!r.ambig[rc.id] && nd <= L / 7) ? 1 : 0;
+            out.corr_shift[slot] = shift;
+            out.corr_use_edits[slot] = (!r.ambig[id] && nd <= L / 7) ? 1 : 0;
         }
     }
 }

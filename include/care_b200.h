@@ -59,7 +59,8 @@ typedef struct care_b200_ctx care_b200_ctx;
  * anchor_status bits: 1 = corrected, 2 = high quality (HQ) MSA,
  * 4 = store as edit list (the reference's useEdits, corrector.hpp:1648-1675).
  * Candidate corrections are in forward read orientation
- * (corrector.hpp:1679-1757). Sequences are max_length bytes per row. */
+ * (corrector.hpp:1679-1757). Sequences are max_length bytes per row; rows
+ * of anchors that were not corrected are zero. */
 typedef struct care_b200_results {
     uint32_t        first_anchor;
     uint32_t        num_anchors;

@@ -1,0 +1,104 @@
+"""The per-thread device helpers (care_b200/csrc/device.cuh), built for the
+host, against the CPU oracle: shifted Hamming both strands + orientation,
+canonical k-mers, MurmurHash finalizer. Runs without a GPU."""
+import ctypes
+import os
+import random
+import subprocess
+
+import numpy as np
+import pytest
+
+import _oracle
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+SRC = os.path.join(ROOT, "tests", "harness", "device_math.cu")
+OUT = os.path.join(ROOT, "tests", "_build", "libdevice_math.so")
+DEPS = [SRC, os.path.join(ROOT, "care_b200", "csrc", "device.cuh")]
+
+
+def harness():
+    os.makedirs(os.path.dirname(OUT), exist_ok=True)
+    if not os.path.exists(OUT) or any(os.path.getmtime(d) > os.path.getmtime(OUT) for d in DEPS):
+        subprocess.run(["nvcc", "-shared", "-Xcompiler", "-fPIC,-ffp-contract=off", "-O2", "-std=c++17",
+                        "-o", OUT, SRC], check=True, capture_output=True)
+    lib = ctypes.CDLL(OUT)
+    P = ctypes.POINTER
+    lib.hd_shd.argtypes = [P(ctypes.c_uint32), ctypes.c_int, P(ctypes.c_uint32), ctypes.c_int, ctypes.c_int,
+                           ctypes.c_float, ctypes.c_float, ctypes.c_int, P(ctypes.c_int)]
+    lib.hd_canonical_kmers.argtypes = [P(ctypes.c_uint32), ctypes.c_int, ctypes.c_int, P(ctypes.c_uint64)]
+    lib.hd_murmur64.argtypes = [ctypes.c_uint64]
+    lib.hd_murmur64.restype = ctypes.c_uint64
+    return lib
+
+
+H = harness()
+O = _oracle.lib()
+
+
+def enc(s):
+    n = (len(s) + 15) // 16
+    out = (ctypes.c_uint32 * max(n, 1))()
+    O.co_encode_2bit(s.encode(), len(s), out)
+    return out
+
+
+def rc(s):
+    return s[::-1].translate(str.maketrans("ACGT", "TGCA"))
+
+
+def mutate(rng, s, k):
+    s = list(s)
+    for _ in range(k):
+        i = rng.randrange(len(s))
+        s[i] = rng.choice([b for b in "ACGT" if b != s[i]])
+    return "".join(s)
+
+
+@pytest.mark.parametrize("seed", range(300))
+def test_alignment_matches_oracle(seed):
+    rng = random.Random(1000 + seed)
+    La = rng.randint(20, 256)
+    Lc = rng.randint(20, 256)
+    g = "".join(rng.choice("ACGT") for _ in range(800))
+    a0 = rng.randrange(0, 500)
+    a = g[a0:a0 + La]
+    c0 = max(0, a0 + rng.randrange(-Lc + 10, La - 10))
+    c = mutate(rng, g[c0:c0 + Lc], rng.randrange(0, 10))
+    c = (c + "".join(rng.choice("ACGT") for _ in range(Lc)))[:Lc]
+    if seed % 2:
+        c = rc(c)
+    if seed % 7 == 0:
+        c = "".join(rng.choice("ACGT") for _ in range(Lc))          # unrelated read
+    mo = rng.choice([30, 30, 20, 45])
+    mer = rng.choice([0.2, 0.2, 0.1, 0.3])
+    ratio = rng.choice([0.3, 0.3, 0.2])
+    nw = {4: 4, 5: 5, 6: 6, 7: 8, 8: 8}[max(4, (max(La, Lc) + 31) // 32)]
+    out = (ctypes.c_int * 11)()
+    assert H.hd_shd(enc(a), La, enc(c), Lc, mo, mer, ratio, nw, out) == 0
+    f, r = _oracle.CoAlign(), _oracle.CoAlign()
+    O.co_shd(enc(a), La, enc(c), Lc, mo, ctypes.c_float(mer), ctypes.c_float(ratio), ctypes.byref(f))
+    O.co_shd(enc(a), La, enc(rc(c)), Lc, mo, ctypes.c_float(mer), ctypes.c_float(ratio), ctypes.byref(r))
+    assert list(out[0:5]) == [f.score, f.overlap, f.shift, f.nops, f.valid]
+    assert list(out[5:10]) == [r.score, r.overlap, r.shift, r.nops, r.valid]
+    assert out[10] == O.co_orientation(ctypes.byref(f), ctypes.byref(r), La, Lc, ctypes.c_float(ratio), mo,
+                                       ctypes.c_float(0.06))
+
+
+@pytest.mark.parametrize("k", [11, 16, 20, 24, 31, 32])
+def test_canonical_kmers(k):
+    rng = random.Random(k)
+    s = "".join(rng.choice("ACGT") for _ in range(250))
+    out = (ctypes.c_uint64 * 250)()
+    H.hd_canonical_kmers(enc(s), 250, k, out)
+    code = {"A": 0, "C": 1, "G": 2, "T": 3}
+    for p in range(250 - k + 1):
+        km = s[p:p + k]
+        f = int("".join(str(code[x]) for x in km), 4)
+        r = int("".join(str(code[x]) for x in rc(km)), 4)
+        assert out[p] == min(f, r)
+
+
+def test_murmur():
+    for x in [0, 1, 7, 2 ** 40 + 3, 2 ** 64 - 1]:
+        assert H.hd_murmur64(x) == O.co_murmur64(x)
