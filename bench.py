@@ -47,7 +47,9 @@ L2_BYTES = 126 * 1024 * 1024
 
 def workload(rank: int, genome_size: int):
     from care_b200 import datagen
-    rs = datagen.paired_end_repeats(seed=2 + 1000 * rank, genome_size=genome_size)
+    # 2% of the genome in 20 copies of one repeat unit (5 kbp at 5 Mbp)
+    rs = datagen.paired_end_repeats(seed=2 + 1000 * rank, genome_size=genome_size,
+                                    repeat_unit=max(100, genome_size // 1000))
     return rs
 
 
