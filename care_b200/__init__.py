@@ -74,7 +74,26 @@ EXPORTS = [
     "care_b200_correct_range_device", "care_b200_serialize_results",
     "care_b200_load_reads_from_files", "care_b200_write_output", "care_b200_last_timing",
     "care_b200_last_stats", "care_b200_num_reads", "care_b200_max_length", "care_b200_num_maps",
+    "care_b200_correct_range_noalloc",
 ]
+
+NOALLOC_MAX_ANCHORS = 16384
+NOALLOC_MAX_PAIRS = 1048576
+
+
+class DeviceReads(ctypes.Structure):
+    """care_b200_device_reads: caller-owned device read storage."""
+    _fields_ = [
+        ("packed", ctypes.c_void_p), ("pitch_ints", ctypes.c_size_t), ("lengths", ctypes.c_void_p),
+        ("quals", ctypes.c_void_p), ("qual_pitch_ints", ctypes.c_size_t), ("ambiguous", ctypes.c_void_p),
+        ("num_reads", ctypes.c_uint32), ("max_length", ctypes.c_int),
+    ]
+
+
+class DeviceTables(ctypes.Structure):
+    """care_b200_device_tables: caller-owned device minhash tables."""
+    _fields_ = [("num_maps", ctypes.c_int), ("descs", ctypes.c_void_p), ("slots", ctypes.c_void_p),
+                ("values", ctypes.c_void_p)]
 
 _lib = None
 
@@ -110,6 +129,9 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.care_b200_write_output.argtypes = [c_ctx, ctypes.c_char_p]
     lib.care_b200_last_timing.argtypes = [c_ctx, P(ctypes.c_float), P(ctypes.c_float), ctypes.c_int]
     lib.care_b200_last_stats.argtypes = [c_ctx, P(ctypes.c_uint64), ctypes.c_int]
+    lib.care_b200_correct_range_noalloc.argtypes = [P(Options), P(DeviceReads), P(DeviceTables), ctypes.c_uint32,
+                                                     ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p,
+                                                     ctypes.c_void_p, ctypes.c_void_p]
     lib.care_b200_num_reads.argtypes = [c_ctx]
     lib.care_b200_num_reads.restype = ctypes.c_uint32
     lib.care_b200_max_length.argtypes = [c_ctx]
@@ -300,6 +322,62 @@ class Corrector:
         st = (ctypes.c_float * 3)()
         self._check(self.lib.care_b200_last_timing(self._ctx, ctypes.byref(t), st, 3), "last_timing")
         return t.value, list(st)
+
+
+def fmix64(x: np.ndarray) -> np.ndarray:
+    """MurmurHash3's 64-bit finalizer over a uint64 array."""
+    x = x.copy()
+    with np.errstate(over="ignore"):
+        x ^= x >> np.uint64(33)
+        x *= np.uint64(0xff51afd7ed558ccd)
+        x ^= x >> np.uint64(33)
+        x *= np.uint64(0xc4ceb9fe1a85ec53)
+        x ^= x >> np.uint64(33)
+    return x
+
+
+def table_device_layout(tables):
+    """Host arrays in the device table layout of care_b200_device_tables:
+    (descs bytes, slots bytes, values uint32) from per-map (keys, offsets,
+    values). Slots: power-of-two capacity >= 2 keys, linear probing from the
+    MurmurHash3 fmix64 of the key."""
+    descs, slots, vals = [], [], []
+    slot_base = value_base = 0
+    sdt = np.dtype([("key", "<u8"), ("offset", "<u4"), ("count", "<u4")])
+    ddt = np.dtype([("slot_base", "<u8"), ("value_base", "<u8"), ("mask", "<u4"), ("pad", "<u4")])
+    for keys, offs, values in tables:
+        n = keys.shape[0]
+        cap = 16
+        while cap < 2 * n:
+            cap <<= 1
+        s = np.zeros(cap, sdt)
+        h = fmix64(keys.astype(np.uint64)) & np.uint64(cap - 1)
+        for i in range(n):
+            pos = int(h[i])
+            while s["count"][pos] != 0:
+                pos = (pos + 1) & (cap - 1)
+            s[pos] = (keys[i], offs[i], offs[i + 1] - offs[i])
+        d = np.zeros(1, ddt)
+        d[0] = (slot_base, value_base, cap - 1, 0)
+        descs.append(d)
+        slots.append(s)
+        vals.append(values.astype(np.uint32))
+        slot_base += cap
+        value_base += values.shape[0]
+    return (np.concatenate(descs).tobytes(), np.concatenate(slots).tobytes(),
+            np.concatenate(vals) if vals else np.zeros(0, np.uint32))
+
+
+def correct_range_noalloc(options: Options, reads: DeviceReads, tables: DeviceTables, first: int, count: int,
+                          status_ptr: int, num_edits_ptr: int, sequences_ptr: int, stream: int = 0) -> None:
+    """care_b200_correct_range_noalloc: anchor correction into caller-owned
+    device buffers, for callers that cannot allocate device memory; the
+    library allocates nothing here either."""
+    lib = load_library()
+    rc = lib.care_b200_correct_range_noalloc(ctypes.byref(options), ctypes.byref(reads), ctypes.byref(tables),
+                                             first, count, status_ptr, num_edits_ptr, sequences_ptr, stream)
+    if rc != 0:
+        raise CareError(f"care_b200_correct_range_noalloc failed ({rc})")
 
 
 def encode_reads(seqs: np.ndarray, lengths: np.ndarray):

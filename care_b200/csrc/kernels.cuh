@@ -803,7 +803,7 @@ k_msa(DevOptions o, DevReads r, uint32_t first, uint32_t count, const uint32_t* 
 }
 
 // Signatures of all reads (for table construction): one warp per read.
-__global__ void k_signatures(DevOptions o, DevReads r, uint32_t first, uint32_t count,
+static __global__ void k_signatures(DevOptions o, DevReads r, uint32_t first, uint32_t count,
                              unsigned long long* __restrict__ sig) {
     const int lane = threadIdx.x & 31;
     const uint32_t ri = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);

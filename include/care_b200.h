@@ -159,6 +159,64 @@ int care_b200_last_timing(const care_b200_ctx* ctx, float* total_ms, float* stag
  * (anchor, candidate) pairs aligned, stats[2] candidate corrections. */
 int care_b200_last_stats(const care_b200_ctx* ctx, uint64_t* stats, int nstats);
 
+/* ---- correction without allocation ---- */
+
+/* Device-resident read storage owned by the caller (layout of
+ * care_b200_upload_reads: 2-bit rows, encoded quality rows, lengths, and
+ * one byte per read, nonzero for reads that contained non-ACGT bases). */
+typedef struct care_b200_device_reads {
+    const uint32_t* packed;
+    size_t          pitch_ints;
+    const int32_t*  lengths;
+    const uint32_t* quals;            /* NULL when qualities are not used */
+    size_t          qual_pitch_ints;
+    const uint8_t*  ambiguous;
+    uint32_t        num_reads;
+    int             max_length;       /* longest read of the storage (<= 256) */
+} care_b200_device_reads;
+
+/* Device-resident minhash tables owned by the caller, in the layout this
+ * library builds: per map a descriptor {uint64 slot_base; uint64 value_base;
+ * uint32 mask; uint32 pad} (24 bytes), an open-addressing slot array of
+ * {uint64 key; uint32 offset; uint32 count} (16 bytes; count 0 = empty;
+ * capacity mask+1 a power of two; a key starts probing at
+ * MurmurHash3-fmix64(key) & mask and moves to the next slot), and one value
+ * array of read ids (the key's ids at value_base + offset, ascending). */
+typedef struct care_b200_device_tables {
+    int             num_maps;
+    const void*     descs;
+    const void*     slots;
+    const uint32_t* values;
+} care_b200_device_tables;
+
+#define CARE_B200_NOALLOC_MAX_ANCHORS 16384
+#define CARE_B200_NOALLOC_MAX_PAIRS   1048576
+
+/* Anchor correction of [first_anchor, first_anchor+num_anchors) that
+ * allocates nothing, for callers that cannot call cudaMalloc (buffers laid
+ * out by a host framework's own pool or mapped from another process, or code
+ * that must not change the device's memory map while it runs). No
+ * counterpart in the reference. Inputs and outputs are device pointers the
+ * caller owns: status (1 byte per anchor, same bits as care_b200_results),
+ * num_edits (int32 per anchor) and sequences (max_length bytes per anchor;
+ * rows of uncorrected anchors are zero). Candidate correction is not
+ * available here (opt->correct_candidates must be 0). Work runs on `stream`
+ * (a cudaStream_t, NULL for the default stream) and the call returns when it
+ * has finished.
+ * Working memory is one device array compiled into the library (about 32 MB;
+ * every GPU that loads the library holds it until the process exits): at
+ * most CARE_B200_NOALLOC_MAX_ANCHORS anchors and
+ * CARE_B200_NOALLOC_MAX_PAIRS (anchor, candidate) pairs per call; larger
+ * requests return CARE_B200_ELIMIT. The first call on a device looks up the
+ * array's device address and loads constants, so make it before any stream
+ * capture. All calls share the array: calls that overlap on the GPU (from
+ * several threads or streams) race and must be serialised by the caller.
+ * Returns 0 or a CARE_B200_E* code. */
+int care_b200_correct_range_noalloc(const care_b200_options* opt, const care_b200_device_reads* reads,
+                                    const care_b200_device_tables* tables, uint32_t first_anchor,
+                                    uint32_t num_anchors, uint8_t* status, int32_t* num_edits,
+                                    char* sequences, void* stream);
+
 /* Read-storage facts after upload. */
 uint32_t care_b200_num_reads(const care_b200_ctx* ctx);
 int      care_b200_max_length(const care_b200_ctx* ctx);
