@@ -127,6 +127,25 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
+def host_cores() -> int:
+    """Cores this process may use: the affinity mask, capped by a cgroup CPU
+    quota (a container can see more CPUs than it is allowed to run on)."""
+    n = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+    try:
+        quota, period = open("/sys/fs/cgroup/cpu.max").read().split()[:2]
+        if quota != "max":
+            n = min(n, max(1, int(float(quota) / float(period) + 0.5)))
+    except (OSError, ValueError):
+        try:
+            q = int(open("/sys/fs/cgroup/cpu/cpu.cfs_quota_us").read())
+            p = int(open("/sys/fs/cgroup/cpu/cpu.cfs_period_us").read())
+            if q > 0:
+                n = min(n, max(1, round(q / p)))
+        except (OSError, ValueError):
+            pass
+    return max(1, n)
+
+
 def care_cpu_sample(tmpdir: str, threads: int):
     """care-cpu on the bounded sample; returns reads/s from its STEP2 line."""
     from care_b200 import datagen
@@ -134,8 +153,12 @@ def care_cpu_sample(tmpdir: str, threads: int):
     if not os.path.exists(path):
         rs = datagen.paired_end_repeats(seed=7, genome_size=1_250_000, repeat_unit=1250)
         write_fastq_fast(rs, path)
-    r = subprocess.run([CARE_CPU, "-i", path, "-d", tmpdir, "-o", "sample_out.fq", "-t", str(threads)]
-                       + ARGS.split(), capture_output=True, text=True)
+    cmd = [CARE_CPU, "-i", path, "-d", tmpdir, "-o", "sample_out.fq", "-t", str(threads)] + ARGS.split()
+    try:
+        r = subprocess.run(cmd, capture_output=True, text=True, timeout=180)
+    except subprocess.TimeoutExpired:
+        # one run of this sample takes seconds; a stalled run is retried once
+        r = subprocess.run(cmd, capture_output=True, text=True, timeout=180)
     if r.returncode != 0:
         raise RuntimeError("care-cpu failed: " + r.stderr[-500:])
     m = re.search(r"Correction throughput : ~([0-9.e+]+) reads/second", r.stdout)
@@ -145,7 +168,7 @@ def care_cpu_sample(tmpdir: str, threads: int):
 def run_reference(args, rank, world):
     if rank != 0:
         return
-    threads = os.cpu_count() or 1
+    threads = host_cores()
     cfg = {"workload": "pe_5Mbp_30x_150bp (sample: 1.25 Mbp genome, 250,000 reads, same model)",
            "args": ARGS, "reads_per_step": 250_000, "threads": threads}
     if not os.path.exists(CARE_CPU):
@@ -164,6 +187,14 @@ def run_reference(args, rank, world):
                              "sample": cfg["workload"]},
             "e2e": {"value": v, "unit": "reads/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
+
+
+T0 = time.time()
+
+
+def progress(msg: str) -> None:
+    """Phase marks on stderr (the JSON line stays the only stdout output)."""
+    print(f"[bench {time.time() - T0:7.1f}s] {msg}", file=sys.stderr, flush=True)
 
 
 def main():
@@ -197,6 +228,7 @@ def main():
         torch.cuda.synchronize()
 
     tmp = tempfile.mkdtemp(prefix=f"careb200_bench_{rank}_")
+    progress("generating reads")
     rs = workload(rank, args.genome)
     n = rs.num_reads
     fq = os.path.join(tmp, "reads.fq")
@@ -205,14 +237,17 @@ def main():
     opts = care_b200.options_from_args(ARGS, device=local)
     corr = care_b200.Corrector(opts)
     t0 = time.perf_counter()
+    progress("STEP1: load + tables")
     corr.load_files([fq])
     corr.build_tables()
+    progress("STEP1 done")
     step1_s = time.perf_counter() - t0
 
     flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device=f"cuda:{local}")
 
-    for _ in range(args.warmup):
+    for w in range(args.warmup):
         corr.correct_range_device(0, n)
+        progress(f"warm-up step {w} done")
     barrier()
     with ClockSampler(local) as clk:
         dev_ms, stage = [], np.zeros(3)
@@ -236,6 +271,7 @@ def main():
     stage /= args.steps
     value = world * n / (ms / 1e3)
 
+    progress("timed steps done")
     # e2e through the C ABI from host buffers
     from care_b200 import encode_reads
     packed = np.ascontiguousarray(encode_reads(rs.seqs, rs.lengths))
@@ -293,7 +329,8 @@ def main():
         "clocks": clk.summary(),
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline and os.path.exists(CARE_CPU):
-        threads = os.cpu_count() or 1
+        threads = host_cores()
+        progress(f"e2e done; care-cpu sample on {threads} threads")
         v = care_cpu_sample(tmp, threads)
         line["cpu_baseline"] = {"value": v, "unit": "reads/s", "cores": threads, "kind": "reference",
                                 "sample": "care-cpu -t all cores on 1.25 Mbp genome, 250,000 reads, same model"}

@@ -452,37 +452,40 @@ k_msa(DevOptions o, DevReads r, uint32_t first, uint32_t count, const uint32_t* 
     }
 
     // stage candidate rows [c, c+n) of recs into slots 0..n-1
+    // one warp per candidate row: lanes copy its packed words, then decode
+    // its bases and qualities position by position
     auto stage = [&](int c, int n) {
         __syncthreads();
-        for (int e = tid; e < n * sp; e += BLOCK) {
-            const int k = e / sp, w = e - k * sp;
-            s_rseq[k * sp + w] = __ldg(r.seq + (size_t)recs[off + c + k].id * sp + w);
-        }
-        if (useQ)
-            for (int e = tid; e < n * qp; e += BLOCK) {
-                const int k = e / qp, w = e - k * qp;
-                s_rqual[k * qp + w] = __ldg(r.qual + (size_t)recs[off + c + k].id * qp + w);
+        for (int k = warp; k < n; k += NWARP) {
+            const CandRec rc = recs[off + c + k];
+            const uint32_t* srow = r.seq + (size_t)rc.id * sp;
+            for (int w = lane; w < sp; w += 32) s_rseq[k * sp + w] = __ldg(srow + w);
+            if (useQ) {
+                const uint32_t* qrow = r.qual + (size_t)rc.id * qp;
+                for (int w = lane; w < qp; w += 32) s_rqual[k * qp + w] = __ldg(qrow + w);
             }
-        if (tid < n) {
-            const CandRec rc = recs[off + c + tid];
-            s_beg[tid] = rc.shift;          // relative to the anchor; abegin added per build
-            s_len[tid] = rc.len;
-            s_w[tid] = rc.weight;
-            s_fwd[tid] = rc.orient == 1;
-            s_id[tid] = rc.id;
+            if (lane == 0) {
+                s_beg[k] = rc.shift;            // relative to the anchor; abegin added per build
+                s_len[k] = rc.len;
+                s_w[k] = rc.weight;
+                s_fwd[k] = rc.orient == 1;
+                s_id[k] = rc.id;
+            }
         }
         __syncthreads();
-        for (int e = tid; e < n * mlen; e += BLOCK) {
-            const int k = e / mlen, p = e - k * mlen;
+        for (int k = warp; k < n; k += NWARP) {
             const int L = s_len[k];
-            if (p < L) {
-                const bool fwd = s_fwd[k];
-                const uint32_t b = fwd ? base_at(s_rseq + k * sp, p) : (base_at(s_rseq + k * sp, L - 1 - p) ^ 3u);
+            const bool fwd = s_fwd[k];
+            const uint32_t* srow = s_rseq + k * sp;
+            const uint32_t* qrow = s_rqual + k * qp;
+            uint16_t* erow = s_elem + k * mlen;
+            for (int p = lane; p < L; p += 32) {
+                const uint32_t b = fwd ? base_at(srow, p) : (base_at(srow, L - 1 - p) ^ 3u);
                 // reverse-complement candidates read their qualities reversed
                 // over the whole quality pitch (reverseQualitiesOfRCAlignments,
                 // corrector.hpp:1227-1239)
-                const uint32_t q = useQ ? qual_char(s_rqual + k * qp, fwd ? p : mlen - 1 - p) : 0u;
-                s_elem[k * mlen + p] = (uint16_t)(b | (q << 2));
+                const uint32_t q = useQ ? qual_char(qrow, fwd ? p : mlen - 1 - p) : 0u;
+                erow[p] = (uint16_t)(b | (q << 2));
             }
         }
         __syncthreads();
