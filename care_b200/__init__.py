@@ -46,6 +46,7 @@ class Options(ctypes.Structure):
         ("threads", ctypes.c_int),
         ("device", ctypes.c_int),
         ("batch_size", ctypes.c_int),
+        ("clf_min_coverage", ctypes.c_int),
     ]
 
 
@@ -75,7 +76,30 @@ EXPORTS = [
     "care_b200_load_reads_from_files", "care_b200_write_output", "care_b200_last_timing",
     "care_b200_last_stats", "care_b200_num_reads", "care_b200_max_length", "care_b200_num_maps",
     "care_b200_correct_range_noalloc",
+    "care_b200_set_mlp", "care_b200_collect_features", "care_b200_mlp_default_train_options",
+    "care_b200_mlp_create", "care_b200_mlp_destroy", "care_b200_mlp_last_error", "care_b200_mlp_set_params",
+    "care_b200_mlp_get_params", "care_b200_mlp_init", "care_b200_mlp_set_data", "care_b200_mlp_train",
+    "care_b200_mlp_gradient", "care_b200_mlp_train_step", "care_b200_mlp_forward",
 ]
+
+MLP_FEATURES = 24
+MLP_HIDDEN = 64
+MLP_PARAMS = 5825
+MLP_FLOATS = 5873
+
+
+class Features(ctypes.Structure):
+    """care_b200_features: decision-column rows of the last collect call."""
+    _fields_ = [("count", ctypes.c_uint64), ("x", ctypes.POINTER(ctypes.c_float)),
+                ("read_ids", ctypes.POINTER(ctypes.c_uint32)), ("meta", ctypes.POINTER(ctypes.c_uint32)),
+                ("logits", ctypes.POINTER(ctypes.c_float))]
+
+
+class TrainOptions(ctypes.Structure):
+    """care_b200_mlp_train_options."""
+    _fields_ = [("epochs", ctypes.c_int), ("batch", ctypes.c_int), ("lr", ctypes.c_double),
+                ("beta1", ctypes.c_double), ("beta2", ctypes.c_double), ("eps", ctypes.c_double),
+                ("seed", ctypes.c_uint64)]
 
 NOALLOC_MAX_ANCHORS = 16384
 NOALLOC_MAX_PAIRS = 1048576
@@ -132,6 +156,24 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.care_b200_correct_range_noalloc.argtypes = [P(Options), P(DeviceReads), P(DeviceTables), ctypes.c_uint32,
                                                      ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p,
                                                      ctypes.c_void_p, ctypes.c_void_p]
+    c_mlp = ctypes.c_void_p
+    fp = P(ctypes.c_float)
+    lib.care_b200_set_mlp.argtypes = [c_ctx, fp]
+    lib.care_b200_collect_features.argtypes = [c_ctx, ctypes.c_uint32, ctypes.c_uint32, P(Results), P(Features)]
+    lib.care_b200_mlp_default_train_options.argtypes = [P(TrainOptions)]
+    lib.care_b200_mlp_default_train_options.restype = None
+    lib.care_b200_mlp_create.argtypes = [ctypes.c_int, P(c_mlp)]
+    lib.care_b200_mlp_destroy.argtypes = [c_mlp]
+    lib.care_b200_mlp_last_error.argtypes = [c_mlp]
+    lib.care_b200_mlp_last_error.restype = ctypes.c_char_p
+    lib.care_b200_mlp_set_params.argtypes = [c_mlp, fp]
+    lib.care_b200_mlp_get_params.argtypes = [c_mlp, fp]
+    lib.care_b200_mlp_init.argtypes = [c_mlp, ctypes.c_uint64]
+    lib.care_b200_mlp_set_data.argtypes = [c_mlp, fp, fp, fp, ctypes.c_uint64, ctypes.c_int]
+    lib.care_b200_mlp_train.argtypes = [c_mlp, P(TrainOptions), fp, ctypes.c_uint64, P(ctypes.c_uint64)]
+    lib.care_b200_mlp_gradient.argtypes = [c_mlp, fp, fp, fp, ctypes.c_uint64, fp, fp]
+    lib.care_b200_mlp_train_step.argtypes = [c_mlp, fp, fp, fp, ctypes.c_uint64, P(TrainOptions), fp]
+    lib.care_b200_mlp_forward.argtypes = [c_mlp, fp, ctypes.c_uint64, fp]
     lib.care_b200_num_reads.argtypes = [c_ctx]
     lib.care_b200_num_reads.restype = ctypes.c_uint32
     lib.care_b200_max_length.argtypes = [c_ctx]
@@ -312,16 +354,164 @@ class Corrector:
     def write_output(self, path: str):
         self._check(self.lib.care_b200_write_output(self._ctx, path.encode()), "write_output")
 
+    # -- learned decision ------------------------------------------------------
+    def set_mlp(self, params: np.ndarray):
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        if p.shape != (MLP_FLOATS,):
+            raise ValueError(f"expected {MLP_FLOATS} parameters")
+        self._check(self.lib.care_b200_set_mlp(self._ctx, _ptr(p, ctypes.c_float)), "set_mlp")
+
+    def collect_features(self, first: int = 0, count: int | None = None):
+        """Correction of the range plus its decision-column rows: dict of
+        read_id, pos, orig, cons (2-bit codes), x (n, 24) and logit (None
+        under the classic rule)."""
+        if count is None:
+            count = self.num_reads - first
+        res = Results()
+        f = Features()
+        self._check(self.lib.care_b200_collect_features(self._ctx, first, count, ctypes.byref(res),
+                                                        ctypes.byref(f)), "collect_features")
+        n = int(f.count)
+        if n == 0:
+            return {"read_id": np.zeros(0, np.uint32), "pos": np.zeros(0, np.int32), "orig": np.zeros(0, np.uint8),
+                    "cons": np.zeros(0, np.uint8), "x": np.zeros((0, MLP_FEATURES), np.float32),
+                    "logit": None if not f.logits else np.zeros(0, np.float32)}
+        meta = np.ctypeslib.as_array(f.meta, shape=(n,)).copy()
+        return {
+            "read_id": np.ctypeslib.as_array(f.read_ids, shape=(n,)).copy(),
+            "pos": (meta & 0xFFFF).astype(np.int32),
+            "orig": ((meta >> 16) & 3).astype(np.uint8),
+            "cons": ((meta >> 18) & 3).astype(np.uint8),
+            "x": np.ctypeslib.as_array(f.x, shape=(n, MLP_FEATURES)).copy(),
+            "logit": np.ctypeslib.as_array(f.logits, shape=(n,)).copy() if f.logits else None,
+        }
+
     def last_stats(self):
         st = (ctypes.c_uint64 * 3)()
         self._check(self.lib.care_b200_last_stats(self._ctx, st, 3), "last_stats")
         return {"anchors": st[0], "pairs": st[1], "candidate_corrections": st[2]}
 
     def last_timing(self):
+        """(total ms, [candidates, alignment, MSA, classifier] ms) of the last call."""
         t = ctypes.c_float()
-        st = (ctypes.c_float * 3)()
-        self._check(self.lib.care_b200_last_timing(self._ctx, ctypes.byref(t), st, 3), "last_timing")
+        st = (ctypes.c_float * 4)()
+        self._check(self.lib.care_b200_last_timing(self._ctx, ctypes.byref(t), st, 4), "last_timing")
         return t.value, list(st)
+
+
+def train_options(**kw) -> TrainOptions:
+    o = TrainOptions()
+    load_library().care_b200_mlp_default_train_options(ctypes.byref(o))
+    for k, v in kw.items():
+        if not hasattr(o, k):
+            raise TypeError(f"unknown training option {k}")
+        setattr(o, k, v)
+    return o
+
+
+class Mlp:
+    """The decision network on one device: parameters, resident training
+    rows, Adam training (one CUDA graph per run), gradients and logits."""
+
+    def __init__(self, device: int = 0, seed: int = 1):
+        self.lib = load_library()
+        self._h = ctypes.c_void_p()
+        rc = self.lib.care_b200_mlp_create(device, ctypes.byref(self._h))
+        if rc != 0:
+            raise CareError(f"care_b200_mlp_create failed ({rc})")
+        if seed != 1:
+            self._check(self.lib.care_b200_mlp_init(self._h, seed), "mlp_init")
+
+    def close(self):
+        if self._h:
+            self.lib.care_b200_mlp_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc: int, what: str):
+        if rc != 0:
+            raise CareError(f"{what} failed ({rc}): {self.lib.care_b200_mlp_last_error(self._h).decode()}")
+
+    @property
+    def params(self) -> np.ndarray:
+        p = np.zeros(MLP_FLOATS, np.float32)
+        self._check(self.lib.care_b200_mlp_get_params(self._h, _ptr(p, ctypes.c_float)), "mlp_get_params")
+        return p
+
+    @params.setter
+    def params(self, p: np.ndarray):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        if p.shape != (MLP_FLOATS,):
+            raise ValueError(f"expected {MLP_FLOATS} parameters")
+        self._check(self.lib.care_b200_mlp_set_params(self._h, _ptr(p, ctypes.c_float)), "mlp_set_params")
+
+    @staticmethod
+    def _rows(x, y=None, w=None):
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        if x.ndim != 2 or x.shape[1] != MLP_FEATURES:
+            raise ValueError("rows must be (n, 24)")
+        out = [x]
+        for v in (y, w):
+            if v is not None:
+                v = np.ascontiguousarray(v, dtype=np.float32)
+                if v.shape != (x.shape[0],):
+                    raise ValueError("one label and one weight per row")
+            out.append(v)
+        return out
+
+    @staticmethod
+    def _fp(a):
+        return None if a is None else _ptr(a, ctypes.c_float)
+
+    def set_data(self, x, y, weights=None, normalise: bool = True):
+        x, y, w = self._rows(x, y, weights)
+        self._check(self.lib.care_b200_mlp_set_data(self._h, _ptr(x, ctypes.c_float), _ptr(y, ctypes.c_float),
+                                                    self._fp(w), x.shape[0], 1 if normalise else 0), "mlp_set_data")
+
+    def train(self, **kw) -> np.ndarray:
+        o = train_options(**kw)
+        n = ctypes.c_uint64()
+        cap = 1 << 20
+        losses = np.zeros(cap, np.float32)
+        self._check(self.lib.care_b200_mlp_train(self._h, ctypes.byref(o), _ptr(losses, ctypes.c_float), cap,
+                                                 ctypes.byref(n)), "mlp_train")
+        return losses[:min(n.value, cap)].copy()
+
+    def gradient(self, x, y, weights=None):
+        x, y, w = self._rows(x, y, weights)
+        g = np.zeros(MLP_PARAMS, np.float32)
+        loss = ctypes.c_float()
+        self._check(self.lib.care_b200_mlp_gradient(self._h, _ptr(x, ctypes.c_float), _ptr(y, ctypes.c_float),
+                                                    self._fp(w), x.shape[0], _ptr(g, ctypes.c_float),
+                                                    ctypes.byref(loss)), "mlp_gradient")
+        return float(loss.value), g
+
+    def train_step(self, x, y, weights=None, **kw) -> float:
+        x, y, w = self._rows(x, y, weights)
+        o = train_options(**kw)
+        loss = ctypes.c_float()
+        self._check(self.lib.care_b200_mlp_train_step(self._h, _ptr(x, ctypes.c_float), _ptr(y, ctypes.c_float),
+                                                      self._fp(w), x.shape[0], ctypes.byref(o), ctypes.byref(loss)),
+                    "mlp_train_step")
+        return float(loss.value)
+
+    def forward(self, x) -> np.ndarray:
+        x = self._rows(x)[0]
+        out = np.zeros(x.shape[0], np.float32)
+        self._check(self.lib.care_b200_mlp_forward(self._h, _ptr(x, ctypes.c_float), x.shape[0],
+                                                   _ptr(out, ctypes.c_float)), "mlp_forward")
+        return out
 
 
 def fmix64(x: np.ndarray) -> np.ndarray:

@@ -3,6 +3,7 @@
 #include "../../include/care_b200.h"
 #include "hostio.hpp"
 #include "kernels.cuh"
+#include "mlp.hpp"
 
 #include <algorithm>
 #include <cmath>
@@ -66,8 +67,8 @@ struct care_b200_ctx {
     care_b200_options opt{};
     std::string err;
     cudaStream_t stream = nullptr;
-    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
-    float last_ms = 0.f, stage_ms[3] = {0.f, 0.f, 0.f};
+    cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    float last_ms = 0.f, stage_ms[4] = {0.f, 0.f, 0.f, 0.f};
 
     // read storage
     uint32_t n = 0;
@@ -94,6 +95,15 @@ struct care_b200_ctx {
     DBuf d_cid, d_canc, d_cshift, d_cue, d_cseq;
     unsigned long long corr_cap = 0;
     HBuf h_small;
+
+    // learned decision: parameters, decision-column rows of a batch
+    DBuf d_mlp, d_mlp_err;
+    bool mlp_set = false;
+    bool collect = false;             // keep the rows of the current call
+    DBuf d_fx, d_fread, d_fmeta, d_flogit, d_touched;
+    unsigned long long feat_cap = 0;
+    std::vector<float> r_fx, r_flogit;
+    std::vector<uint32_t> r_fread, r_fmeta;
 
     // results of the last call (pinned host)
     HBuf r_status, r_nedits, r_seq;
@@ -135,6 +145,8 @@ DevOptions make_dev_options(const care_b200_ctx* ctx) {
     d.threshold = ctx->threshold;
     d.coverage_int = (int)o.estimated_coverage;
     d.correction_type = o.correction_type;
+    d.clf_mode = o.correction_type == 1 ? 2 : (ctx->collect ? 1 : 0);
+    d.clf_min_coverage = o.clf_min_coverage;
     d.max_error_rate = o.max_error_rate;
     d.min_overlap_ratio = o.min_overlap_ratio;
     d.estimated_errorrate = o.estimated_errorrate;
@@ -186,6 +198,7 @@ int validate_options(care_b200_ctx* ctx, const care_b200_options& o) {
     if (o.kmerlength < 1 || o.kmerlength > 32) return fail(ctx, CARE_B200_EINVAL, "kmer length must be in [1,32]");
     if (o.quality_bits != 1 && o.quality_bits != 2 && o.quality_bits != 8) return fail(ctx, CARE_B200_EINVAL, "qualityScoreBits must be 1, 2 or 8");
     if (o.correction_type != 0 && o.correction_type != 1) return fail(ctx, CARE_B200_EINVAL, "correction_type must be 0 or 1");
+    if (o.clf_min_coverage < 0) return fail(ctx, CARE_B200_EINVAL, "clf_min_coverage must be >= 0");
     return CARE_B200_OK;
 }
 
@@ -209,6 +222,7 @@ void care_b200_default_options(care_b200_options* o) {
     o->quality_bits = 8;
     o->threads = 0;
     o->device = 0;
+    o->clf_min_coverage = 3;
 }
 
 int care_b200_create(const care_b200_options* opt, care_b200_ctx** out) {
@@ -443,6 +457,12 @@ int run_batch(care_b200_ctx* ctx, uint32_t first, uint32_t count, bool timed) {
     CK(ctx->h_small.ensure(64), "alloc");
     if (ctx->cand_cap < (unsigned long long)count * 96) ctx->cand_cap = (unsigned long long)count * 96;
     if (ctx->corr_cap == 0) ctx->corr_cap = ctx->opt.correct_candidates ? (unsigned long long)count * 16 + 1024 : 1024;
+    const bool emit = o.clf_mode != 0;
+    if (emit) {
+        if (ctx->feat_cap < (unsigned long long)count / 2 + 4096) ctx->feat_cap = (unsigned long long)count / 2 + 4096;
+        CK(ctx->d_touched.ensure(count), "alloc");
+        CK(ctx->d_mlp_err.ensure(16), "alloc");
+    }
 
     for (int attempt = 0; attempt < 8; ++attempt) {
         const unsigned long long cap = ctx->cand_cap;
@@ -456,6 +476,15 @@ int run_batch(care_b200_ctx* ctx, uint32_t first, uint32_t count, bool timed) {
         CK(ctx->d_cshift.ensure(ccap * 4), "alloc");
         CK(ctx->d_cue.ensure(ccap), "alloc");
         CK(ctx->d_cseq.ensure(ccap * ctx->max_len), "alloc");
+        const unsigned long long fcap = ctx->feat_cap;
+        if (emit) {
+            CK(ctx->d_fx.ensure(fcap * kNumFeatures * 4), "alloc decision rows");
+            CK(ctx->d_fread.ensure(fcap * 4), "alloc decision rows");
+            CK(ctx->d_fmeta.ensure(fcap * 4), "alloc decision rows");
+            CK(ctx->d_flogit.ensure(fcap * 4), "alloc decision rows");
+            CK(cudaMemsetAsync(ctx->d_touched.p, 0, count, ctx->stream), "memset");
+            CK(cudaMemsetAsync(ctx->d_mlp_err.p, 0, 16, ctx->stream), "memset");
+        }
 
         unsigned long long* counters = ctx->d_counters.as<unsigned long long>();
         int* status = ctx->d_status.as<int>();
@@ -496,6 +525,11 @@ int run_batch(care_b200_ctx* ctx, uint32_t first, uint32_t count, bool timed) {
         mo.corr_seq = ctx->d_cseq.as<char>();
         mo.corr_count = counters + 1;
         mo.corr_cap = ccap;
+        mo.feat = emit ? ctx->d_fx.as<float>() : nullptr;
+        mo.feat_read = emit ? ctx->d_fread.as<uint32_t>() : nullptr;
+        mo.feat_meta = emit ? ctx->d_fmeta.as<uint32_t>() : nullptr;
+        mo.feat_count = counters + 2;
+        mo.feat_cap = emit ? fcap : 0;
         // widest possible MSA: La + 2*Lmax - 2*minoverlap(La), maximised over La
         int maxcols = 1;
         for (int la = 1; la <= ctx->max_len; ++la) {
@@ -504,15 +538,20 @@ int run_batch(care_b200_ctx* ctx, uint32_t first, uint32_t count, bool timed) {
             maxcols = std::max(maxcols, la + 2 * ctx->max_len - 2 * std::min(mo, ctx->max_len));
         }
         const int jb = (maxcols + 32 * (kMsaBlock / 32) - 1) / (32 * (kMsaBlock / 32));
-        const size_t msmem = msa_smem_bytes(ctx->max_len, ctx->seq_pitch, ctx->has_qual ? ctx->qual_pitch : 0);
-#define LAUNCH_MSA(JB)                                                                                  \
+        const size_t msmem = msa_smem_bytes(ctx->max_len, ctx->seq_pitch, ctx->has_qual ? ctx->qual_pitch : 0, emit);
+#define LAUNCH_MSA_E(JB, E)                                                                             \
     do {                                                                                                \
-        CK(cudaFuncSetAttribute(k_msa<kMsaBlock, JB>, cudaFuncAttributeMaxDynamicSharedMemorySize,       \
+        CK(cudaFuncSetAttribute(k_msa<kMsaBlock, JB, E>, cudaFuncAttributeMaxDynamicSharedMemorySize,    \
                                 (int)msmem), "smem attr");                                              \
-        k_msa<kMsaBlock, JB><<<count, kMsaBlock, msmem, ctx->stream>>>(                                 \
+        k_msa<kMsaBlock, JB, E><<<count, kMsaBlock, msmem, ctx->stream>>>(                              \
             o, r, first, count, nullptr, ctx->d_cand_ids.as<uint32_t>(), ctx->d_seg_off.as<uint32_t>(), \
             ctx->d_seg_cnt.as<uint32_t>(), ctx->d_ares.as<AlignRes>(), ctx->d_recs.as<CandRec>(), mo,   \
             status);                                                                                    \
+    } while (0)
+#define LAUNCH_MSA(JB)                          \
+    do {                                        \
+        if (emit) LAUNCH_MSA_E(JB, true);       \
+        else LAUNCH_MSA_E(JB, false);           \
     } while (0)
         if (jb <= 1) LAUNCH_MSA(1);
         else if (jb <= 2) LAUNCH_MSA(2);
@@ -521,26 +560,65 @@ int run_batch(care_b200_ctx* ctx, uint32_t first, uint32_t count, bool timed) {
         else if (jb <= 5) LAUNCH_MSA(5);
         else LAUNCH_MSA(6);
 #undef LAUNCH_MSA
+#undef LAUNCH_MSA_E
         CK(cudaGetLastError(), "k_msa");
         if (timed) CK(cudaEventRecord(ctx->ev[3], ctx->stream), "event");
-        CK(cudaMemcpyAsync(ctx->h_small.p, counters, 16, cudaMemcpyDeviceToHost, ctx->stream), "counters");
-        CK(cudaMemcpyAsync(ctx->h_small.as<char>() + 16, status, 4, cudaMemcpyDeviceToHost, ctx->stream), "status");
+        if (o.clf_mode == 2) {
+            // the network decides the batch's decision columns (row count
+            // read on the device), then the changed anchors' edit counts
+            CK(mlp_infer(ctx->d_mlp.as<float>(), ctx->d_fx.as<float>(), fcap, counters + 2,
+                         ctx->d_flogit.as<float>(), ctx->d_mlp_err.as<int>(), ctx->stream), "k_mlp_infer");
+            int sms = 148;
+            CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->opt.device), "attr");
+            k_clf_apply<<<sms * 4, 256, 0, ctx->stream>>>(ctx->d_fread.as<uint32_t>(), ctx->d_fmeta.as<uint32_t>(),
+                                                          ctx->d_flogit.as<float>(), counters + 2, fcap, first,
+                                                          ctx->max_len, ctx->d_oseq.as<char>(), ctx->d_touched.as<uint8_t>());
+            CK(cudaGetLastError(), "k_clf_apply");
+            k_clf_recount<<<(count + 7) / 8, 256, 0, ctx->stream>>>(r, first, count, ctx->d_touched.as<uint8_t>(),
+                                                                   ctx->d_oseq.as<char>(), ctx->d_st.as<uint8_t>(),
+                                                                   ctx->d_ned.as<int32_t>());
+            CK(cudaGetLastError(), "k_clf_recount");
+        }
+        if (timed) CK(cudaEventRecord(ctx->ev[4], ctx->stream), "event");
+        CK(cudaMemcpyAsync(ctx->h_small.p, counters, 24, cudaMemcpyDeviceToHost, ctx->stream), "counters");
+        CK(cudaMemcpyAsync(ctx->h_small.as<char>() + 32, status, 4, cudaMemcpyDeviceToHost, ctx->stream), "status");
+        if (o.clf_mode == 2)
+            CK(cudaMemcpyAsync(ctx->h_small.as<char>() + 36, ctx->d_mlp_err.p, 4, cudaMemcpyDeviceToHost, ctx->stream), "status");
         CK(cudaStreamSynchronize(ctx->stream), "batch");
         const unsigned long long used = ctx->h_small.as<unsigned long long>()[0];
         const unsigned long long corr = ctx->h_small.as<unsigned long long>()[1];
-        const int st = *(int*)(ctx->h_small.as<char>() + 16);
+        const unsigned long long nfeat = ctx->h_small.as<unsigned long long>()[2];
+        const int st = *(int*)(ctx->h_small.as<char>() + 32);
         if (st & kStatusColumns) return fail(ctx, CARE_B200_ELIMIT, "MSA wider than the kernel's column capacity");
         bool again = false;
         if ((st & kStatusCandOverflow) || used > cap) { ctx->cand_cap = used + used / 8 + 1024; again = true; }
         if ((st & kStatusCorrOverflow) || corr > ccap) { ctx->corr_cap = corr + corr / 8 + 1024; again = true; }
+        if (emit && ((st & kStatusFeatOverflow) || nfeat > fcap)) { ctx->feat_cap = nfeat + nfeat / 8 + 4096; again = true; }
         if (again) continue;
+        if (o.clf_mode == 2 && *(int*)(ctx->h_small.as<char>() + 36))
+            return fail(ctx, CARE_B200_ECUDA, "tensor-core completion wait ran out");
         if (timed) {
-            float a = 0, b = 0, c = 0;
+            float a = 0, b = 0, c = 0, d = 0;
             cudaEventElapsedTime(&a, ctx->ev[0], ctx->ev[1]);
             cudaEventElapsedTime(&b, ctx->ev[1], ctx->ev[2]);
             cudaEventElapsedTime(&c, ctx->ev[2], ctx->ev[3]);
-            ctx->stage_ms[0] += a; ctx->stage_ms[1] += b; ctx->stage_ms[2] += c;
-            ctx->last_ms += a + b + c;
+            cudaEventElapsedTime(&d, ctx->ev[3], ctx->ev[4]);
+            ctx->stage_ms[0] += a; ctx->stage_ms[1] += b; ctx->stage_ms[2] += c; ctx->stage_ms[3] += d;
+            ctx->last_ms += a + b + c + d;
+        }
+        if (emit && ctx->collect && nfeat) {
+            const size_t b0 = ctx->r_fread.size();
+            ctx->r_fx.resize((b0 + nfeat) * kNumFeatures);
+            ctx->r_fread.resize(b0 + nfeat);
+            ctx->r_fmeta.resize(b0 + nfeat);
+            CK(cudaMemcpyAsync(ctx->r_fx.data() + b0 * kNumFeatures, ctx->d_fx.p, nfeat * kNumFeatures * 4, cudaMemcpyDeviceToHost, ctx->stream), "rows");
+            CK(cudaMemcpyAsync(ctx->r_fread.data() + b0, ctx->d_fread.p, nfeat * 4, cudaMemcpyDeviceToHost, ctx->stream), "rows");
+            CK(cudaMemcpyAsync(ctx->r_fmeta.data() + b0, ctx->d_fmeta.p, nfeat * 4, cudaMemcpyDeviceToHost, ctx->stream), "rows");
+            if (o.clf_mode == 2) {
+                ctx->r_flogit.resize(b0 + nfeat);
+                CK(cudaMemcpyAsync(ctx->r_flogit.data() + b0, ctx->d_flogit.p, nfeat * 4, cudaMemcpyDeviceToHost, ctx->stream), "rows");
+            }
+            CK(cudaStreamSynchronize(ctx->stream), "rows");
         }
         ctx->r_ncand += corr;
         ctx->r_pairs += used;
@@ -555,12 +633,14 @@ int correct_impl(care_b200_ctx* ctx, uint32_t first, uint32_t count, care_b200_r
     if (!ctx->tables_ready) return fail(ctx, CARE_B200_ESTATE, "no tables uploaded or built");
     if ((uint64_t)first + count > ctx->n) return fail(ctx, CARE_B200_EINVAL, "anchor range beyond the read storage");
     if (ctx->opt.paired_end && ((first | count) & 1)) return fail(ctx, CARE_B200_EINVAL, "paired-end ranges must be pair aligned");
+    if (ctx->opt.correction_type == 1 && !ctx->mlp_set) return fail(ctx, CARE_B200_ESTATE, "correction_type 1 needs care_b200_set_mlp");
     CK(cudaSetDevice(ctx->opt.device), "cudaSetDevice");
+    ctx->r_fx.clear(); ctx->r_fread.clear(); ctx->r_fmeta.clear(); ctx->r_flogit.clear();
     uint32_t B = ctx->opt.batch_size > 0 ? (uint32_t)ctx->opt.batch_size : (1u << 21);
     if (ctx->opt.paired_end) B &= ~1u;
     if (B == 0) B = 2;
     ctx->last_ms = 0.f;
-    ctx->stage_ms[0] = ctx->stage_ms[1] = ctx->stage_ms[2] = 0.f;
+    ctx->stage_ms[0] = ctx->stage_ms[1] = ctx->stage_ms[2] = ctx->stage_ms[3] = 0.f;
     ctx->r_ncand = 0;
     ctx->r_pairs = 0;
     ctx->r_valid = false;
@@ -641,6 +721,33 @@ int care_b200_correct_range(care_b200_ctx* ctx, uint32_t first, uint32_t count, 
 
 int care_b200_correct_range_device(care_b200_ctx* ctx, uint32_t first, uint32_t count) {
     return correct_impl(ctx, first, count, nullptr, false);
+}
+
+int care_b200_set_mlp(care_b200_ctx* ctx, const float* params) {
+    if (!ctx || !params) return CARE_B200_EINVAL;
+    for (int i = 0; i < kMlpFloats; i++)
+        if (!std::isfinite(params[i])) return fail(ctx, CARE_B200_EINVAL, "non-finite network parameter");
+    CK(cudaSetDevice(ctx->opt.device), "cudaSetDevice");
+    CK(ctx->d_mlp.ensure(kMlpFloats * 4), "alloc network");
+    CK(cudaMemcpy(ctx->d_mlp.p, params, kMlpFloats * 4, cudaMemcpyHostToDevice), "upload network");
+    ctx->mlp_set = true;
+    return CARE_B200_OK;
+}
+
+int care_b200_collect_features(care_b200_ctx* ctx, uint32_t first, uint32_t count, care_b200_results* res,
+                               care_b200_features* feats) {
+    if (!ctx || !feats) return CARE_B200_EINVAL;
+    ctx->collect = true;
+    const int rc = correct_impl(ctx, first, count, res, true);
+    ctx->collect = false;
+    std::memset(feats, 0, sizeof(*feats));
+    if (rc) return rc;
+    feats->count = ctx->r_fread.size();
+    feats->x = ctx->r_fx.data();
+    feats->read_ids = ctx->r_fread.data();
+    feats->meta = ctx->r_fmeta.data();
+    feats->logits = ctx->opt.correction_type == 1 ? ctx->r_flogit.data() : nullptr;
+    return CARE_B200_OK;
 }
 
 int care_b200_serialize_results(care_b200_ctx* ctx, const care_b200_results* res, uint8_t* out,
@@ -737,7 +844,7 @@ int care_b200_write_output(care_b200_ctx* ctx, const char* outfile) {
 int care_b200_last_timing(const care_b200_ctx* ctx, float* total_ms, float* stage_ms, int nstages) {
     if (!ctx) return CARE_B200_EINVAL;
     if (total_ms) *total_ms = ctx->last_ms;
-    for (int i = 0; i < nstages && i < 3 && stage_ms; i++) stage_ms[i] = ctx->stage_ms[i];
+    for (int i = 0; i < nstages && i < 4 && stage_ms; i++) stage_ms[i] = ctx->stage_ms[i];
     return CARE_B200_OK;
 }
 

@@ -96,6 +96,8 @@ struct DevOptions {
     int threshold;                    // resultsPerMapThreshold
     int coverage_int;                 // int(estimatedCoverage), the refinement's dataset_coverage
     int correction_type;
+    int clf_mode;                     // 0 plain rule, 1 plain + decision rows, 2 network decides
+    int clf_min_coverage;             // decision columns below this coverage keep the plain rule
     float max_error_rate;
     float min_overlap_ratio;
     float estimated_errorrate;
@@ -156,6 +158,7 @@ enum : int {
     kStatusCandOverflow = 1,          // candidate arena too small, rerun with more space
     kStatusCorrOverflow = 2,          // candidate-correction arena too small
     kStatusColumns = 4,               // more MSA columns than the kernel holds
+    kStatusFeatOverflow = 8,          // decision-column arena too small
 };
 
 // MurmurHash3 64-bit finalizer (the published fmix64), as used by the

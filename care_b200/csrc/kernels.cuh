@@ -281,18 +281,27 @@ struct MsaOut {
     char* corr_seq;                   // corr_cap * max_len
     unsigned long long* corr_count;
     unsigned long long corr_cap;
+    // decision columns (EMIT): 24 features, read id, pos | orig << 16 | cons << 18
+    float* feat;
+    uint32_t* feat_read;
+    uint32_t* feat_meta;
+    unsigned long long* feat_count;
+    unsigned long long feat_cap;
 };
+
+constexpr int kNumFeatures = 24;
 
 constexpr int kStage = 64;            // candidate rows held in shared memory
 
-// dynamic shared memory of k_msa: decoded rows (kStage + anchor) and raw rows
-__host__ __device__ inline size_t msa_smem_bytes(int max_len, int seq_pitch, int qual_pitch) {
+// dynamic shared memory of k_msa: decoded rows (kStage + anchor) and raw
+// rows; with decision rows also three per-anchor-column weights
+__host__ __device__ inline size_t msa_smem_bytes(int max_len, int seq_pitch, int qual_pitch, bool emit = false) {
     const size_t elem = (size_t)(kStage + 1) * max_len * 2;
     const size_t raw = (size_t)kStage * (seq_pitch + qual_pitch) * 4;
-    return ((elem + 15) & ~(size_t)15) + raw;
+    return ((elem + 15) & ~(size_t)15) + raw + (emit ? (size_t)3 * max_len * 4 : 0);
 }
 
-template <int BLOCK, int JB>
+template <int BLOCK, int JB, bool EMIT = false>
 __global__ void __launch_bounds__(BLOCK)
 k_msa(DevOptions o, DevReads r, uint32_t first, uint32_t count, const uint32_t* __restrict__ order,
       const uint32_t* __restrict__ cand_ids, const uint32_t* __restrict__ seg_off,
@@ -312,7 +321,7 @@ k_msa(DevOptions o, DevReads r, uint32_t first, uint32_t count, const uint32_t* 
     __shared__ uint8_t s_fwd[kStage];
     __shared__ uint8_t s_alive[kStage];
     __shared__ int s_red[NWARP][4];
-    __shared__ int s_vals[8];
+    __shared__ int s_vals[12];
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     if (blockIdx.x >= count) return;
@@ -328,6 +337,9 @@ k_msa(DevOptions o, DevReads r, uint32_t first, uint32_t count, const uint32_t* 
     uint16_t* s_aelem = s_elem + (size_t)kStage * mlen;      // anchor row
     uint32_t* s_rseq = (uint32_t*)(dsm + (((size_t)(kStage + 1) * mlen * 2 + 15) & ~(size_t)15));
     uint32_t* s_rqual = s_rseq + (size_t)kStage * r.seq_pitch;
+    // per anchor column: column weight sum, consensus weight, weight of the
+    // anchor's base (EMIT only)
+    float* s_fw = (float*)(s_rqual + (size_t)kStage * r.qual_pitch);
 
     if (cnt == 0) {
         if (tid == 0) { out.status[ai] = 0; out.nedits[ai] = 0; }
@@ -602,6 +614,15 @@ k_msa(DevOptions o, DevReads r, uint32_t first, uint32_t count, const uint32_t* 
                 s_cov[col] = (uint16_t)(nA + nC + nG + nT);
                 s_cnt[col][0] = (uint16_t)nA; s_cnt[col][1] = (uint16_t)nC;
                 s_cnt[col][2] = (uint16_t)nG; s_cnt[col][3] = (uint16_t)nT;
+                if constexpr (EMIT) {
+                    const int p = col - abegin;
+                    if (p >= 0 && p < La) {
+                        const uint32_t ob = s_aelem[p] & 3u;
+                        s_fw[p] = colw;
+                        s_fw[mlen + p] = cw;
+                        s_fw[2 * mlen + p] = ob == 0 ? wA[j] : ob == 1 ? wC[j] : ob == 2 ? wG[j] : wT[j];
+                    }
+                }
             }
         }
         __syncthreads();
@@ -738,6 +759,9 @@ k_msa(DevOptions o, DevReads r, uint32_t first, uint32_t count, const uint32_t* 
             }
             s_vals[4] = good;
             s_vals[5] = isHQ;
+            s_vals[6] = __float_as_int(avgSup);
+            s_vals[7] = __float_as_int(minSup);
+            s_vals[8] = minCov;
         }
         __syncthreads();
         allGood = s_vals[4];
@@ -771,6 +795,87 @@ k_msa(DevOptions o, DevReads r, uint32_t first, uint32_t count, const uint32_t* 
         out.nedits[ai] = useEdits ? nd : 0;
     }
 
+    // ---- decision columns (correctAnchorClf, corrector.hpp:1448-1472) ----
+    // Non-HQ MSAs only: each anchor position whose base differs from the
+    // consensus (and whose column reaches clf_min_coverage) becomes a row of
+    // 24 features. The plain rule's base stays in aout; with the network
+    // deciding, k_clf_apply overwrites it from the row's logit.
+    if constexpr (EMIT) {
+        if (!hq) {
+            int nm = 0, mxc = 0;
+            for (int p = tid; p < La; p += BLOCK) {
+                nm += (s_aelem[p] & 3u) != s_cons[abegin + p];
+                mxc = max(mxc, (int)s_cov[abegin + p]);
+            }
+#pragma unroll
+            for (int d = 16; d > 0; d >>= 1) {
+                nm += __shfl_xor_sync(0xffffffffu, nm, d);
+                mxc = max(mxc, __shfl_xor_sync(0xffffffffu, mxc, d));
+            }
+            __syncthreads();
+            if (lane == 0) { s_red[warp][0] = nm; s_red[warp][1] = mxc; }
+            __syncthreads();
+            int nmis = 0, maxCov = 0;
+#pragma unroll
+            for (int w = 0; w < NWARP; ++w) { nmis += s_red[w][0]; maxCov = max(maxCov, s_red[w][1]); }
+            const float avgSup = __int_as_float(s_vals[6]), minSup = __int_as_float(s_vals[7]);
+            const int minCov = s_vals[8];
+            const float E = o.estimated_coverage;
+            for (int p = tid; p < La; p += BLOCK) {
+                const int col = abegin + p;
+                const uint32_t ob = s_aelem[p] & 3u, cb = s_cons[col];
+                if (ob == cb || (int)s_cov[col] < o.clf_min_coverage) continue;
+                const float cov = (float)s_cov[col];
+                const int oc = s_cnt[col][ob], cc = s_cnt[col][cb];
+                const float wsum = s_fw[p], wc = s_fw[mlen + p], wo = s_fw[2 * mlen + p];
+                float x[kNumFeatures];
+                x[0] = fdiv_rn((float)oc, cov);
+                x[1] = fdiv_rn(wo, wsum);
+                x[2] = fdiv_rn(wo, (float)oc);
+                x[3] = fdiv_rn((float)cc, cov);
+                x[4] = s_support[col];
+                x[5] = fdiv_rn(wc, (float)cc);
+                x[6] = fdiv_rn(wsum, cov);
+                x[7] = fdiv_rn(cov, E);
+                x[8] = fdiv_rn(wsum, E);
+                x[9] = avgSup;
+                x[10] = minSup;
+                x[11] = fdiv_rn((float)maxCov, E);
+                x[12] = fdiv_rn((float)minCov, E);
+                x[13] = useQ ? s_qw[s_aelem[p] >> 2] : 1.0f;
+                x[14] = fdiv_rn((float)min(p, La - 1 - p), (float)La);
+                x[15] = fdiv_rn(fsub_rn(fsub_rn(wsum, wc), wo), wsum);
+                const int lo = max(p - 3, 0), hi = min(p + 3, La - 1);
+                float ssum = 0.0f, smin = s_support[abegin + lo], qsum = 0.0f;
+                for (int q = lo; q <= hi; ++q) {
+                    const float sv = s_support[abegin + q];
+                    ssum = __fadd_rn(ssum, sv);
+                    if (sv < smin) smin = sv;
+                    qsum = __fadd_rn(qsum, useQ ? s_qw[s_aelem[q] >> 2] : 1.0f);
+                }
+                const float nwin = (float)(hi - lo + 1);
+                x[16] = fdiv_rn(ssum, nwin);
+                x[17] = smin;
+                x[18] = fdiv_rn((float)nmis, (float)La);
+                int nloc = 0;
+                for (int q = max(p - 5, 0); q <= min(p + 5, La - 1); ++q)
+                    nloc += q != p && (s_aelem[q] & 3u) != s_cons[abegin + q];
+                x[19] = fdiv_rn((float)nloc, 10.0f);
+                x[20] = fdiv_rn((float)V, E);
+                x[21] = allGood ? 1.0f : 0.0f;
+                x[22] = (allGood || (s_support[col] > 0.90f && oc <= 2)) ? 1.0f : 0.0f;
+                x[23] = fdiv_rn(qsum, nwin);
+                const unsigned long long slot = atomicAdd(out.feat_count, 1ull);
+                if (slot >= out.feat_cap) { atomicOr(status, kStatusFeatOverflow); continue; }
+                float4* dst = reinterpret_cast<float4*>(out.feat + slot * kNumFeatures);
+#pragma unroll
+                for (int q = 0; q < kNumFeatures / 4; ++q) dst[q] = make_float4(x[4 * q], x[4 * q + 1], x[4 * q + 2], x[4 * q + 3]);
+                out.feat_read[slot] = a;
+                out.feat_meta[slot] = (uint32_t)p | (ob << 16) | (cb << 18);
+            }
+        }
+    }
+
     // ---- candidate correction (getCorrectedCandidates, msa.cpp:457-522) ----
     if (hq && o.correct_candidates) {
         const int ncc = o.new_columns;
@@ -802,6 +907,46 @@ k_msa(DevOptions o, DevReads r, uint32_t first, uint32_t count, const uint32_t* 
             out.corr_shift[slot] = shift;
             out.corr_use_edits[slot] = (!r.ambig[id] && nd <= L / 7) ? 1 : 0;
         }
+    }
+}
+
+// The network's verdict on each decision column of the batch: the consensus
+// base where the logit is positive, else the original base.
+static __global__ void k_clf_apply(const uint32_t* __restrict__ feat_read, const uint32_t* __restrict__ feat_meta,
+                            const float* __restrict__ logit, const unsigned long long* __restrict__ count,
+                            unsigned long long cap, uint32_t first, int mlen, char* __restrict__ seq,
+                            uint8_t* __restrict__ touched) {
+    const unsigned long long n = min(*count, cap);
+    for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (unsigned long long)gridDim.x * blockDim.x) {
+        const uint32_t meta = feat_meta[i];
+        const uint32_t ai = feat_read[i] - first;
+        const uint32_t b = logit[i] > 0.0f ? (meta >> 18) & 3u : (meta >> 16) & 3u;
+        seq[(size_t)ai * mlen + (meta & 0xFFFFu)] = "ACGT"[b];
+        touched[ai] = 1;
+    }
+}
+
+// Edit counts of the anchors whose corrected sequence k_clf_apply changed
+// (makeOutputOfTask, corrector.hpp:1648-1675): one warp per anchor.
+static __global__ void k_clf_recount(DevReads r, uint32_t first, uint32_t count, const uint8_t* __restrict__ touched,
+                              const char* __restrict__ seq, uint8_t* __restrict__ status,
+                              int32_t* __restrict__ nedits) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t ai = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+    if (ai >= count || !touched[ai]) return;
+    const uint32_t a = first + ai;
+    const int La = r.len[a];
+    const uint32_t* row = r.seq + (size_t)a * r.seq_pitch;
+    const char* s = seq + (size_t)ai * r.max_len;
+    int nd = 0;
+    for (int p = lane; p < La; p += 32) nd += "ACGT"[base_at(row, p)] != s[p];
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) nd += __shfl_xor_sync(0xffffffffu, nd, d);
+    if (lane == 0) {
+        const bool useEdits = !r.ambig[a] && nd <= La / 7;
+        status[ai] = (uint8_t)((status[ai] & ~4u) | (useEdits ? 4u : 0u));
+        nedits[ai] = useEdits ? nd : 0;
     }
 }
 

@@ -26,7 +26,8 @@ void usage() {
         "  --candidateCorrection        --candidateCorrectionNewColumns N\n"
         "  --minalignmentoverlap N      --maxmismatchratio F     --minalignmentoverlapratio F\n"
         "  --errorfactortuning F        --coveragefactortuning F --pairedFilterThreshold F\n"
-        "  --correctionQualityLabels    --batchsize N            -g,--gpu N");
+        "  --correctionQualityLabels    --batchsize N            -g,--gpu N\n"
+        "  --correctionType 0|1 (1: learned decision)  --ml-mlpfile FILE  --clfMinCoverage N");
 }
 
 bool flag_value(int& i, int argc, char** argv) {
@@ -43,7 +44,7 @@ int main(int argc, char** argv) {
     care_b200_options o;
     care_b200_default_options(&o);
     std::vector<std::string> inputs;
-    std::string outdir, outname;
+    std::string outdir, outname, mlpfile;
     bool haveCov = false, havePair = false;
     for (int i = 1; i < argc; i++) {
         const std::string a = argv[i];
@@ -87,6 +88,8 @@ int main(int argc, char** argv) {
         else if (a == "--pairedFilterThreshold") o.paired_filter_threshold = (float)std::atof(val());
         else if (a == "--batchsize") o.batch_size = std::atoi(val());
         else if (a == "--correctionType") o.correction_type = std::atoi(val()) == 1 ? 1 : 0;
+        else if (a == "--ml-mlpfile") mlpfile = val();
+        else if (a == "--clfMinCoverage") o.clf_min_coverage = std::atoi(val());
         else if (a == "--help") { usage(); return 0; }
         else { std::fprintf(stderr, "unknown option %s\n", a.c_str()); usage(); return 1; }
     }
@@ -103,6 +106,19 @@ int main(int argc, char** argv) {
         care_b200_destroy(ctx);
         return 1;
     };
+    if (o.correction_type == 1) {
+        // network parameters: CARE_B200_MLP_FLOATS little-endian float32 values
+        std::vector<float> params(CARE_B200_MLP_FLOATS);
+        FILE* f = mlpfile.empty() ? nullptr : std::fopen(mlpfile.c_str(), "rb");
+        const bool ok = f && std::fread(params.data(), 4, params.size(), f) == params.size();
+        if (f) std::fclose(f);
+        if (!ok) {
+            std::fprintf(stderr, "care-b200: --correctionType 1 needs --ml-mlpfile with %d float32 values\n", CARE_B200_MLP_FLOATS);
+            care_b200_destroy(ctx);
+            return 1;
+        }
+        if (care_b200_set_mlp(ctx, params.data())) return die("loading the network");
+    }
     std::printf("STEP 1: Database construction\n");
     const double t0 = now();
     std::vector<const char*> fp;

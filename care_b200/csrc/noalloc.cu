@@ -69,6 +69,7 @@ extern "C" int care_b200_correct_range_noalloc(const care_b200_options* opt, con
     if (!opt || !reads || !tables || !status || !num_edits || !sequences) return CARE_B200_EINVAL;
     if (num_anchors == 0) return CARE_B200_OK;
     if (opt->correct_candidates) return CARE_B200_EINVAL;                 // anchor correction only
+    if (opt->correction_type != 0) return CARE_B200_EINVAL;               // plain rule only
     if (opt->num_maps < 1 || opt->num_maps > kMaxMaps || tables->num_maps != opt->num_maps) return CARE_B200_EINVAL;
     if (opt->kmerlength < 1 || opt->kmerlength > 32) return CARE_B200_EINVAL;
     if (opt->quality_bits != 1 && opt->quality_bits != 2 && opt->quality_bits != 8) return CARE_B200_EINVAL;

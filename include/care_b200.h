@@ -50,6 +50,8 @@ typedef struct care_b200_options {
     int   threads;                  /* host threads for STEP1/STEP3 helpers */
     int   device;                   /* CUDA device ordinal */
     int   batch_size;               /* anchors per device batch, 0 = automatic */
+    int   clf_min_coverage;         /* learned form: decision columns with a lower
+                                       coverage keep the classic rule, default 3 */
 } care_b200_options;
 
 typedef struct care_b200_ctx care_b200_ctx;
@@ -216,6 +218,87 @@ int care_b200_correct_range_noalloc(const care_b200_options* opt, const care_b20
                                     const care_b200_device_tables* tables, uint32_t first_anchor,
                                     uint32_t num_anchors, uint8_t* status, int32_t* num_edits,
                                     char* sequences, void* stream);
+
+/* ---- learned decision (correction_type 1) ----
+ *
+ * The reference's classifier hook, correctAnchorClf (corrector.hpp:1448-1472)
+ * with ClfAgent::decide_anchor (classification.hpp:123-133), asks for every
+ * anchor position of a non-HQ MSA whose base differs from the consensus
+ * whether the consensus base is written. Here a 24 -> 64 -> 64 -> 1 MLP with
+ * GELU answers (logit > 0: write the consensus); positions whose column
+ * coverage is below clf_min_coverage keep the classic rule. The reference
+ * serves the hook with a random forest read from a file (forest.hpp:217-226);
+ * the network, its training kernels and the feature rows are this library's
+ * own.
+ *
+ * Parameter vector (float32, CARE_B200_MLP_FLOATS): W1[64][24] b1[64]
+ * W2[64][64] b2[64] w3[64] b3 (the CARE_B200_MLP_PARAMS trained values),
+ * then the input normalisation mean[24] inv_std[24]. Weights and hidden
+ * activations enter the tensor-core GEMMs as bfloat16 with FP32
+ * accumulation. */
+#define CARE_B200_MLP_FEATURES 24
+#define CARE_B200_MLP_HIDDEN   64
+#define CARE_B200_MLP_PARAMS   5825
+#define CARE_B200_MLP_FLOATS   5873
+
+/* Decision-column rows of the last care_b200_collect_features() call, owned
+ * by the context. meta = position | orig << 16 | cons << 18 (2-bit base
+ * codes A=0 C=1 G=2 T=3); logits only when the network decided. Row order is
+ * unspecified. */
+typedef struct care_b200_features {
+    uint64_t        count;
+    const float*    x;                /* count * 24 */
+    const uint32_t* read_ids;
+    const uint32_t* meta;
+    const float*    logits;           /* NULL under correction_type 0 */
+} care_b200_features;
+
+/* Parameters used by correction_type 1 (copied). */
+int care_b200_set_mlp(care_b200_ctx* ctx, const float* params);
+
+/* care_b200_correct_range() that also returns the decision-column rows:
+ * under correction_type 0 the rows the classic rule passed over (training
+ * data), under correction_type 1 the rows the network decided. */
+int care_b200_collect_features(care_b200_ctx* ctx, uint32_t first_anchor, uint32_t num_anchors,
+                               care_b200_results* results, care_b200_features* features);
+
+/* Training and batched inference of the network on one device. */
+typedef struct care_b200_mlp care_b200_mlp;
+
+typedef struct care_b200_mlp_train_options {
+    int      epochs;
+    int      batch;                   /* rows per Adam step, e.g. 65536 */
+    double   lr, beta1, beta2, eps;   /* Adam: 1e-3, 0.9, 0.999, 1e-8 */
+    uint64_t seed;                    /* row shuffling */
+} care_b200_mlp_train_options;
+
+void        care_b200_mlp_default_train_options(care_b200_mlp_train_options* o);
+int         care_b200_mlp_create(int device, care_b200_mlp** out);
+int         care_b200_mlp_destroy(care_b200_mlp* m);
+const char* care_b200_mlp_last_error(const care_b200_mlp* m);
+/* parameters in and out (CARE_B200_MLP_FLOATS); setting resets Adam */
+int care_b200_mlp_set_params(care_b200_mlp* m, const float* params);
+int care_b200_mlp_get_params(care_b200_mlp* m, float* params);
+/* uniform fan-in initialisation of the trained values (seeded) */
+int care_b200_mlp_init(care_b200_mlp* m, uint64_t seed);
+/* training rows made resident on the device (labels 0 or 1; weights scale
+ * each row's loss, NULL = 1); with set_normalisation the mean and 1/std of
+ * each feature are taken from them */
+int care_b200_mlp_set_data(care_b200_mlp* m, const float* x, const float* labels, const float* weights,
+                           uint64_t n, int set_normalisation);
+/* Adam over the resident rows, shuffled each epoch, the whole run replayed as
+ * one CUDA graph; losses (mean BCE per step) are written when non-NULL */
+int care_b200_mlp_train(care_b200_mlp* m, const care_b200_mlp_train_options* o, float* losses,
+                        uint64_t loss_capacity, uint64_t* num_steps);
+/* gradient (CARE_B200_MLP_PARAMS) and loss of host rows: sum over rows of
+ * weight * BCE(logit, label), divided by the row count (weights NULL = 1) */
+int care_b200_mlp_gradient(care_b200_mlp* m, const float* x, const float* labels, const float* weights,
+                           uint64_t n, float* grad, float* loss);
+/* one Adam step on host rows */
+int care_b200_mlp_train_step(care_b200_mlp* m, const float* x, const float* labels, const float* weights,
+                             uint64_t n, const care_b200_mlp_train_options* o, float* loss);
+/* logits of host rows */
+int care_b200_mlp_forward(care_b200_mlp* m, const float* x, uint64_t n, float* logits);
 
 /* Read-storage facts after upload. */
 uint32_t care_b200_num_reads(const care_b200_ctx* ctx);

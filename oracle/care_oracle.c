@@ -49,6 +49,7 @@ void co_default_opts(co_opts* o) {
     o->new_columns_to_correct = 15;
     o->quality_bits = 8;
     o->threads = 1;
+    o->clf_min_coverage = 3;
 }
 
 /* ------------------------------------------------------------------ */
@@ -918,6 +919,142 @@ static void compact(task_t* t, const uint8_t* keep, int sp, int dp, int with_msa
     t->n = w;
 }
 
+/* ------------------------------------------------------------------ */
+/* Learned decision columns. The reference's classifier hook asks, for  */
+/* every anchor column of a non-HQ MSA whose original base differs from  */
+/* the consensus, whether the consensus base should be written          */
+/* (correctAnchorClf, corrector.hpp:1448-1472; features in the spirit   */
+/* of extract_anchor_v3, classification.hpp:748-797, widened to 24).    */
+/* ------------------------------------------------------------------ */
+
+/* float -> bfloat16 -> float, round to nearest even */
+float co_bf16_round(float x) {
+    uint32_t u;
+    memcpy(&u, &x, 4);
+    if ((u & 0x7fffffffu) > 0x7f800000u) return x;          /* NaN */
+    u += 0x7fffu + ((u >> 16) & 1u);
+    u &= 0xffff0000u;
+    memcpy(&x, &u, 4);
+    return x;
+}
+
+static float gelu_f(float x) { return (0.5f * x) * (1.0f + erff(x * 0.70710678118654752f)); }
+
+/* Forward pass with the device path's roundings: normalised inputs,
+ * weights and hidden activations are bfloat16 values; products and sums
+ * are FP32 (sums here run in index order). */
+float co_mlp_logit(const float* P, const float* x) {
+    float xn[CO_NFEAT], h1[CO_HIDDEN];
+    for (int k = 0; k < CO_NFEAT; k++) xn[k] = co_bf16_round((x[k] - P[CO_MLP_MEAN + k]) * P[CO_MLP_ISTD + k]);
+    for (int n = 0; n < CO_HIDDEN; n++) {
+        float z = 0.0f;
+        for (int k = 0; k < CO_NFEAT; k++) z += xn[k] * co_bf16_round(P[CO_MLP_W1 + n * CO_NFEAT + k]);
+        h1[n] = co_bf16_round(gelu_f(z + P[CO_MLP_B1 + n]));
+    }
+    float s = 0.0f;
+    for (int n = 0; n < CO_HIDDEN; n++) {
+        float z = 0.0f;
+        for (int k = 0; k < CO_HIDDEN; k++) z += h1[k] * co_bf16_round(P[CO_MLP_W2 + n * CO_HIDDEN + k]);
+        const float h2 = co_bf16_round(gelu_f(z + P[CO_MLP_B2 + n]));
+        s += h2 * co_bf16_round(P[CO_MLP_W3 + n]);
+    }
+    return s + P[CO_MLP_B3];
+}
+
+typedef struct {
+    int allGood, minCov, maxCov, nmis;
+    float avgSup, minSup;
+} clf_anchor;
+
+static int code_of(char b) { return b == 'A' ? 0 : b == 'C' ? 1 : b == 'G' ? 2 : 3; }
+
+/* the 24 features of anchor position p; every float operation in the
+ * order the device code performs it */
+static void clf_features(const task_t* t, const ctx_t* c, int la, int p, const clf_anchor* A, float* x) {
+    const co_opts* o = c->o;
+    const int useQ = o->use_quality && c->r->has_quality;
+    const int col = t->abegin + p;
+    const float E = o->estimated_coverage;
+    const int cb = code_of(t->cons[col]);
+    const int cnt[4] = {t->cA[col], t->cC[col], t->cG[col], t->cT[col]};
+    const float w[4] = {t->wA[col], t->wC[col], t->wG[col], t->wT[col]};
+    const float wsum = ((w[0] + w[1]) + w[2]) + w[3];
+    const float wc = w[cb];
+    const float wo = t->origW[col];
+    const int oc = t->origCov[col];
+    const int cc = cnt[cb];
+    const float cov = (float)t->cov[col];
+    x[0] = (float)oc / cov;
+    x[1] = wo / wsum;
+    x[2] = wo / (float)oc;
+    x[3] = (float)cc / cov;
+    x[4] = t->support[col];
+    x[5] = wc / (float)cc;
+    x[6] = wsum / cov;
+    x[7] = cov / E;
+    x[8] = wsum / E;
+    x[9] = A->avgSup;
+    x[10] = A->minSup;
+    x[11] = (float)A->maxCov / E;
+    x[12] = (float)A->minCov / E;
+    x[13] = useQ ? t->qw[(unsigned char)t->anchor_q[p]] : 1.0f;
+    x[14] = (float)(p < la - 1 - p ? p : la - 1 - p) / (float)la;
+    x[15] = ((wsum - wc) - wo) / wsum;
+    const int lo = p - 3 > 0 ? p - 3 : 0, hi = p + 3 < la - 1 ? p + 3 : la - 1;
+    float ssum = 0.0f, smin = t->support[t->abegin + lo], qsum = 0.0f;
+    for (int q = lo; q <= hi; q++) {
+        const float sv = t->support[t->abegin + q];
+        ssum += sv;
+        if (sv < smin) smin = sv;
+        qsum += useQ ? t->qw[(unsigned char)t->anchor_q[q]] : 1.0f;
+    }
+    const float nwin = (float)(hi - lo + 1);
+    x[16] = ssum / nwin;
+    x[17] = smin;
+    x[18] = (float)A->nmis / (float)la;
+    int nloc = 0;
+    const int lo5 = p - 5 > 0 ? p - 5 : 0, hi5 = p + 5 < la - 1 ? p + 5 : la - 1;
+    for (int q = lo5; q <= hi5; q++)
+        if (q != p && t->anchor_dec[q] != t->cons[t->abegin + q]) nloc++;
+    x[19] = (float)nloc / 10.0f;
+    x[20] = (float)t->n / E;
+    x[21] = A->allGood ? 1.0f : 0.0f;
+    x[22] = (A->allGood || (t->support[col] > 0.90f && oc <= 2)) ? 1.0f : 0.0f;
+    x[23] = qsum / nwin;
+}
+
+static void push_feature(co_results* res, const co_feature* f) {
+    if (res->num_feats == res->cap_feats) {
+        res->cap_feats = res->cap_feats ? res->cap_feats * 2 : 256;
+        res->feats = realloc(res->feats, res->cap_feats * sizeof(co_feature));
+    }
+    res->feats[res->num_feats++] = *f;
+}
+
+/* decision columns of one corrected non-HQ anchor; in clf_mode 2 the
+ * network's verdict replaces the plain rule's base in corr */
+static void clf_columns(const ctx_t* c, const task_t* t, int la, uint32_t anchor, const clf_anchor* A,
+                        char* corr, co_results* res) {
+    const co_opts* o = c->o;
+    for (int p = 0; p < la; p++) {
+        const int col = t->abegin + p;
+        const char ob = t->anchor_dec[p], cb = t->cons[col];
+        if (ob == cb || t->cov[col] < o->clf_min_coverage) continue;
+        co_feature f;
+        memset(&f, 0, sizeof(f));
+        f.read_id = anchor;
+        f.pos = (int16_t)p;
+        f.orig = (uint8_t)code_of(ob);
+        f.cons = (uint8_t)code_of(cb);
+        clf_features(t, c, la, p, A, f.x);
+        if (o->clf_mode == 2) {
+            f.logit = co_mlp_logit(o->mlp, f.x);
+            corr[p] = f.logit > 0.0f ? cb : ob;
+        }
+        push_feature(res, &f);
+    }
+}
+
 typedef struct {
     int corrected, hq;
     /* candidate corrections, indices into the final candidate list */
@@ -1042,8 +1179,9 @@ static void correct_one(const ctx_t* c, task_t* t, uint32_t anchor, co_results* 
     float sum = 0.0f;
     for (int i = fc; i < lc; i++) sum += t->support[i];
     const float avgSup = sum / dist;
-    int minCov = t->cov[fc];
+    int minCov = t->cov[fc], maxCov = t->cov[fc];
     for (int i = fc + 1; i < lc; i++) if (t->cov[i] < minCov) minCov = t->cov[i];
+    for (int i = fc + 1; i < lc; i++) if (t->cov[i] > maxCov) maxCov = t->cov[i];
     int hq = 0;
     const int allGood = fgeq(avgSup, avgThr) && fgeq(minSup, minThr) && fgeq((float)minCov, covThr);
     if (allGood) {
@@ -1067,6 +1205,14 @@ static void correct_one(const ctx_t* c, task_t* t, uint32_t anchor, co_results* 
         else
             for (int i = 0; i < la; i++)
                 corr[i] = (t->support[t->abegin + i] > 0.90f && t->origCov[t->abegin + i] <= 2) ? t->cons[t->abegin + i] : t->anchor_dec[i];
+        if (o->clf_mode && !hq) {
+            clf_anchor A;
+            A.allGood = allGood; A.minCov = minCov; A.maxCov = maxCov;
+            A.avgSup = avgSup; A.minSup = minSup;
+            A.nmis = 0;
+            for (int i = 0; i < la; i++) A.nmis += t->anchor_dec[i] != t->cons[t->abegin + i];
+            clf_columns(c, t, la, anchor, &A, corr, res);
+        }
     }
     AR->hq = (uint8_t)hq;
     if (AR->status) {
@@ -1185,6 +1331,7 @@ co_results* co_correct(const co_reads* r, const co_tables* tb, const co_opts* o,
         if (o->paired_end) { b &= ~1ull; e &= ~1ull; if (i == threads - 1) e = first + count; }
         part[i] = *res;
         part[i].cands = NULL; part[i].cand_seq = NULL; part[i].num_cands = part[i].cap_cands = 0;
+        part[i].feats = NULL; part[i].num_feats = part[i].cap_feats = 0;
         jobs[i] = (corr_job){&c, &part[i], (uint32_t)b, (uint32_t)e, max_candidates(tb)};
         pthread_create(&th[i], NULL, correct_range, &jobs[i]);
     }
@@ -1201,13 +1348,23 @@ co_results* co_correct(const co_reads* r, const co_tables* tb, const co_opts* o,
         w += part[i].num_cands;
         free(part[i].cands); free(part[i].cand_seq);
     }
+    size_t nf = 0;
+    for (int i = 0; i < threads; i++) nf += part[i].num_feats;
+    res->num_feats = res->cap_feats = nf;
+    res->feats = xmalloc((nf ? nf : 1) * sizeof(co_feature));
+    w = 0;
+    for (int i = 0; i < threads; i++) {
+        if (part[i].num_feats) memcpy(res->feats + w, part[i].feats, part[i].num_feats * sizeof(co_feature));
+        w += part[i].num_feats;
+        free(part[i].feats);
+    }
     free(part);
     return res;
 }
 
 void co_results_free(co_results* res) {
     if (!res) return;
-    free(res->anchors); free(res->anchor_seq); free(res->cands); free(res->cand_seq); free(res);
+    free(res->anchors); free(res->anchor_seq); free(res->cands); free(res->cand_seq); free(res->feats); free(res);
 }
 
 int co_trace_anchor(const co_reads* r, const co_tables* tb, const co_opts* o,
@@ -1240,7 +1397,7 @@ int co_trace_anchor(const co_reads* r, const co_tables* tb, const co_opts* o,
     for (int i = 0; i < t.n && i < cap; i++) {
         ids[i] = t.ids[i]; shifts[i] = t.shifts[i]; orient[i] = t.flag[i]; weights[i] = t.w[i];
     }
-    free(res.anchor_seq); free(res.cands); free(res.cand_seq);
+    free(res.anchor_seq); free(res.cands); free(res.cand_seq); free(res.feats);
     task_free(&t);
     return tr->n_final;
 }

@@ -40,7 +40,40 @@ typedef struct {
     int   paired_end;               /* --pairmode PE */
     int   threads;                  /* -t */
     int   quality_labels;           /* --correctionQualityLabels */
+    /* classifier hook (correctAnchorClf, corrector.hpp:1448-1472): 0 = the
+     * plain rule only; 1 = plain rule, decision columns reported as feature
+     * rows; 2 = the MLP decides each decision column (plain rule below
+     * clf_min_coverage) */
+    int   clf_mode;
+    int   clf_min_coverage;
+    const float* mlp;               /* CO_MLP_FLOATS values, clf_mode 2 */
 } co_opts;
+
+/* ---- learned decision: features and the MLP ---- */
+#define CO_NFEAT 24
+#define CO_HIDDEN 64
+/* parameter vector: W1[64][24] b1[64] W2[64][64] b2[64] w3[64] b3, then the
+ * input normalisation mean[24] inv_std[24] */
+#define CO_MLP_W1 0
+#define CO_MLP_B1 1536
+#define CO_MLP_W2 1600
+#define CO_MLP_B2 5696
+#define CO_MLP_W3 5760
+#define CO_MLP_B3 5824
+#define CO_MLP_NPARAM 5825
+#define CO_MLP_MEAN 5825
+#define CO_MLP_ISTD 5849
+#define CO_MLP_FLOATS 5873
+
+/* One decision column: an anchor position of a non-HQ MSA whose original
+ * base differs from the consensus (orig/cons are 2-bit codes). */
+typedef struct {
+    uint32_t read_id;
+    int16_t  pos;
+    uint8_t  orig, cons;
+    float    logit;                 /* clf_mode 2 only */
+    float    x[CO_NFEAT];
+} co_feature;
 
 void co_default_opts(co_opts* o);
 
@@ -106,6 +139,9 @@ typedef struct {
     co_cand_result*   cands;
     char*             cand_seq;    /* num_cands * max_len, forward orientation */
     size_t            num_cands, cap_cands;
+    /* decision columns (clf_mode 1 and 2), in anchor then position order */
+    co_feature*       feats;
+    size_t            num_feats, cap_feats;
 } co_results;
 
 /* ---- end-to-end (STEP1 + STEP2 + STEP3 of care-cpu) ---- */
@@ -132,6 +168,8 @@ int      co_threshold(float coverage);
 void     co_encode_quality(const char* q, int len, int bits, uint32_t* out);
 void     co_decode_quality(const uint32_t* enc, int len, int bits, char* out);
 void     co_quality_weights(float* out256);
+float    co_bf16_round(float x);
+float    co_mlp_logit(const float* params, const float* x);
 
 typedef struct {
     int score, overlap, shift, nops, valid;

@@ -26,7 +26,8 @@ class CoOpts(ctypes.Structure):
         ("new_columns_to_correct", ctypes.c_int), ("use_quality", ctypes.c_int),
         ("quality_bits", ctypes.c_int), ("exclude_ambiguous", ctypes.c_int),
         ("correct_candidates", ctypes.c_int), ("paired_end", ctypes.c_int), ("threads", ctypes.c_int),
-        ("quality_labels", ctypes.c_int),
+        ("quality_labels", ctypes.c_int), ("clf_mode", ctypes.c_int), ("clf_min_coverage", ctypes.c_int),
+        ("mlp", ctypes.POINTER(ctypes.c_float)),
     ]
 
 
@@ -61,11 +62,22 @@ class CoCand(ctypes.Structure):
                 ("length", ctypes.c_int32), ("use_edits", ctypes.c_uint8), ("pad", ctypes.c_uint8 * 3)]
 
 
+NFEAT = 24
+MLP_FLOATS = 5873
+
+
+class CoFeature(ctypes.Structure):
+    _fields_ = [("read_id", ctypes.c_uint32), ("pos", ctypes.c_int16), ("orig", ctypes.c_uint8),
+                ("cons", ctypes.c_uint8), ("logit", ctypes.c_float), ("x", ctypes.c_float * NFEAT)]
+
+
 class CoResults(ctypes.Structure):
     _fields_ = [("first", ctypes.c_uint32), ("count", ctypes.c_uint32), ("max_len", ctypes.c_int),
                 ("anchors", ctypes.POINTER(CoAnchor)), ("anchor_seq", ctypes.POINTER(ctypes.c_char)),
                 ("cands", ctypes.POINTER(CoCand)), ("cand_seq", ctypes.POINTER(ctypes.c_char)),
-                ("num_cands", ctypes.c_size_t), ("cap_cands", ctypes.c_size_t)]
+                ("num_cands", ctypes.c_size_t), ("cap_cands", ctypes.c_size_t),
+                ("feats", ctypes.POINTER(CoFeature)), ("num_feats", ctypes.c_size_t),
+                ("cap_feats", ctypes.c_size_t)]
 
 
 class CoAlign(ctypes.Structure):
@@ -96,6 +108,10 @@ def lib() -> ctypes.CDLL:
     L.co_results_free.argtypes = [P(CoResults)]
     L.co_write_output.argtypes = [P(CoReads), P(CoResults), P(CoOpts), ctypes.c_char_p]
     L.co_run.argtypes = [P(ctypes.c_char_p), ctypes.c_int, ctypes.c_char_p, P(CoOpts), P(ctypes.c_double)]
+    L.co_bf16_round.argtypes = [ctypes.c_float]
+    L.co_bf16_round.restype = ctypes.c_float
+    L.co_mlp_logit.argtypes = [P(ctypes.c_float), P(ctypes.c_float)]
+    L.co_mlp_logit.restype = ctypes.c_float
     L.co_encode_2bit.argtypes = [ctypes.c_char_p, ctypes.c_int, P(ctypes.c_uint32)]
     L.co_decode_2bit.argtypes = [P(ctypes.c_uint32), ctypes.c_int, ctypes.c_char_p]
     L.co_revcomp_2bit.argtypes = [P(ctypes.c_uint32), ctypes.c_int, P(ctypes.c_uint32)]
@@ -204,6 +220,22 @@ class OracleRun:
              for i in range(nc)]
         seq = np.ctypeslib.as_array(ctypes.cast(res.cand_seq, ctypes.POINTER(ctypes.c_uint8)), shape=(nc, L)).copy()
         return c, seq
+
+    def features(self):
+        """Decision-column rows: dict of read_id, pos, orig, cons (2-bit
+        codes), logit and x (n, 24), in anchor then position order."""
+        res = self.res.contents
+        n = res.num_feats
+        if n == 0:
+            return {"read_id": np.zeros(0, np.uint32), "pos": np.zeros(0, np.int16),
+                    "orig": np.zeros(0, np.uint8), "cons": np.zeros(0, np.uint8),
+                    "logit": np.zeros(0, np.float32), "x": np.zeros((0, NFEAT), np.float32)}
+        raw = np.ctypeslib.as_array(ctypes.cast(res.feats, ctypes.POINTER(ctypes.c_uint8)),
+                                    shape=(n * ctypes.sizeof(CoFeature),)).copy()
+        dt = np.dtype([("read_id", "<u4"), ("pos", "<i2"), ("orig", "u1"), ("cons", "u1"),
+                       ("logit", "<f4"), ("x", "<f4", (NFEAT,))])
+        a = raw.view(dt)
+        return {k: a[k].copy() for k in dt.names}
 
     def lengths(self):
         r = self.reads.contents
