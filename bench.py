@@ -18,6 +18,10 @@ src/dispatch_care_correct_cpu.cpp:157-168; reads/s = reads / STEP2 time).
   --impl reference : the reference's care-cpu (built from its sources by
           oracle/Makefile) on all host cores, on a bounded sample of the
           workload (same model, 1.25 Mbp genome, 250,000 reads).
+  learned : the same steps with the learned decision (correction_type 1,
+          network parameters care_b200/data/mlp_pe30x.bin, trained by
+          `python -m care_b200.learned` on three other seeded genomes), and
+          base-level TP/FP/FN/F1 of both forms against the true reads.
 
 Multi-GPU: one process per GPU; each rank corrects its own 1M-read set
 (independent genome partitions, no data-path collective) -> weak scaling.
@@ -40,7 +44,11 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 ARGS = "-c 30 -k 20 -h 32 -q --qualityScoreBits 2 --pairmode PE"
-METRIC = "reads corrected/s (STEP2), 5 Mbp / 30x paired-end, plain method"
+METRIC = "reads corrected/s on 1 B200: plain vs MLP-classifier form at matched base F1"
+MLP_FILE = os.path.join(ROOT, "care_b200", "data", "mlp_pe30x.bin")
+# k_msa DRAM bytes per anchor: dram__bytes_read.sum + dram__bytes_write.sum of
+# one ncu capture of 100,000 anchors of this workload model (116.39 MB)
+MSA_DRAM_BYTES_PER_ANCHOR = 1163.9
 CARE_CPU = os.path.join(ROOT, "oracle", "_ref", "care-cpu")
 L2_BYTES = 126 * 1024 * 1024
 
@@ -197,6 +205,31 @@ def progress(msg: str) -> None:
     print(f"[bench {time.time() - T0:7.1f}s] {msg}", file=sys.stderr, flush=True)
 
 
+def base_counts(rs, path):
+    """TP/FP/FN/TN of a corrected FASTQ against the true reads."""
+    from care_b200 import datagen
+    n, L = rs.seqs.shape
+    data = open(path, "rb").read().split(b"\n")
+    corr = np.frombuffer(b"".join(data[1:4 * n:4]), np.uint8).reshape(n, L)
+    return datagen.base_level_counts(rs.seqs, corr, rs.truth, rs.lengths)
+
+
+def timed_steps(corr, n, steps, flush):
+    """Device ms and per-stage ms (mean over steps), wall ms per step."""
+    import torch
+    dev_ms, stage, t_wall = [], np.zeros(4), 0.0
+    for _ in range(steps):
+        flush.fill_(1.0)
+        torch.cuda.synchronize()
+        w0 = time.perf_counter()
+        corr.correct_range_device(0, n)
+        t_wall += time.perf_counter() - w0
+        tot, st = corr.last_timing()
+        dev_ms.append(tot)
+        stage += np.array(st)
+    return float(np.mean(dev_ms)), stage / steps, t_wall / steps * 1e3
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -205,6 +238,7 @@ def main():
     ap.add_argument("--impl", default="care_b200", choices=["care_b200", "reference"])
     ap.add_argument("--genome", type=int, default=5_000_000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-learned", action="store_true")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -250,26 +284,52 @@ def main():
         progress(f"warm-up step {w} done")
     barrier()
     with ClockSampler(local) as clk:
-        dev_ms, stage = [], np.zeros(3)
-        t_wall = 0.0
-        for _ in range(args.steps):
-            flush.fill_(1.0)
-            torch.cuda.synchronize()
-            w0 = time.perf_counter()
-            corr.correct_range_device(0, n)
-            t_wall += time.perf_counter() - w0
-            tot, st = corr.last_timing()
-            dev_ms.append(tot)
-            stage += np.array(st)
+        ms, stage, wall_ms = timed_steps(corr, n, args.steps, flush)
         barrier()
     stats = corr.last_stats()
-    ms = float(np.mean(dev_ms))
     if world > 1:
         t = torch.tensor([ms], device=f"cuda:{local}")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
-    stage /= args.steps
     value = world * n / (ms / 1e3)
+
+    # the learned decision on the same reads: device time of the same steps,
+    # then base-level counts of both forms against the true reads
+    learned = None
+    if not args.no_learned and os.path.exists(MLP_FILE):
+        from care_b200 import learned as lrn, datagen
+        params = lrn.load_params(MLP_FILE)
+        progress("learned form: load + tables")
+        mcorr = care_b200.Corrector(care_b200.options_from_args(ARGS, device=local, correction_type=1))
+        mcorr.set_mlp(params)
+        mcorr.load_files([fq])
+        mcorr.build_tables()
+        for _ in range(args.warmup):
+            mcorr.correct_range_device(0, n)
+        barrier()
+        mms, mstage, _ = timed_steps(mcorr, n, args.steps, flush)
+        barrier()
+        if world > 1:
+            t = torch.tensor([mms], device=f"cuda:{local}")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            mms = float(t.item())
+        progress("learned form timed; base-level counts")
+        counts = {}
+        for name, c in (("plain", corr), ("learned", mcorr)):
+            c.correct_range(0, n)
+            out = os.path.join(tmp, f"{name}.fq")
+            c.write_output(out)
+            tp, fp, fn, tn = base_counts(rs, out)
+            counts[name] = {"tp": tp, "fp": fp, "fn": fn, "f1": datagen.f1(tp, fp, fn)}
+            os.unlink(out)
+        mcorr.close()
+        mvalue = world * n / (mms / 1e3)
+        learned = {"value": mvalue, "unit": "reads/s", "ms_per_step": mms, "ratio_vs_plain": mvalue / value,
+                   "stage_ms": {"candidates": mstage[0], "align": mstage[1], "msa": mstage[2],
+                                "classifier": mstage[3]},
+                   "network": "24-64-64-1 GELU, bf16 tcgen05 GEMMs, fp32 accumulate",
+                   "params": os.path.relpath(MLP_FILE, ROOT),
+                   "base_level": counts, "gpu_launches": 6 * args.steps}
 
     progress("timed steps done")
     # e2e through the C ABI from host buffers
@@ -316,10 +376,11 @@ def main():
                    "genome_bp": args.genome, "l2": "flushed between steps (252 MB write); working set > L2",
                    "parallelism": f"replicas x{world} (independent read sets)",
                    "stage_ms": {"candidates": stage[0], "align": stage[1], "msa": stage[2]},
-                   "pairs_per_step": stats["pairs"], "wall_ms_per_step": t_wall / args.steps * 1e3,
+                   "pairs_per_step": stats["pairs"], "wall_ms_per_step": wall_ms,
                    "step1_s": step1_s},
         "roofline": {"kernel": "k_msa", "bound": "hbm", "achieved": msa_gbs, "peak": hbm_peak,
-                     "unit": "GB/s", "frac": msa_gbs / hbm_peak, "traffic": None,
+                     "unit": "GB/s", "frac": msa_gbs / hbm_peak, "traffic": MSA_DRAM_BYTES_PER_ANCHOR * n,
+                     "traffic_source": "ncu capture of 100,000 anchors scaled by anchors per launch",
                      "peak_source": "measured" if peaks else "fallback"},
         "roofline_alignment": {"kernel": "k_align", "word_compares_per_s": align_words / (stage[1] / 1e3),
                                "ms": stage[1]},
@@ -328,6 +389,8 @@ def main():
         "gpu_launches": 3 * args.steps,
         "clocks": clk.summary(),
     }
+    if learned is not None:
+        line["learned"] = learned
     if rank == 0 and world == 1 and not args.no_cpu_baseline and os.path.exists(CARE_CPU):
         threads = host_cores()
         progress(f"e2e done; care-cpu sample on {threads} threads")
