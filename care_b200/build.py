@@ -1,6 +1,7 @@
 """Builds the sm_100a library and the care-b200 driver in place.
 
-    python -m care_b200.build            # -> care_b200/libcareb200.so, care_b200/care-b200
+    python -m care_b200.build            # -> care_b200/libcareb200.so, care_b200/care-b200,
+                                         #    care_b200/care-b200-peaks
 
 Objects go to care_b200/_build/ (git-ignored). Every CUDA translation unit is
 compiled for sm_100a only, with FMA contraction off (--fmad=false): the
@@ -19,6 +20,7 @@ CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libcareb200.so")
 EXE = os.path.join(HERE, "care-b200")
+PEAKS = os.path.join(HERE, "care-b200-peaks")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ARCH + ["-O3", "-lineinfo", "--fmad=false", "-std=c++17", "-Xcompiler", "-fPIC",
@@ -75,6 +77,9 @@ def build(force: bool = False, verbose: bool = False) -> str:
     if force or _newer(EXE, [LIB, os.path.join(CSRC, "main.cpp")]):
         run(["g++", "-O2", "-std=c++17", "-o", EXE, os.path.join(CSRC, "main.cpp"),
              "-L" + HERE, "-lcareb200", "-Wl,-rpath,$ORIGIN", "-lpthread"])
+    peaks_src = os.path.join(CSRC, "peaks.cu")
+    if force or _newer(PEAKS, [peaks_src]):
+        run([nvcc()] + ARCH + ["-O3", "-lineinfo", "-o", PEAKS, peaks_src])
     return LIB
 
 
