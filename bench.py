@@ -23,7 +23,12 @@ src/dispatch_care_correct_cpu.cpp:157-168; reads/s = reads / STEP2 time).
           `python -m care_b200.learned` on three other seeded genomes), and
           base-level TP/FP/FN/F1 of both forms against the true reads.
 
-Multi-GPU: one process per GPU; each rank corrects its own 1M-read set
+--workload uneven : the batched uneven set instead -- 10 Mbp genome with 8%
+          repeats in families of 5-500 copies (0.5-2% divergence), single-end
+          reads of 50-250 bp at 40x (~2.7M reads), same error and quality
+          model; -c 40 -k 20 -h 32 -q --qualityScoreBits 2 --pairmode SE.
+
+Multi-GPU: one process per GPU; each rank corrects its own read set
 (independent genome partitions, no data-path collective) -> weak scaling.
 """
 from __future__ import annotations
@@ -44,6 +49,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 ARGS = "-c 30 -k 20 -h 32 -q --qualityScoreBits 2 --pairmode PE"
+ARGS_UNEVEN = "-c 40 -k 20 -h 32 -q --qualityScoreBits 2 --pairmode SE"
 METRIC = "reads corrected/s on 1 B200: plain vs MLP-classifier form at matched base F1"
 MLP_FILE = os.path.join(ROOT, "care_b200", "data", "mlp_pe30x.bin")
 # k_msa DRAM bytes per anchor: dram__bytes_read.sum + dram__bytes_write.sum of
@@ -53,8 +59,10 @@ CARE_CPU = os.path.join(ROOT, "oracle", "_ref", "care-cpu")
 L2_BYTES = 126 * 1024 * 1024
 
 
-def workload(rank: int, genome_size: int):
+def workload(rank: int, genome_size: int, kind: str = "pe"):
     from care_b200 import datagen
+    if kind == "uneven":
+        return datagen.single_end_uneven(seed=3 + 1000 * rank, genome_size=genome_size, coverage=40.0)
     # 2% of the genome in 20 copies of one repeat unit (5 kbp at 5 Mbp)
     rs = datagen.paired_end_repeats(seed=2 + 1000 * rank, genome_size=genome_size,
                                     repeat_unit=max(100, genome_size // 1000))
@@ -62,9 +70,8 @@ def workload(rank: int, genome_size: int):
 
 
 def write_fastq_fast(rs, path):
-    n, L = rs.num_reads, rs.seqs.shape[1]
-    assert (rs.lengths == L).all()
-    heads = [b"@r%d\n" % i for i in range(n)]
+    n, W = rs.num_reads, rs.seqs.shape[1]
+    lens = rs.lengths
     seqs = rs.seqs.tobytes()
     quals = rs.quals.tobytes()
     with open(path, "wb") as f:
@@ -72,7 +79,8 @@ def write_fastq_fast(rs, path):
         for b in range(0, n, chunk):
             parts = []
             for i in range(b, min(n, b + chunk)):
-                parts += [heads[i], seqs[i * L:(i + 1) * L], b"\n+\n", quals[i * L:(i + 1) * L], b"\n"]
+                o, L = i * W, int(lens[i])
+                parts += [b"@r%d\n" % i, seqs[o:o + L], b"\n+\n", quals[o:o + L], b"\n"]
             f.write(b"".join(parts))
 
 
@@ -246,10 +254,17 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="care_b200", choices=["care_b200", "reference"])
-    ap.add_argument("--genome", type=int, default=5_000_000)
+    ap.add_argument("--workload", default="pe", choices=["pe", "uneven"])
+    ap.add_argument("--genome", type=int, default=None, help="bp (default 5 Mbp, uneven 10 Mbp)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned", action="store_true")
+    ap.add_argument("--tuning", default="auto", choices=["auto", "default"],
+                    help="auto: the committed launch mapping of the workload (care_b200/tuning/)")
     args = ap.parse_args()
+    if args.genome is None:
+        args.genome = 10_000_000 if args.workload == "uneven" else 5_000_000
+    uneven = args.workload == "uneven"
+    run_args = ARGS_UNEVEN if uneven else ARGS
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -273,13 +288,17 @@ def main():
 
     tmp = tempfile.mkdtemp(prefix=f"careb200_bench_{rank}_")
     progress("generating reads")
-    rs = workload(rank, args.genome)
+    rs = workload(rank, args.genome, args.workload)
     n = rs.num_reads
     fq = os.path.join(tmp, "reads.fq")
     write_fastq_fast(rs, fq)
 
-    opts = care_b200.options_from_args(ARGS, device=local)
+    opts = care_b200.options_from_args(run_args, device=local)
     corr = care_b200.Corrector(opts)
+    from care_b200 import autotune
+    tuned = autotune.load(args.workload) if args.tuning == "auto" else None
+    if tuned:
+        corr.tuning = tuned
     t0 = time.perf_counter()
     progress("STEP1: load + tables")
     corr.load_files([fq])
@@ -306,12 +325,14 @@ def main():
     # the learned decision on the same reads: device time of the same steps,
     # then base-level counts of both forms against the true reads
     learned = None
-    if not args.no_learned and os.path.exists(MLP_FILE):
+    if not args.no_learned and not uneven and os.path.exists(MLP_FILE):
         from care_b200 import learned as lrn, datagen
         params = lrn.load_params(MLP_FILE)
         progress("learned form: load + tables")
         mcorr = care_b200.Corrector(care_b200.options_from_args(ARGS, device=local, correction_type=1))
         mcorr.set_mlp(params)
+        if tuned:
+            mcorr.tuning = tuned
         mcorr.load_files([fq])
         mcorr.build_tables()
         for _ in range(args.warmup):
@@ -371,27 +392,36 @@ def main():
     if os.path.exists(pk):
         peaks = json.load(open(pk))
     hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
-    # MSA stage, HBM roofline: per pair 40 B packed read + 40 B 2-bit
-    # qualities + 4 B id + 13 B alignment tuple; per anchor its own row and
-    # qualities (84 B) and the corrected row (150 B)
-    msa_bytes = stats["pairs"] * 97 + n * (84 + 150)
+    # MSA stage, HBM roofline: per pair the packed read (4*ceil(L/16) B, 40 B
+    # at L=150) + 2-bit qualities (same) + 4 B id + 13 B alignment tuple; per
+    # anchor its own row and qualities and the corrected row (L B); L taken
+    # as the mean of the set's rows
+    row_b = float(np.mean(8 * ((rs.lengths.astype(np.int64) + 15) // 16)))
+    mean_len = float(np.mean(rs.lengths))
+    per_pair = row_b + 17
+    msa_bytes = stats["pairs"] * per_pair + n * (row_b + mean_len)
     msa_gbs = msa_bytes / (stage[2] / 1e3) / 1e9
-    # alignment stage: un-pruned 32-bit word compares, 1486 per pair at L=150
-    align_words = stats["pairs"] * 1486
+    # alignment stage: un-pruned 32-bit word compares counted by k_align
+    # (1486 per pair at L=150)
+    align_words = stats["word_compares"]
     align_rate = align_words / (stage[1] / 1e3)
     ip = int_peaks()
     line = {
         "metric": METRIC, "value": value, "unit": "reads/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded), " + rs.name,
-        "config": {"workload": "pe_5Mbp_30x_150bp", "reads_per_gpu": n, "args": ARGS,
+        "config": {"workload": ("se_uneven_%dMbp_40x_50-250bp" % (args.genome // 1_000_000)) if uneven
+                   else "pe_5Mbp_30x_150bp", "reads_per_gpu": n, "args": run_args,
                    "genome_bp": args.genome, "l2": "flushed between steps (252 MB write); working set > L2",
                    "parallelism": f"replicas x{world} (independent read sets)",
                    "stage_ms": {"candidates": stage[0], "align": stage[1], "msa": stage[2]},
                    "pairs_per_step": stats["pairs"], "wall_ms_per_step": wall_ms,
+                   "tuning": corr.tuning, "tuning_source": "care_b200/tuning (autotuned)" if tuned else "default",
                    "step1_s": step1_s},
         "roofline": {"kernel": "k_msa", "bound": "hbm", "achieved": msa_gbs, "peak": hbm_peak,
-                     "unit": "GB/s", "frac": msa_gbs / hbm_peak, "traffic": MSA_DRAM_BYTES_PER_ANCHOR * n,
+                     "bytes_per_pair": per_pair,
+                     "unit": "GB/s", "frac": msa_gbs / hbm_peak,
+                     "traffic": None if uneven else MSA_DRAM_BYTES_PER_ANCHOR * n,
                      "traffic_source": "ncu capture of 100,000 anchors scaled by anchors per launch",
                      "peak_source": "measured" if peaks else "fallback"},
         "roofline_alignment": {"kernel": "k_align", "bound": "int", "unit": "word compares/s",
@@ -399,7 +429,8 @@ def main():
                                "peak": ip["word_compares_per_s"] if ip else None,
                                "frac": align_rate / ip["word_compares_per_s"] if ip else None,
                                "popc_per_s": ip["popc_per_s"] if ip else None,
-                               "work": "un-pruned: 2 orientations x sum over shifts of ceil(overlap/32); 1486 per pair",
+                               "work": "un-pruned: 2 orientations x sum over shifts of ceil(overlap/32), counted per pair "
+                                       "by k_align (1486 per pair at L=150)", "work_per_step": align_words,
                                "peak_source": "care-b200-peaks (measured, registers only)" if ip else None},
         "e2e": {"value": world * n / e2e_t, "unit": "reads/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
@@ -408,7 +439,7 @@ def main():
     }
     if learned is not None:
         line["learned"] = learned
-    if rank == 0 and world == 1 and not args.no_cpu_baseline and os.path.exists(CARE_CPU):
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and not uneven and os.path.exists(CARE_CPU):
         threads = host_cores()
         progress(f"e2e done; care-cpu sample on {threads} threads")
         v = care_cpu_sample(tmp, threads)

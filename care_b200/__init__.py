@@ -80,7 +80,27 @@ EXPORTS = [
     "care_b200_mlp_create", "care_b200_mlp_destroy", "care_b200_mlp_last_error", "care_b200_mlp_set_params",
     "care_b200_mlp_get_params", "care_b200_mlp_init", "care_b200_mlp_set_data", "care_b200_mlp_train",
     "care_b200_mlp_gradient", "care_b200_mlp_train_step", "care_b200_mlp_forward",
+    "care_b200_default_tuning", "care_b200_set_tuning", "care_b200_get_tuning",
 ]
+
+
+class Tuning(ctypes.Structure):
+    """care_b200_tuning: launch mapping of a batch (results do not depend on it)."""
+    _fields_ = [("msa_order", ctypes.c_int), ("msa_queue", ctypes.c_int), ("msa_warps", ctypes.c_int),
+                ("align_block", ctypes.c_int), ("pair_order", ctypes.c_int), ("graph", ctypes.c_int)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+    @classmethod
+    def from_dict(cls, d):
+        t = cls()
+        load_library().care_b200_default_tuning(ctypes.byref(t))
+        for k, v in d.items():
+            if not hasattr(t, k):
+                raise TypeError(f"unknown tuning field {k}")
+            setattr(t, k, int(v))
+        return t
 
 MLP_FEATURES = 24
 MLP_HIDDEN = 64
@@ -174,6 +194,9 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.care_b200_mlp_gradient.argtypes = [c_mlp, fp, fp, fp, ctypes.c_uint64, fp, fp]
     lib.care_b200_mlp_train_step.argtypes = [c_mlp, fp, fp, fp, ctypes.c_uint64, P(TrainOptions), fp]
     lib.care_b200_mlp_forward.argtypes = [c_mlp, fp, ctypes.c_uint64, fp]
+    lib.care_b200_default_tuning.argtypes = [P(Tuning)]
+    lib.care_b200_set_tuning.argtypes = [c_ctx, P(Tuning)]
+    lib.care_b200_get_tuning.argtypes = [c_ctx, P(Tuning)]
     lib.care_b200_num_reads.argtypes = [c_ctx]
     lib.care_b200_num_reads.restype = ctypes.c_uint32
     lib.care_b200_max_length.argtypes = [c_ctx]
@@ -354,6 +377,18 @@ class Corrector:
     def write_output(self, path: str):
         self._check(self.lib.care_b200_write_output(self._ctx, path.encode()), "write_output")
 
+    # -- launch mapping --------------------------------------------------------
+    @property
+    def tuning(self) -> dict:
+        t = Tuning()
+        self._check(self.lib.care_b200_get_tuning(self._ctx, ctypes.byref(t)), "get_tuning")
+        return t.as_dict()
+
+    @tuning.setter
+    def tuning(self, d: dict):
+        t = Tuning.from_dict(d)
+        self._check(self.lib.care_b200_set_tuning(self._ctx, ctypes.byref(t)), "set_tuning")
+
     # -- learned decision ------------------------------------------------------
     def set_mlp(self, params: np.ndarray):
         p = np.ascontiguousarray(params, dtype=np.float32)
@@ -387,9 +422,9 @@ class Corrector:
         }
 
     def last_stats(self):
-        st = (ctypes.c_uint64 * 3)()
-        self._check(self.lib.care_b200_last_stats(self._ctx, st, 3), "last_stats")
-        return {"anchors": st[0], "pairs": st[1], "candidate_corrections": st[2]}
+        st = (ctypes.c_uint64 * 4)()
+        self._check(self.lib.care_b200_last_stats(self._ctx, st, 4), "last_stats")
+        return {"anchors": st[0], "pairs": st[1], "candidate_corrections": st[2], "word_compares": st[3]}
 
     def last_timing(self):
         """(total ms, [candidates, alignment, MSA, classifier] ms) of the last call."""

@@ -105,10 +105,16 @@ struct care_b200_ctx {
     std::vector<float> r_fx, r_flogit;
     std::vector<uint32_t> r_fread, r_fmeta;
 
+    // launch mapping (care_b200_set_tuning) and its scratch
+    care_b200_tuning tune{0, 0, 4, 128, 0, 0};
+    DBuf d_order, d_bins, d_pair_order;
+    cudaGraphExec_t gexec = nullptr;
+    int sms = 0;
+
     // results of the last call (pinned host)
     HBuf r_status, r_nedits, r_seq;
     HBuf r_cid, r_canc, r_cshift, r_cue, r_cseq;
-    uint64_t r_ncand = 0, r_pairs = 0;
+    uint64_t r_ncand = 0, r_pairs = 0, r_words = 0;
     uint32_t r_first = 0, r_count = 0;
     bool r_valid = false;
 };
@@ -252,6 +258,7 @@ int care_b200_destroy(care_b200_ctx* ctx) {
     cudaSetDevice(ctx->opt.device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     for (auto& e : ctx->ev) if (e) cudaEventDestroy(e);
+    if (ctx->gexec) cudaGraphExecDestroy(ctx->gexec);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return CARE_B200_OK;
@@ -432,11 +439,84 @@ int care_b200_get_table(care_b200_ctx* ctx, int map, const uint64_t** keys, cons
 
 namespace {
 
-// Runs the three stages for anchors [first, first+count) into the device
-// output buffers; grows the arenas and repeats on overflow.
+// ---- launch dispatch of the tuned stage mappings ----
+
+struct AlignArgs {
+    DevOptions o; DevReads r; uint32_t first;
+    const uint32_t* cand_ids; const uint32_t* cand_anchor; const uint32_t* seg_off; const uint32_t* seg_cnt;
+    const unsigned long long* total; unsigned long long cap; const int* status; AlignRes* out;
+    unsigned long long* words; const uint32_t* pair_order;
+};
+
+template <int B, int NW>
+cudaError_t align_go(const AlignArgs& a, cudaStream_t st) {
+    const unsigned long long blocks = (a.cap + B - 1) / B;
+    k_align<B, NW><<<(unsigned)blocks, B, 0, st>>>(a.o, a.r, a.first, a.cand_ids, a.cand_anchor, a.seg_off,
+                                                   a.seg_cnt, a.total, a.cap, a.status, a.out, a.words,
+                                                   a.pair_order);
+    return cudaGetLastError();
+}
+
+cudaError_t align_dispatch(int block, int nw, const AlignArgs& a, cudaStream_t st) {
+#define AL(B)                                       \
+    if (nw <= 4) return align_go<B, 4>(a, st);      \
+    if (nw <= 5) return align_go<B, 5>(a, st);      \
+    if (nw <= 6) return align_go<B, 6>(a, st);      \
+    return align_go<B, 8>(a, st);
+    if (block == 256) { AL(256) }
+    AL(128)
+#undef AL
+}
+
+struct MsaArgs {
+    DevOptions o; DevReads r; uint32_t first, count;
+    const uint32_t* order; unsigned int* cursor;
+    const uint32_t* cand_ids; const uint32_t* seg_off; const uint32_t* seg_cnt; const AlignRes* ares;
+    CandRec* recs; MsaOut out; int* status; size_t smem;
+    bool queue; int sms; int grid;             // grid: resident CTAs of the queue form (prepare)
+};
+
+// prepare (host only: attributes, occupancy) or launch one MSA variant
+template <int B, int JB, bool E>
+cudaError_t msa_go(MsaArgs& a, bool prepare, cudaStream_t st) {
+    if (prepare) {
+        cudaError_t e = cudaFuncSetAttribute(k_msa<B, JB, E>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)a.smem);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k_msa_queue<B, JB, E>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)a.smem);
+        int nb = 0;
+        if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_msa_queue<B, JB, E>, B, a.smem);
+        a.grid = (int)std::min<uint64_t>(a.count, (uint64_t)a.sms * (uint64_t)std::max(nb, 1));
+        return e;
+    }
+    if (a.queue)
+        k_msa_queue<B, JB, E><<<a.grid, B, a.smem, st>>>(a.o, a.r, a.first, a.count, a.order, a.cursor, a.cand_ids,
+                                                        a.seg_off, a.seg_cnt, a.ares, a.recs, a.out, a.status);
+    else
+        k_msa<B, JB, E><<<a.count, B, a.smem, st>>>(a.o, a.r, a.first, a.count, a.order, a.cand_ids, a.seg_off,
+                                                    a.seg_cnt, a.ares, a.recs, a.out, a.status);
+    return cudaGetLastError();
+}
+
+cudaError_t msa_dispatch(int warps, int jb, bool emit, MsaArgs& a, bool prepare, cudaStream_t st) {
+#define MS(B, J) return emit ? msa_go<B, J, true>(a, prepare, st) : msa_go<B, J, false>(a, prepare, st);
+    if (warps == 8) {
+        switch (jb) { case 1: MS(256, 1) case 2: MS(256, 2) default: MS(256, 3) }
+    }
+    switch (jb) {
+        case 1: MS(128, 1) case 2: MS(128, 2) case 3: MS(128, 3)
+        case 4: MS(128, 4) case 5: MS(128, 5) default: MS(128, 6)
+    }
+#undef MS
+}
+
+// Runs the stages for anchors [first, first+count) into the device output
+// buffers; grows the arenas and repeats on overflow. With tune.graph each
+// attempt's launches, memsets and copies are captured and replayed as one
+// CUDA graph (the instantiated graph is updated in place for the next batch).
 int run_batch(care_b200_ctx* ctx, uint32_t first, uint32_t count, bool timed) {
     const DevOptions o = make_dev_options(ctx);
     const DevReads r = make_dev_reads(ctx);
+    const care_b200_tuning& tu = ctx->tune;
     const int h = ctx->num_maps;
     // shared hash set for de-duplication: > num_maps * threshold entries
     const size_t tmax = (size_t)h * ctx->threshold;
@@ -446,6 +526,7 @@ int run_batch(care_b200_ctx* ctx, uint32_t first, uint32_t count, bool timed) {
     const size_t cand_smem = CandSmem::total(ctx->max_len, groups, h, ctx->seq_pitch, 1 << set_log2);
     if (cand_smem > 227 * 1024) return fail(ctx, CARE_B200_ELIMIT, "num_maps * threshold too large for the de-duplication set");
     CK(cudaFuncSetAttribute(k_candidates<kCandBlock>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cand_smem), "smem attr");
+    if (ctx->sms == 0) CK(cudaDeviceGetAttribute(&ctx->sms, cudaDevAttrMultiProcessorCount, ctx->opt.device), "attr");
 
     CK(ctx->d_seg_off.ensure((size_t)count * 4), "alloc");
     CK(ctx->d_seg_cnt.ensure((size_t)count * 4), "alloc");
@@ -455,6 +536,10 @@ int run_batch(care_b200_ctx* ctx, uint32_t first, uint32_t count, bool timed) {
     CK(ctx->d_ned.ensure((size_t)count * 4), "alloc");
     CK(ctx->d_oseq.ensure((size_t)count * ctx->max_len), "alloc");
     CK(ctx->h_small.ensure(64), "alloc");
+    if (tu.msa_order) {
+        CK(ctx->d_order.ensure((size_t)count * 4), "alloc");
+        CK(ctx->d_bins.ensure(kLptBins * 4), "alloc");
+    }
     if (ctx->cand_cap < (unsigned long long)count * 96) ctx->cand_cap = (unsigned long long)count * 96;
     if (ctx->corr_cap == 0) ctx->corr_cap = ctx->opt.correct_candidates ? (unsigned long long)count * 16 + 1024 : 1024;
     const bool emit = o.clf_mode != 0;
@@ -463,6 +548,17 @@ int run_batch(care_b200_ctx* ctx, uint32_t first, uint32_t count, bool timed) {
         CK(ctx->d_touched.ensure(count), "alloc");
         CK(ctx->d_mlp_err.ensure(16), "alloc");
     }
+    // widest possible MSA: La + 2*Lmax - 2*minoverlap(La), maximised over La
+    int maxcols = 1;
+    for (int la = 1; la <= ctx->max_len; ++la) {
+        const int lo = (int)((float)la * ctx->opt.min_overlap_ratio);
+        const int mo = std::max(ctx->opt.min_overlap, lo);
+        maxcols = std::max(maxcols, la + 2 * ctx->max_len - 2 * std::min(mo, ctx->max_len));
+    }
+    const int warps = tu.msa_warps == 8 ? 8 : 4;
+    const int jb = (maxcols + 32 * warps - 1) / (32 * warps);
+    const int nw = (ctx->max_len + 31) / 32;           // bit-plane width: 32-base words of the longest read
+    const size_t msmem = msa_smem_bytes(ctx->max_len, ctx->seq_pitch, ctx->has_qual ? ctx->qual_pitch : 0, emit);
 
     for (int attempt = 0; attempt < 8; ++attempt) {
         const unsigned long long cap = ctx->cand_cap;
@@ -470,6 +566,7 @@ int run_batch(care_b200_ctx* ctx, uint32_t first, uint32_t count, bool timed) {
         CK(ctx->d_cand_anchor.ensure(cap * 4), "alloc candidates");
         CK(ctx->d_ares.ensure(cap * sizeof(AlignRes)), "alloc alignments");
         CK(ctx->d_recs.ensure(cap * sizeof(CandRec)), "alloc records");
+        if (tu.pair_order) CK(ctx->d_pair_order.ensure(cap * 4), "alloc pair order");
         const unsigned long long ccap = ctx->corr_cap;
         CK(ctx->d_cid.ensure(ccap * 4), "alloc");
         CK(ctx->d_canc.ensure(ccap * 4), "alloc");
@@ -482,38 +579,10 @@ int run_batch(care_b200_ctx* ctx, uint32_t first, uint32_t count, bool timed) {
             CK(ctx->d_fread.ensure(fcap * 4), "alloc decision rows");
             CK(ctx->d_fmeta.ensure(fcap * 4), "alloc decision rows");
             CK(ctx->d_flogit.ensure(fcap * 4), "alloc decision rows");
-            CK(cudaMemsetAsync(ctx->d_touched.p, 0, count, ctx->stream), "memset");
-            CK(cudaMemsetAsync(ctx->d_mlp_err.p, 0, 16, ctx->stream), "memset");
         }
-
         unsigned long long* counters = ctx->d_counters.as<unsigned long long>();
         int* status = ctx->d_status.as<int>();
-        CK(cudaMemsetAsync(counters, 0, 64, ctx->stream), "memset");
-        CK(cudaMemsetAsync(status, 0, 16, ctx->stream), "memset");
-        // rows of anchors that are not corrected read as zero bytes
-        CK(cudaMemsetAsync(ctx->d_oseq.p, 0, (size_t)count * ctx->max_len, ctx->stream), "memset");
-        if (timed) CK(cudaEventRecord(ctx->ev[0], ctx->stream), "event");
-        k_candidates<kCandBlock><<<count, kCandBlock, cand_smem, ctx->stream>>>(
-            o, r, ctx->d_tdesc.as<TableDesc>(), ctx->d_slots.as<Slot>(), ctx->d_values.as<uint32_t>(), first,
-            count, set_log2, ctx->d_cand_ids.as<uint32_t>(), ctx->d_cand_anchor.as<uint32_t>(),
-            ctx->d_seg_off.as<uint32_t>(), ctx->d_seg_cnt.as<uint32_t>(), counters, cap, status);
-        CK(cudaGetLastError(), "k_candidates");
-        if (timed) CK(cudaEventRecord(ctx->ev[1], ctx->stream), "event");
-        const unsigned long long ablocks = (cap + kAlignBlock - 1) / kAlignBlock;
-#define LAUNCH_ALIGN(NW)                                                                          \
-    k_align<kAlignBlock, NW><<<(unsigned)ablocks, kAlignBlock, 0, ctx->stream>>>(                 \
-        o, r, first, ctx->d_cand_ids.as<uint32_t>(), ctx->d_cand_anchor.as<uint32_t>(),           \
-        ctx->d_seg_off.as<uint32_t>(), ctx->d_seg_cnt.as<uint32_t>(), counters, cap, status,      \
-        ctx->d_ares.as<AlignRes>())
-        // bit-plane width: 32-base words covering the longest read
-        const int nw = (ctx->max_len + 31) / 32;
-        if (nw <= 4) LAUNCH_ALIGN(4);
-        else if (nw <= 5) LAUNCH_ALIGN(5);
-        else if (nw <= 6) LAUNCH_ALIGN(6);
-        else LAUNCH_ALIGN(8);
-#undef LAUNCH_ALIGN
-        CK(cudaGetLastError(), "k_align");
-        if (timed) CK(cudaEventRecord(ctx->ev[2], ctx->stream), "event");
+
         MsaOut mo;
         mo.status = ctx->d_st.as<uint8_t>();
         mo.nedits = ctx->d_ned.as<int32_t>();
@@ -530,70 +599,115 @@ int run_batch(care_b200_ctx* ctx, uint32_t first, uint32_t count, bool timed) {
         mo.feat_meta = emit ? ctx->d_fmeta.as<uint32_t>() : nullptr;
         mo.feat_count = counters + 2;
         mo.feat_cap = emit ? fcap : 0;
-        // widest possible MSA: La + 2*Lmax - 2*minoverlap(La), maximised over La
-        int maxcols = 1;
-        for (int la = 1; la <= ctx->max_len; ++la) {
-            const int lo = (int)((float)la * ctx->opt.min_overlap_ratio);
-            const int mo = std::max(ctx->opt.min_overlap, lo);
-            maxcols = std::max(maxcols, la + 2 * ctx->max_len - 2 * std::min(mo, ctx->max_len));
-        }
-        const int jb = (maxcols + 32 * (kMsaBlock / 32) - 1) / (32 * (kMsaBlock / 32));
-        const size_t msmem = msa_smem_bytes(ctx->max_len, ctx->seq_pitch, ctx->has_qual ? ctx->qual_pitch : 0, emit);
-#define LAUNCH_MSA_E(JB, E)                                                                             \
-    do {                                                                                                \
-        CK(cudaFuncSetAttribute(k_msa<kMsaBlock, JB, E>, cudaFuncAttributeMaxDynamicSharedMemorySize,    \
-                                (int)msmem), "smem attr");                                              \
-        k_msa<kMsaBlock, JB, E><<<count, kMsaBlock, msmem, ctx->stream>>>(                              \
-            o, r, first, count, nullptr, ctx->d_cand_ids.as<uint32_t>(), ctx->d_seg_off.as<uint32_t>(), \
-            ctx->d_seg_cnt.as<uint32_t>(), ctx->d_ares.as<AlignRes>(), ctx->d_recs.as<CandRec>(), mo,   \
-            status);                                                                                    \
-    } while (0)
-#define LAUNCH_MSA(JB)                          \
-    do {                                        \
-        if (emit) LAUNCH_MSA_E(JB, true);       \
-        else LAUNCH_MSA_E(JB, false);           \
-    } while (0)
-        if (jb <= 1) LAUNCH_MSA(1);
-        else if (jb <= 2) LAUNCH_MSA(2);
-        else if (jb <= 3) LAUNCH_MSA(3);
-        else if (jb <= 4) LAUNCH_MSA(4);
-        else if (jb <= 5) LAUNCH_MSA(5);
-        else LAUNCH_MSA(6);
-#undef LAUNCH_MSA
-#undef LAUNCH_MSA_E
-        CK(cudaGetLastError(), "k_msa");
-        if (timed) CK(cudaEventRecord(ctx->ev[3], ctx->stream), "event");
-        if (o.clf_mode == 2) {
-            // the network decides the batch's decision columns (row count
-            // read on the device), then the changed anchors' edit counts
-            CK(mlp_infer(ctx->d_mlp.as<float>(), ctx->d_fx.as<float>(), fcap, counters + 2,
-                         ctx->d_flogit.as<float>(), ctx->d_mlp_err.as<int>(), ctx->stream), "k_mlp_infer");
-            int sms = 148;
-            CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->opt.device), "attr");
-            k_clf_apply<<<sms * 4, 256, 0, ctx->stream>>>(ctx->d_fread.as<uint32_t>(), ctx->d_fmeta.as<uint32_t>(),
+
+        AlignArgs aa{o, r, first, ctx->d_cand_ids.as<uint32_t>(), ctx->d_cand_anchor.as<uint32_t>(),
+                     ctx->d_seg_off.as<uint32_t>(), ctx->d_seg_cnt.as<uint32_t>(), counters, cap, status,
+                     ctx->d_ares.as<AlignRes>(), counters + 3,
+                     tu.pair_order ? ctx->d_pair_order.as<uint32_t>() : nullptr};
+        MsaArgs ma{o, r, first, count, tu.msa_order ? ctx->d_order.as<uint32_t>() : nullptr,
+                   reinterpret_cast<unsigned int*>(counters + 4), ctx->d_cand_ids.as<uint32_t>(),
+                   ctx->d_seg_off.as<uint32_t>(), ctx->d_seg_cnt.as<uint32_t>(), ctx->d_ares.as<AlignRes>(),
+                   ctx->d_recs.as<CandRec>(), mo, status, msmem, tu.msa_queue != 0, ctx->sms, 0};
+        CK(msa_dispatch(warps, jb, emit, ma, true, ctx->stream), "MSA launch setup");
+
+        cudaStream_t st = ctx->stream;
+        const bool graph = tu.graph != 0;
+        auto mark = [&](int k) -> cudaError_t {
+            if (!timed) return cudaSuccess;
+            return graph ? cudaEventRecordWithFlags(ctx->ev[k], st, cudaEventRecordExternal)
+                         : cudaEventRecord(ctx->ev[k], st);
+        };
+        // every operation of one attempt, in stream order
+        auto enqueue = [&]() -> int {
+#define EQ(call, where) do { const cudaError_t e_ = (call); if (e_ != cudaSuccess) return cuda_fail(ctx, e_, where); } while (0)
+            EQ(cudaMemsetAsync(counters, 0, 64, st), "memset");
+            EQ(cudaMemsetAsync(status, 0, 16, st), "memset");
+            // rows of anchors that are not corrected read as zero bytes
+            EQ(cudaMemsetAsync(ctx->d_oseq.p, 0, (size_t)count * ctx->max_len, st), "memset");
+            if (emit) {
+                EQ(cudaMemsetAsync(ctx->d_touched.p, 0, count, st), "memset");
+                EQ(cudaMemsetAsync(ctx->d_mlp_err.p, 0, 16, st), "memset");
+            }
+            EQ(mark(0), "event");
+            k_candidates<kCandBlock><<<count, kCandBlock, cand_smem, st>>>(
+                o, r, ctx->d_tdesc.as<TableDesc>(), ctx->d_slots.as<Slot>(), ctx->d_values.as<uint32_t>(), first,
+                count, set_log2, ctx->d_cand_ids.as<uint32_t>(), ctx->d_cand_anchor.as<uint32_t>(),
+                ctx->d_seg_off.as<uint32_t>(), ctx->d_seg_cnt.as<uint32_t>(), counters, cap, status);
+            EQ(cudaGetLastError(), "k_candidates");
+            EQ(mark(1), "event");
+            if (tu.pair_order) {
+                k_pair_order<<<count, 128, 0, st>>>(r, ctx->d_cand_ids.as<uint32_t>(), ctx->d_seg_off.as<uint32_t>(),
+                                                    ctx->d_seg_cnt.as<uint32_t>(), count, status,
+                                                    ctx->d_pair_order.as<uint32_t>());
+                EQ(cudaGetLastError(), "k_pair_order");
+            }
+            EQ(align_dispatch(tu.align_block, nw, aa, st), "k_align");
+            EQ(mark(2), "event");
+            if (tu.msa_order) {
+                const unsigned g = (unsigned)std::min<uint64_t>(((uint64_t)count + 255) / 256, (uint64_t)ctx->sms * 8);
+                EQ(cudaMemsetAsync(ctx->d_bins.p, 0, kLptBins * 4, st), "memset");
+                k_lpt_hist<<<g, 256, 0, st>>>(ctx->d_seg_cnt.as<uint32_t>(), count, ctx->d_bins.as<unsigned int>());
+                k_lpt_scan<<<1, 1024, 0, st>>>(ctx->d_bins.as<unsigned int>());
+                k_lpt_scatter<<<g, 256, 0, st>>>(ctx->d_seg_cnt.as<uint32_t>(), count, ctx->d_bins.as<unsigned int>(),
+                                                 ctx->d_order.as<uint32_t>());
+                EQ(cudaGetLastError(), "LPT order");
+            }
+            EQ(msa_dispatch(warps, jb, emit, ma, false, st), "k_msa");
+            EQ(mark(3), "event");
+            if (o.clf_mode == 2) {
+                // the network decides the batch's decision columns (row count
+                // read on the device), then the changed anchors' edit counts
+                EQ(mlp_infer(ctx->d_mlp.as<float>(), ctx->d_fx.as<float>(), fcap, counters + 2,
+                             ctx->d_flogit.as<float>(), ctx->d_mlp_err.as<int>(), st), "k_mlp_infer");
+                k_clf_apply<<<ctx->sms * 4, 256, 0, st>>>(ctx->d_fread.as<uint32_t>(), ctx->d_fmeta.as<uint32_t>(),
                                                           ctx->d_flogit.as<float>(), counters + 2, fcap, first,
-                                                          ctx->max_len, ctx->d_oseq.as<char>(), ctx->d_touched.as<uint8_t>());
-            CK(cudaGetLastError(), "k_clf_apply");
-            k_clf_recount<<<(count + 7) / 8, 256, 0, ctx->stream>>>(r, first, count, ctx->d_touched.as<uint8_t>(),
-                                                                   ctx->d_oseq.as<char>(), ctx->d_st.as<uint8_t>(),
-                                                                   ctx->d_ned.as<int32_t>());
-            CK(cudaGetLastError(), "k_clf_recount");
+                                                          ctx->max_len, ctx->d_oseq.as<char>(),
+                                                          ctx->d_touched.as<uint8_t>());
+                EQ(cudaGetLastError(), "k_clf_apply");
+                k_clf_recount<<<(count + 7) / 8, 256, 0, st>>>(r, first, count, ctx->d_touched.as<uint8_t>(),
+                                                               ctx->d_oseq.as<char>(), ctx->d_st.as<uint8_t>(),
+                                                               ctx->d_ned.as<int32_t>());
+                EQ(cudaGetLastError(), "k_clf_recount");
+            }
+            EQ(mark(4), "event");
+            EQ(cudaMemcpyAsync(ctx->h_small.p, counters, 32, cudaMemcpyDeviceToHost, st), "counters");
+            EQ(cudaMemcpyAsync(ctx->h_small.as<char>() + 32, status, 4, cudaMemcpyDeviceToHost, st), "status");
+            if (o.clf_mode == 2)
+                EQ(cudaMemcpyAsync(ctx->h_small.as<char>() + 36, ctx->d_mlp_err.p, 4, cudaMemcpyDeviceToHost, st), "status");
+#undef EQ
+            return CARE_B200_OK;
+        };
+        if (graph) {
+            CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "begin capture");
+            const int rc = enqueue();
+            cudaGraph_t g = nullptr;
+            const cudaError_t ee = cudaStreamEndCapture(st, &g);
+            if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+            CK(ee, "end capture");
+            cudaError_t ge = cudaErrorUnknown;
+            if (ctx->gexec) {
+                cudaGraphExecUpdateResultInfo info;
+                ge = cudaGraphExecUpdate(ctx->gexec, g, &info);
+                if (ge != cudaSuccess) { cudaGetLastError(); cudaGraphExecDestroy(ctx->gexec); ctx->gexec = nullptr; }
+            }
+            if (!ctx->gexec) ge = cudaGraphInstantiate(&ctx->gexec, g, 0);
+            cudaGraphDestroy(g);
+            CK(ge, "instantiate graph");
+            CK(cudaGraphLaunch(ctx->gexec, st), "graph launch");
+        } else {
+            if (int rc = enqueue()) return rc;
         }
-        if (timed) CK(cudaEventRecord(ctx->ev[4], ctx->stream), "event");
-        CK(cudaMemcpyAsync(ctx->h_small.p, counters, 24, cudaMemcpyDeviceToHost, ctx->stream), "counters");
-        CK(cudaMemcpyAsync(ctx->h_small.as<char>() + 32, status, 4, cudaMemcpyDeviceToHost, ctx->stream), "status");
-        if (o.clf_mode == 2)
-            CK(cudaMemcpyAsync(ctx->h_small.as<char>() + 36, ctx->d_mlp_err.p, 4, cudaMemcpyDeviceToHost, ctx->stream), "status");
-        CK(cudaStreamSynchronize(ctx->stream), "batch");
+        CK(cudaStreamSynchronize(st), "batch");
         const unsigned long long used = ctx->h_small.as<unsigned long long>()[0];
         const unsigned long long corr = ctx->h_small.as<unsigned long long>()[1];
         const unsigned long long nfeat = ctx->h_small.as<unsigned long long>()[2];
-        const int st = *(int*)(ctx->h_small.as<char>() + 32);
-        if (st & kStatusColumns) return fail(ctx, CARE_B200_ELIMIT, "MSA wider than the kernel's column capacity");
+        const unsigned long long words = ctx->h_small.as<unsigned long long>()[3];
+        const int stw = *(int*)(ctx->h_small.as<char>() + 32);
+        if (stw & kStatusColumns) return fail(ctx, CARE_B200_ELIMIT, "MSA wider than the kernel's column capacity");
         bool again = false;
-        if ((st & kStatusCandOverflow) || used > cap) { ctx->cand_cap = used + used / 8 + 1024; again = true; }
-        if ((st & kStatusCorrOverflow) || corr > ccap) { ctx->corr_cap = corr + corr / 8 + 1024; again = true; }
-        if (emit && ((st & kStatusFeatOverflow) || nfeat > fcap)) { ctx->feat_cap = nfeat + nfeat / 8 + 4096; again = true; }
+        if ((stw & kStatusCandOverflow) || used > cap) { ctx->cand_cap = used + used / 8 + 1024; again = true; }
+        if ((stw & kStatusCorrOverflow) || corr > ccap) { ctx->corr_cap = corr + corr / 8 + 1024; again = true; }
+        if (emit && ((stw & kStatusFeatOverflow) || nfeat > fcap)) { ctx->feat_cap = nfeat + nfeat / 8 + 4096; again = true; }
         if (again) continue;
         if (o.clf_mode == 2 && *(int*)(ctx->h_small.as<char>() + 36))
             return fail(ctx, CARE_B200_ECUDA, "tensor-core completion wait ran out");
@@ -611,17 +725,18 @@ int run_batch(care_b200_ctx* ctx, uint32_t first, uint32_t count, bool timed) {
             ctx->r_fx.resize((b0 + nfeat) * kNumFeatures);
             ctx->r_fread.resize(b0 + nfeat);
             ctx->r_fmeta.resize(b0 + nfeat);
-            CK(cudaMemcpyAsync(ctx->r_fx.data() + b0 * kNumFeatures, ctx->d_fx.p, nfeat * kNumFeatures * 4, cudaMemcpyDeviceToHost, ctx->stream), "rows");
-            CK(cudaMemcpyAsync(ctx->r_fread.data() + b0, ctx->d_fread.p, nfeat * 4, cudaMemcpyDeviceToHost, ctx->stream), "rows");
-            CK(cudaMemcpyAsync(ctx->r_fmeta.data() + b0, ctx->d_fmeta.p, nfeat * 4, cudaMemcpyDeviceToHost, ctx->stream), "rows");
+            CK(cudaMemcpyAsync(ctx->r_fx.data() + b0 * kNumFeatures, ctx->d_fx.p, nfeat * kNumFeatures * 4, cudaMemcpyDeviceToHost, st), "rows");
+            CK(cudaMemcpyAsync(ctx->r_fread.data() + b0, ctx->d_fread.p, nfeat * 4, cudaMemcpyDeviceToHost, st), "rows");
+            CK(cudaMemcpyAsync(ctx->r_fmeta.data() + b0, ctx->d_fmeta.p, nfeat * 4, cudaMemcpyDeviceToHost, st), "rows");
             if (o.clf_mode == 2) {
                 ctx->r_flogit.resize(b0 + nfeat);
-                CK(cudaMemcpyAsync(ctx->r_flogit.data() + b0, ctx->d_flogit.p, nfeat * 4, cudaMemcpyDeviceToHost, ctx->stream), "rows");
+                CK(cudaMemcpyAsync(ctx->r_flogit.data() + b0, ctx->d_flogit.p, nfeat * 4, cudaMemcpyDeviceToHost, st), "rows");
             }
-            CK(cudaStreamSynchronize(ctx->stream), "rows");
+            CK(cudaStreamSynchronize(st), "rows");
         }
         ctx->r_ncand += corr;
         ctx->r_pairs += used;
+        ctx->r_words += words;
         return (int)std::min<unsigned long long>(corr, 0x7fffffff);
     }
     return fail(ctx, CARE_B200_ENOMEM, "arena growth did not converge");
@@ -643,6 +758,7 @@ int correct_impl(care_b200_ctx* ctx, uint32_t first, uint32_t count, care_b200_r
     ctx->stage_ms[0] = ctx->stage_ms[1] = ctx->stage_ms[2] = ctx->stage_ms[3] = 0.f;
     ctx->r_ncand = 0;
     ctx->r_pairs = 0;
+    ctx->r_words = 0;
     ctx->r_valid = false;
     const int L = ctx->max_len;
     if (copy) {
@@ -721,6 +837,28 @@ int care_b200_correct_range(care_b200_ctx* ctx, uint32_t first, uint32_t count, 
 
 int care_b200_correct_range_device(care_b200_ctx* ctx, uint32_t first, uint32_t count) {
     return correct_impl(ctx, first, count, nullptr, false);
+}
+
+int care_b200_default_tuning(care_b200_tuning* t) {
+    if (!t) return CARE_B200_EINVAL;
+    *t = care_b200_tuning{0, 0, 4, 128, 0, 0};
+    return CARE_B200_OK;
+}
+
+int care_b200_set_tuning(care_b200_ctx* ctx, const care_b200_tuning* t) {
+    if (!ctx || !t) return CARE_B200_EINVAL;
+    if ((t->msa_warps != 4 && t->msa_warps != 8) || (t->align_block != 128 && t->align_block != 256) ||
+        (unsigned)t->msa_order > 1 || (unsigned)t->msa_queue > 1 || (unsigned)t->pair_order > 1 ||
+        (unsigned)t->graph > 1)
+        return fail(ctx, CARE_B200_EINVAL, "invalid tuning");
+    ctx->tune = *t;
+    return CARE_B200_OK;
+}
+
+int care_b200_get_tuning(const care_b200_ctx* ctx, care_b200_tuning* t) {
+    if (!ctx || !t) return CARE_B200_EINVAL;
+    *t = ctx->tune;
+    return CARE_B200_OK;
 }
 
 int care_b200_set_mlp(care_b200_ctx* ctx, const float* params) {
@@ -850,8 +988,8 @@ int care_b200_last_timing(const care_b200_ctx* ctx, float* total_ms, float* stag
 
 int care_b200_last_stats(const care_b200_ctx* ctx, uint64_t* stats, int nstats) {
     if (!ctx || !stats) return CARE_B200_EINVAL;
-    const uint64_t v[3] = {ctx->r_count, ctx->r_pairs, ctx->r_ncand};
-    for (int i = 0; i < nstats && i < 3; i++) stats[i] = v[i];
+    const uint64_t v[4] = {ctx->r_count, ctx->r_pairs, ctx->r_ncand, ctx->r_words};
+    for (int i = 0; i < nstats && i < 4; i++) stats[i] = v[i];
     return CARE_B200_OK;
 }
 

@@ -324,6 +324,36 @@ CB_HD void shd_scan(uint32_t (&Sh)[NW + 2], uint32_t (&Sl)[NW + 2],
     }
 }
 
+// Sum of ceil(v/32) for v = 1..n (0 for n <= 0).
+CB_HD int words_prefix(int n) {
+    if (n <= 0) return 0;
+    const int q = n >> 5, r = n & 31;
+    return 16 * q * (q + 1) + (q + 1) * r;
+}
+
+// Un-pruned work of one orientation of shifted_hamming: 32-bit word
+// compares over every scanned shift, ceil(overlap/32) each. Closed form of
+// the two scans above: shifts t = 0..La-minov with overlap min(La-t, Lc),
+// then t = 1..Lc-minov with overlap min(La, Lc-t). 743 at La = Lc = 150.
+CB_HD int unpruned_words(int La, int Lc, int minov) {
+    int w = 0;
+    const int T0 = La - minov;
+    if (T0 >= 0) {
+        const int flat = La >= Lc ? min(T0, La - Lc) + 1 : 0;     // overlap == Lc
+        w += flat * ((Lc + 31) >> 5);
+        const int top = La - max(0, La - Lc + 1);                 // overlap La - t below that
+        if (top >= minov) w += words_prefix(top) - words_prefix(minov - 1);
+    }
+    const int T1 = Lc - minov;
+    if (T1 >= 1) {
+        const int flat = Lc > La ? min(T1, Lc - La) : 0;          // overlap == La
+        w += flat * ((La + 31) >> 5);
+        const int top = Lc - max(1, Lc - La + 1);
+        if (top >= minov) w += words_prefix(top) - words_prefix(minov - 1);
+    }
+    return w;
+}
+
 // cpuShiftedHammingDistancePopcount2BitHiLo (src/cpu_alignment.cpp:32-323):
 // shifts 0..La-minov (anchor slid against the candidate), then -1..-(Lc-minov)
 // (candidate slid against the anchor).

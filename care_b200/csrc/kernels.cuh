@@ -197,7 +197,8 @@ __global__ void __launch_bounds__(BLOCK)
 k_align(DevOptions o, DevReads r, uint32_t first, const uint32_t* __restrict__ cand_ids,
         const uint32_t* __restrict__ cand_anchor, const uint32_t* __restrict__ seg_off,
         const uint32_t* __restrict__ seg_cnt, const unsigned long long* __restrict__ total_ptr,
-        unsigned long long arena_cap, const int* __restrict__ status, AlignRes* __restrict__ out) {
+        unsigned long long arena_cap, const int* __restrict__ status, AlignRes* __restrict__ out,
+        unsigned long long* __restrict__ work_count, const uint32_t* __restrict__ pair_order) {
     __shared__ int s_mex[kMaxLen + 1];
     // int(float(ov) * maxErrorRate), the first term of max_errors_excl
     for (int i = threadIdx.x; i <= kMaxLen; i += BLOCK) s_mex[i] = __float2int_rz(__fmul_rn((float)i, o.max_error_rate));
@@ -205,9 +206,10 @@ k_align(DevOptions o, DevReads r, uint32_t first, const uint32_t* __restrict__ c
     // an overflowed candidate arena holds unwritten entries: the batch is
     // repeated with a larger arena, nothing here may read them
     if (*status & kStatusCandOverflow) return;
-    const unsigned long long i = (unsigned long long)blockIdx.x * BLOCK + threadIdx.x;
+    const unsigned long long slot = (unsigned long long)blockIdx.x * BLOCK + threadIdx.x;
     const unsigned long long total = *total_ptr;
-    if (total > arena_cap || i >= total) return;
+    if (total > arena_cap || slot >= total) return;
+    const unsigned long long i = pair_order ? pair_order[slot] : slot;
     const uint32_t ai = cand_anchor[i];
     const uint32_t a = first + ai;
     const uint32_t c = cand_ids[i];
@@ -217,6 +219,11 @@ k_align(DevOptions o, DevReads r, uint32_t first, const uint32_t* __restrict__ c
     load_planes<NW>(r.seq + (size_t)c * r.seq_pitch, Lc, Ch, Cl);
     const int lo = __float2int_rz(__fmul_rn((float)La, o.min_overlap_ratio));
     const int minov = o.min_overlap > lo ? o.min_overlap : lo;
+    if (work_count) {                 // un-pruned word compares, both orientations (roofline work)
+        const unsigned m = __activemask();
+        const unsigned ws = __reduce_add_sync(m, (unsigned)(2 * unpruned_words(La, Lc, minov)));
+        if ((int)(threadIdx.x & 31) == __ffs(m) - 1) atomicAdd(work_count, (unsigned long long)ws);
+    }
     const ShdResult f = shifted_hamming<NW>(Ah, Al, La, Ch, Cl, Lc, minov, s_mex);
     uint32_t Rh[NW + 2], Rl[NW + 2];
     revcomp_planes<NW>(Ch, Cl, Lc, Rh, Rl);
@@ -301,12 +308,14 @@ __host__ __device__ inline size_t msa_smem_bytes(int max_len, int seq_pitch, int
     return ((elem + 15) & ~(size_t)15) + raw + (emit ? (size_t)3 * max_len * 4 : 0);
 }
 
-template <int BLOCK, int JB, bool EMIT = false>
-__global__ void __launch_bounds__(BLOCK)
-k_msa(DevOptions o, DevReads r, uint32_t first, uint32_t count, const uint32_t* __restrict__ order,
-      const uint32_t* __restrict__ cand_ids, const uint32_t* __restrict__ seg_off,
-      const uint32_t* __restrict__ seg_cnt, const AlignRes* __restrict__ ares,
-      CandRec* __restrict__ recs, MsaOut out, int* __restrict__ status) {
+// The whole MSA stage of one anchor (local index ai) for one CTA. Every
+// early return is taken by all threads of the CTA together.
+template <int BLOCK, int JB, bool EMIT>
+__device__ __forceinline__ void
+msa_anchor(const DevOptions& o, const DevReads& r, uint32_t first, uint32_t ai,
+           const uint32_t* __restrict__ cand_ids, const uint32_t* __restrict__ seg_off,
+           const uint32_t* __restrict__ seg_cnt, const AlignRes* __restrict__ ares,
+           CandRec* __restrict__ recs, const MsaOut& out, int* __restrict__ status) {
     constexpr int NWARP = BLOCK / 32;
     constexpr int MAXCOLS = 32 * JB * NWARP;
     extern __shared__ __align__(16) unsigned char dsm[];
@@ -324,9 +333,6 @@ k_msa(DevOptions o, DevReads r, uint32_t first, uint32_t count, const uint32_t* 
     __shared__ int s_vals[12];
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    if (blockIdx.x >= count) return;
-    if (*status & kStatusCandOverflow) return;   // batch is repeated with a larger arena
-    const uint32_t ai = order ? order[blockIdx.x] : blockIdx.x;
     const uint32_t a = first + ai;
     const uint32_t off = seg_off[ai], cnt = seg_cnt[ai];
     const int La = r.len[a];
@@ -902,12 +908,110 @@ k_msa(DevOptions o, DevReads r, uint32_t first, uint32_t count, const uint32_t* 
                 dst[p] = "ACGT"[cs];
                 nd += cs != base_at(row, p);
             }
+            for (int p = L; p < mlen; ++p) dst[p] = 0;   // rows read as zero past the read
             out.corr_id[slot] = id;
             out.corr_anchor[slot] = a;
             out.corr_shift[slot] = shift;
             out.corr_use_edits[slot] = (!r.ambig[id] && nd <= L / 7) ? 1 : 0;
         }
     }
+}
+
+// One CTA per anchor, in `order` (e.g. most candidates first) when given;
+// the hardware block scheduler hands out the anchors.
+template <int BLOCK, int JB, bool EMIT = false>
+__global__ void __launch_bounds__(BLOCK)
+k_msa(DevOptions o, DevReads r, uint32_t first, uint32_t count, const uint32_t* __restrict__ order,
+      const uint32_t* __restrict__ cand_ids, const uint32_t* __restrict__ seg_off,
+      const uint32_t* __restrict__ seg_cnt, const AlignRes* __restrict__ ares,
+      CandRec* __restrict__ recs, MsaOut out, int* __restrict__ status) {
+    if (blockIdx.x >= count) return;
+    if (*status & kStatusCandOverflow) return;   // batch is repeated with a larger arena
+    msa_anchor<BLOCK, JB, EMIT>(o, r, first, order ? order[blockIdx.x] : blockIdx.x, cand_ids, seg_off,
+                                seg_cnt, ares, recs, out, status);
+}
+
+// Persistent form: a grid of resident CTAs pulls anchors from a device work
+// queue (an atomic cursor over `order`) until the batch is done.
+template <int BLOCK, int JB, bool EMIT = false>
+__global__ void __launch_bounds__(BLOCK)
+k_msa_queue(DevOptions o, DevReads r, uint32_t first, uint32_t count, const uint32_t* __restrict__ order,
+            unsigned int* __restrict__ cursor, const uint32_t* __restrict__ cand_ids,
+            const uint32_t* __restrict__ seg_off, const uint32_t* __restrict__ seg_cnt,
+            const AlignRes* __restrict__ ares, CandRec* __restrict__ recs, MsaOut out,
+            int* __restrict__ status) {
+    __shared__ uint32_t s_item;
+    if (*status & kStatusCandOverflow) return;
+    for (;;) {
+        __syncthreads();                      // the previous anchor is done with shared memory
+        if (threadIdx.x == 0) s_item = atomicAdd(cursor, 1u);
+        __syncthreads();
+        const uint32_t it = s_item;
+        if (it >= count) return;
+        msa_anchor<BLOCK, JB, EMIT>(o, r, first, order ? order[it] : it, cand_ids, seg_off, seg_cnt, ares,
+                                    recs, out, status);
+    }
+}
+
+// Longest-processing-time order of a batch's anchors: a counting sort by
+// candidate count, most candidates first (order within a count arbitrary:
+// anchors are independent, results are written by anchor index).
+constexpr int kLptBins = 4096;
+static __global__ void k_lpt_hist(const uint32_t* __restrict__ seg_cnt, uint32_t count,
+                                  unsigned int* __restrict__ bins) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x)
+        atomicAdd(&bins[kLptBins - 1 - min(seg_cnt[i], (uint32_t)(kLptBins - 1))], 1u);
+}
+// exclusive scan of the bins in place (one CTA of 1024 threads)
+static __global__ void k_lpt_scan(unsigned int* __restrict__ bins) {
+    __shared__ unsigned int s_part[1024];
+    constexpr int per = kLptBins / 1024;
+    const int t = threadIdx.x;
+    unsigned int loc[per], sum = 0;
+#pragma unroll
+    for (int k = 0; k < per; ++k) { loc[k] = bins[t * per + k]; sum += loc[k]; }
+    s_part[t] = sum;
+    __syncthreads();
+    for (int d = 1; d < 1024; d <<= 1) {
+        const unsigned int v = t >= d ? s_part[t - d] : 0u;
+        __syncthreads();
+        s_part[t] += v;
+        __syncthreads();
+    }
+    unsigned int run = s_part[t] - sum;
+#pragma unroll
+    for (int k = 0; k < per; ++k) { bins[t * per + k] = run; run += loc[k]; }
+}
+static __global__ void k_lpt_scatter(const uint32_t* __restrict__ seg_cnt, uint32_t count,
+                                     unsigned int* __restrict__ bins, uint32_t* __restrict__ order) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x)
+        order[atomicAdd(&bins[kLptBins - 1 - min(seg_cnt[i], (uint32_t)(kLptBins - 1))], 1u)] = i;
+}
+
+// Per-alignment order of each anchor's candidate segment by candidate length
+// (a counting sort over 16-base length classes, one CTA per anchor): warps of
+// k_align then hold pairs of similar scan length. Results stay at their pair
+// index, so the MSA still sees candidates in id order.
+static __global__ void k_pair_order(const DevReads r, const uint32_t* __restrict__ cand_ids,
+                                    const uint32_t* __restrict__ seg_off, const uint32_t* __restrict__ seg_cnt,
+                                    uint32_t count, const int* __restrict__ status,
+                                    uint32_t* __restrict__ pair_order) {
+    constexpr int NB = kMaxLen / 16 + 1;
+    __shared__ unsigned int s_bin[NB];
+    const uint32_t ai = blockIdx.x;
+    if (ai >= count || (*status & kStatusCandOverflow)) return;
+    const uint32_t off = seg_off[ai], cnt = seg_cnt[ai];
+    for (int b = threadIdx.x; b < NB; b += blockDim.x) s_bin[b] = 0;
+    __syncthreads();
+    for (uint32_t k = threadIdx.x; k < cnt; k += blockDim.x) atomicAdd(&s_bin[r.len[cand_ids[off + k]] >> 4], 1u);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned int run = 0;
+        for (int b = 0; b < NB; ++b) { const unsigned int c = s_bin[b]; s_bin[b] = run; run += c; }
+    }
+    __syncthreads();
+    for (uint32_t k = threadIdx.x; k < cnt; k += blockDim.x)
+        pair_order[off + atomicAdd(&s_bin[r.len[cand_ids[off + k]] >> 4], 1u)] = off + k;
 }
 
 // The network's verdict on each decision column of the batch: the consensus

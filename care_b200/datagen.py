@@ -199,9 +199,15 @@ def single_end_uneven(seed: int = 3, genome_size: int = 10_000_000,
     idx = np.minimum(idx, genome_size - 1)
     truth = genome[idx]
     rc = rng.random(n) < 0.5
-    for i in np.nonzero(rc)[0]:
-        L = lengths[i]
-        truth[i, :L] = revcomp_codes(truth[i, :L])
+    # reverse-complement the first L bases of the rows drawn for the minus strand
+    j = np.arange(Lmax)[None, :]
+    rows = np.nonzero(rc)[0]
+    for b in range(0, rows.shape[0], 100_000):
+        r = rows[b:b + 100_000]
+        Lr = lengths[r][:, None]
+        src = np.where(j < Lr, Lr - 1 - j, j)
+        sub = np.take_along_axis(truth[r], src, axis=1)
+        truth[r] = np.where(j < Lr, 3 - sub, sub)
     codes, q, valid = _pos_dependent_errors(rng, truth, lengths)
     return _finish(codes, truth, q, valid, lengths, False, "se_uneven")
 

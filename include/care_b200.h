@@ -61,8 +61,8 @@ typedef struct care_b200_ctx care_b200_ctx;
  * anchor_status bits: 1 = corrected, 2 = high quality (HQ) MSA,
  * 4 = store as edit list (the reference's useEdits, corrector.hpp:1648-1675).
  * Candidate corrections are in forward read orientation
- * (corrector.hpp:1679-1757). Sequences are max_length bytes per row; rows
- * of anchors that were not corrected are zero. */
+ * (corrector.hpp:1679-1757). Sequences are max_length bytes per row, zero
+ * past the read's length; rows of anchors that were not corrected are zero. */
 typedef struct care_b200_results {
     uint32_t        first_anchor;
     uint32_t        num_anchors;
@@ -158,7 +158,9 @@ int care_b200_write_output(care_b200_ctx* ctx, const char* outfile);
 int care_b200_last_timing(const care_b200_ctx* ctx, float* total_ms, float* stage_ms, int nstages);
 
 /* Counters of the last correction call: stats[0] anchors, stats[1]
- * (anchor, candidate) pairs aligned, stats[2] candidate corrections. */
+ * (anchor, candidate) pairs aligned, stats[2] candidate corrections,
+ * stats[3] un-pruned 32-bit word compares of the alignments (both
+ * orientations, every scanned shift: the alignment stage's roofline work). */
 int care_b200_last_stats(const care_b200_ctx* ctx, uint64_t* stats, int nstats);
 
 /* ---- correction without allocation ---- */
@@ -299,6 +301,24 @@ int care_b200_mlp_train_step(care_b200_mlp* m, const float* x, const float* labe
                              uint64_t n, const care_b200_mlp_train_options* o, float* loss);
 /* logits of host rows */
 int care_b200_mlp_forward(care_b200_mlp* m, const float* x, uint64_t n, float* logits);
+
+/* ---- launch mapping (tuning) ----
+ *
+ * How the batch's work is mapped onto the GPU; the results do not depend on
+ * it (every variant is byte-identical). care_b200.autotune measures the
+ * variants on a sample of a workload and commits the fastest per workload. */
+typedef struct care_b200_tuning {
+    int msa_order;     /* 1: anchors in longest-processing-time order (most candidates first) */
+    int msa_queue;     /* 1: persistent MSA CTAs pulling anchors from a device work queue */
+    int msa_warps;     /* warps per anchor in the MSA stage: 4 or 8 */
+    int align_block;   /* threads per CTA of the alignment stage: 128 or 256 */
+    int pair_order;    /* 1: alignment pairs packed by candidate length within each anchor */
+    int graph;         /* 1: each batch's launches replayed as one CUDA graph */
+} care_b200_tuning;
+
+int care_b200_default_tuning(care_b200_tuning* t);
+int care_b200_set_tuning(care_b200_ctx* ctx, const care_b200_tuning* t);
+int care_b200_get_tuning(const care_b200_ctx* ctx, care_b200_tuning* t);
 
 /* Read-storage facts after upload. */
 uint32_t care_b200_num_reads(const care_b200_ctx* ctx);

@@ -55,4 +55,6 @@ void hd_canonical_kmers(const uint32_t* seq, int len, int k, unsigned long long*
 }
 
 unsigned long long hd_murmur64(unsigned long long x) { return murmur64(x); }
+
+int hd_unpruned_words(int la, int lc, int minov) { return unpruned_words(la, lc, minov); }
 }

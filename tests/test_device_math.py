@@ -29,6 +29,7 @@ def harness():
     lib.hd_canonical_kmers.argtypes = [P(ctypes.c_uint32), ctypes.c_int, ctypes.c_int, P(ctypes.c_uint64)]
     lib.hd_murmur64.argtypes = [ctypes.c_uint64]
     lib.hd_murmur64.restype = ctypes.c_uint64
+    lib.hd_unpruned_words.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int]
     return lib
 
 
@@ -102,3 +103,19 @@ def test_canonical_kmers(k):
 def test_murmur():
     for x in [0, 1, 7, 2 ** 40 + 3, 2 ** 64 - 1]:
         assert H.hd_murmur64(x) == O.co_murmur64(x)
+
+
+def test_unpruned_word_count_closed_form():
+    """The work counter of k_align (un-pruned 32-bit word compares of one
+    orientation) against a loop over the scanned shifts."""
+    def brute(la, lc, mo):
+        w = sum(-(-min(la - t, lc) // 32) for t in range(0, la - mo + 1) if min(la - t, lc) > 0)
+        w += sum(-(-min(la, lc - t) // 32) for t in range(1, lc - mo + 1) if min(la, lc - t) > 0)
+        return w
+    assert H.hd_unpruned_words(150, 150, 45) == 743
+    assert H.hd_unpruned_words(100, 100, 30) == 354
+    rng = random.Random(5)
+    for _ in range(3000):
+        la, lc = rng.randint(1, 256), rng.randint(1, 256)
+        mo = max(rng.randint(1, 80), int(la * 0.3))
+        assert H.hd_unpruned_words(la, lc, mo) == brute(la, lc, mo), (la, lc, mo)
