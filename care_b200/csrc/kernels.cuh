@@ -273,9 +273,10 @@ k_align(DevOptions o, DevReads r, uint32_t first, const uint32_t* __restrict__ c
 // first and then candidates in list order, with separate IEEE multiply and
 // add (no FMA) -- the reference's order and rounding, so the sums are
 // bit-identical. A warp skips a candidate that covers none of a block's
-// columns (a warp-uniform test). Candidate rows are decoded once into 16-bit
-// elements (2-bit base | quality character << 2) in shared memory and kept
-// across refinement rebuilds when the candidate list fits (kStage rows).
+// columns (a warp-uniform test). Candidate rows are staged in shared memory
+// as their packed sequence and quality words (all warps loading, eight rows
+// in flight per lane) and read in place; they stay staged across refinement
+// rebuilds when the candidate list fits (up to 128 rows in 16 KB).
 // ---------------------------------------------------------------------------
 struct MsaOut {
     uint8_t* status;
@@ -298,14 +299,22 @@ struct MsaOut {
 
 constexpr int kNumFeatures = 24;
 
-constexpr int kStage = 64;            // candidate rows held in shared memory
+constexpr int kStageMax = 128;        // candidate rows held in shared memory, at most
+constexpr int kStageBudget = 16384;   // bytes of staged packed rows
 
-// dynamic shared memory of k_msa: decoded rows (kStage + anchor) and raw
-// rows; with decision rows also three per-anchor-column weights
+// candidate rows staged at once: packed sequence + encoded quality words
+__host__ __device__ inline int msa_stage_rows(int seq_pitch, int qual_pitch) {
+    const int rows = kStageBudget / ((seq_pitch + qual_pitch) * 4);
+    return rows > kStageMax ? kStageMax : (rows < 16 ? 16 : rows);
+}
+
+// dynamic shared memory of k_msa: the anchor's decoded row, the staged
+// packed candidate rows; with decision rows also three per-anchor-column
+// weights
 __host__ __device__ inline size_t msa_smem_bytes(int max_len, int seq_pitch, int qual_pitch, bool emit = false) {
-    const size_t elem = (size_t)(kStage + 1) * max_len * 2;
-    const size_t raw = (size_t)kStage * (seq_pitch + qual_pitch) * 4;
-    return ((elem + 15) & ~(size_t)15) + raw + (emit ? (size_t)3 * max_len * 4 : 0);
+    const size_t elem = ((size_t)max_len * 2 + 15) & ~(size_t)15;
+    const size_t raw = (size_t)msa_stage_rows(seq_pitch, qual_pitch) * (seq_pitch + qual_pitch) * 4;
+    return elem + raw + (emit ? (size_t)3 * max_len * 4 : 0);
 }
 
 // The whole MSA stage of one anchor (local index ai) for one CTA. Every
@@ -324,11 +333,12 @@ msa_anchor(const DevOptions& o, const DevReads& r, uint32_t first, uint32_t ai,
     __shared__ uint16_t s_cov[MAXCOLS];
     __shared__ uint16_t s_cnt[MAXCOLS][4];
     __shared__ float s_qw[256];
-    __shared__ int s_beg[kStage], s_len[kStage];
-    __shared__ float s_w[kStage];
-    __shared__ uint32_t s_id[kStage];
-    __shared__ uint8_t s_fwd[kStage];
-    __shared__ uint8_t s_alive[kStage];
+    __shared__ float s_qwc[4];               // weight of a 1- or 2-bit quality code
+    __shared__ int s_beg[kStageMax], s_len[kStageMax];
+    __shared__ float s_w[kStageMax];
+    __shared__ uint32_t s_id[kStageMax];
+    __shared__ uint8_t s_fwd[kStageMax];
+    __shared__ uint8_t s_alive[kStageMax];
     __shared__ int s_red[NWARP][4];
     __shared__ int s_vals[12];
 
@@ -339,13 +349,13 @@ msa_anchor(const DevOptions& o, const DevReads& r, uint32_t first, uint32_t ai,
     const int mlen = r.max_len;
     const bool useQ = o.use_quality && r.qual != nullptr;
     char* aout = out.seq + (size_t)ai * mlen;
-    uint16_t* s_elem = (uint16_t*)dsm;                       // [kStage][mlen]
-    uint16_t* s_aelem = s_elem + (size_t)kStage * mlen;      // anchor row
-    uint32_t* s_rseq = (uint32_t*)(dsm + (((size_t)(kStage + 1) * mlen * 2 + 15) & ~(size_t)15));
-    uint32_t* s_rqual = s_rseq + (size_t)kStage * r.seq_pitch;
+    const int nstage = msa_stage_rows(r.seq_pitch, r.qual_pitch);
+    const int rw = r.seq_pitch + r.qual_pitch;               // words per staged row
+    uint16_t* s_aelem = (uint16_t*)dsm;                      // anchor row: base | quality char << 2
+    uint32_t* s_raw = (uint32_t*)(dsm + (((size_t)mlen * 2 + 15) & ~(size_t)15));   // [nstage][rw]
     // per anchor column: column weight sum, consensus weight, weight of the
     // anchor's base (EMIT only)
-    float* s_fw = (float*)(s_rqual + (size_t)kStage * r.qual_pitch);
+    float* s_fw = (float*)(s_raw + (size_t)nstage * rw);
 
     if (cnt == 0) {
         if (tid == 0) { out.status[ai] = 0; out.nedits[ai] = 0; }
@@ -450,6 +460,12 @@ msa_anchor(const DevOptions& o, const DevReads& r, uint32_t first, uint32_t ai,
     for (int i = tid; i < 256; i += BLOCK) s_qw[i] = c_qweight[i];
     const int qbits = o.quality_bits;
     const int sp = r.seq_pitch, qp = r.qual_pitch;
+    if (tid < 4) {
+        // the characters a 2- or 1-bit code stands for (qualityscorecompression.hpp:121-145)
+        const uint32_t ch = qbits == 2 ? (tid == 0 ? '$' : tid == 1 ? '(' : tid == 2 ? '1' : '9')
+                                       : (tid == 1 ? '5' : '(');
+        s_qwc[tid] = c_qweight[ch];
+    }
     // quality character at position q of an encoded row (qualityscorecompression.hpp:121-145)
     auto qual_char = [&](const uint32_t* row, int q) -> uint32_t {
         if (qbits == 8) return (row[q >> 2] >> (8 * (q & 3))) & 0xFFu;
@@ -469,47 +485,60 @@ msa_anchor(const DevOptions& o, const DevReads& r, uint32_t first, uint32_t ai,
         }
     }
 
-    // stage candidate rows [c, c+n) of recs into slots 0..n-1
-    // one warp per candidate row: lanes copy its packed words, then decode
-    // its bases and qualities position by position
+    // stage candidate rows [c, c+n) of recs into slots 0..n-1: their packed
+    // sequence and quality words, eight rows in flight per lane
     auto stage = [&](int c, int n) {
         __syncthreads();
-        for (int k = warp; k < n; k += NWARP) {
+        for (int k = tid; k < n; k += BLOCK) {
             const CandRec rc = recs[off + c + k];
-            const uint32_t* srow = r.seq + (size_t)rc.id * sp;
-            for (int w = lane; w < sp; w += 32) s_rseq[k * sp + w] = __ldg(srow + w);
-            if (useQ) {
-                const uint32_t* qrow = r.qual + (size_t)rc.id * qp;
-                for (int w = lane; w < qp; w += 32) s_rqual[k * qp + w] = __ldg(qrow + w);
-            }
-            if (lane == 0) {
-                s_beg[k] = rc.shift;            // relative to the anchor; abegin added per build
-                s_len[k] = rc.len;
-                s_w[k] = rc.weight;
-                s_fwd[k] = rc.orient == 1;
-                s_id[k] = rc.id;
-            }
+            s_beg[k] = rc.shift;                // relative to the anchor; abegin added per build
+            s_len[k] = rc.len;
+            s_w[k] = rc.weight;
+            s_fwd[k] = rc.orient == 1;
+            s_id[k] = rc.id;
         }
         __syncthreads();
-        for (int k = warp; k < n; k += NWARP) {
-            const int L = s_len[k];
-            const bool fwd = s_fwd[k];
-            const uint32_t* srow = s_rseq + k * sp;
-            const uint32_t* qrow = s_rqual + k * qp;
-            uint16_t* erow = s_elem + k * mlen;
-            for (int p = lane; p < L; p += 32) {
-                const uint32_t b = fwd ? base_at(srow, p) : (base_at(srow, L - 1 - p) ^ 3u);
-                // reverse-complement candidates read their qualities reversed
-                // over the whole quality pitch (reverseQualitiesOfRCAlignments,
-                // corrector.hpp:1227-1239)
-                const uint32_t q = useQ ? qual_char(qrow, fwd ? p : mlen - 1 - p) : 0u;
-                erow[p] = (uint16_t)(b | (q << 2));
+        for (int k0 = warp; k0 < n; k0 += 8 * NWARP) {
+            for (int w0 = 0; w0 < rw; w0 += 32) {
+                const int w = w0 + lane;
+                uint32_t v[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    const int k = k0 + u * NWARP;
+                    v[u] = 0u;
+                    if (k < n && w < rw) {
+                        const size_t id = s_id[k];
+                        v[u] = w < sp ? __ldg(r.seq + id * sp + w) : __ldg(r.qual + id * qp + (w - sp));
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    const int k = k0 + u * NWARP;
+                    if (k < n && w < rw) s_raw[k * rw + w] = v[u];
+                }
             }
         }
         __syncthreads();
     };
+    // base (2-bit, in the candidate's aligned orientation) of staged row k at
+    // position p < s_len[k]
+    auto cand_base = [&](int k, int p) -> uint32_t {
+        const uint32_t* srow = s_raw + k * rw;
+        if (s_fwd[k]) return base_at(srow, p);
+        return base_at(srow, s_len[k] - 1 - p) ^ 3u;
+    };
+    // quality weight of staged row k at position p; reverse-complement
+    // candidates read their qualities reversed over the whole quality pitch
+    // (reverseQualitiesOfRCAlignments, corrector.hpp:1227-1239)
+    auto cand_qweight = [&](int k, int p) -> float {
+        const uint32_t* qrow = s_raw + k * rw + sp;
+        const int q = s_fwd[k] ? p : mlen - 1 - p;
+        if (qbits == 2) return s_qwc[(qrow[q >> 4] >> (30 - 2 * (q & 15))) & 3u];
+        if (qbits == 8) return s_qw[(qrow[q >> 2] >> (8 * (q & 3))) & 0xFFu];
+        return s_qwc[(qrow[q >> 5] >> (31 - (q & 31))) & 1u];
+    };
 
-    const bool persistent = V <= kStage;      // all rows stay staged across rebuilds
+    const bool persistent = V <= nstage;      // all rows stay staged across rebuilds
     int nalive = V;
     if (persistent) {
         stage(0, V);
@@ -554,69 +583,95 @@ msa_anchor(const DevOptions& o, const DevReads& r, uint32_t first, uint32_t ai,
             return;
         }
 
-        // ---- column sums: anchor, then candidates in list order ----
-        unsigned long long cntp[JB];         // four 16-bit counts per column
-        float wA[JB], wC[JB], wG[JB], wT[JB];
-#pragma unroll
+        // ---- column sums (anchor first, then candidates in list order) and
+        //      consensus (findConsensus, msa.cpp:135-157): each warp takes one
+        //      32-column block at a time, lane = column ----
         for (int j = 0; j < JB; ++j) {
-            cntp[j] = 0ull;
-            wA[j] = wC[j] = wG[j] = wT[j] = 0.0f;
-            const int col = 32 * (warp + NWARP * j) + lane;
-            const int p = col - abegin;
-            if (p >= 0 && p < La) {
-                const uint32_t e = s_aelem[p];
-                const uint32_t b = e & 3u;
-                const float w = useQ ? s_qw[e >> 2] : 1.0f;   // factor 1.0f
-                cntp[j] = 1ull << (16 * b);
-                if (b == 0) wA[j] = w; else if (b == 1) wC[j] = w; else if (b == 2) wG[j] = w; else wT[j] = w;
-            }
-        }
-        auto accumulate = [&](int k) {
-            const int cb = abegin + s_beg[k];
-            const int L = s_len[k];
-            const float fk = s_w[k];
-            const uint16_t* row = s_elem + k * mlen;
-#pragma unroll
-            for (int j = 0; j < JB; ++j) {
-                const int c0 = 32 * (warp + NWARP * j);
-                if (c0 < cb + L && c0 + 32 > cb) {           // warp-uniform
-                    const int p = c0 + lane - cb;
-                    if (p >= 0 && p < L) {
-                        const uint32_t e = row[p];
-                        const uint32_t b = e & 3u;
-                        const float w = useQ ? fmul_rn(fk, s_qw[e >> 2]) : fk;
-                        cntp[j] += 1ull << (16 * b);
-                        if (b == 0) wA[j] = __fadd_rn(wA[j], w);
-                        if (b == 1) wC[j] = __fadd_rn(wC[j], w);
-                        if (b == 2) wG[j] = __fadd_rn(wG[j], w);
-                        if (b == 3) wT[j] = __fadd_rn(wT[j], w);
-                    }
+            const int c0 = 32 * (warp + NWARP * j);
+            const int col = c0 + lane;
+            const bool active = c0 < ncols;                  // warp-uniform
+            uint32_t cAC = 0u, cGT = 0u;                     // 16-bit counts: A | C << 16, G | T << 16
+            float wA = 0.0f, wC = 0.0f, wG = 0.0f, wT = 0.0f;
+            // branch-free add of one element; a lane outside the row adds
+            // weight +0.0f (an exact identity on the non-negative sums) and
+            // no count
+            auto add = [&](uint32_t b, float w, bool valid) {
+                const uint32_t inc = valid ? (1u << (16 * (b & 1u))) : 0u;
+                cAC += (b & 2u) ? 0u : inc;
+                cGT += (b & 2u) ? inc : 0u;
+                wA = __fadd_rn(wA, b == 0 ? w : 0.0f);
+                wC = __fadd_rn(wC, b == 1 ? w : 0.0f);
+                wG = __fadd_rn(wG, b == 2 ? w : 0.0f);
+                wT = __fadd_rn(wT, b == 3 ? w : 0.0f);
+            };
+            {
+                const int p = col - abegin;
+                if (active && p >= 0 && p < La) {
+                    const uint32_t e = s_aelem[p];
+                    add(e & 3u, useQ ? s_qw[e >> 2] : 1.0f, true);     // factor 1.0f
                 }
             }
-        };
-        if (persistent) {
-            for (int i = 0; i < nalive; ++i) accumulate(s_alive[i]);
-        } else {
-            for (int c = 0; c < nalive; c += kStage) {
-                const int n = min(kStage, nalive - c);
-                stage(c, n);
-                for (int k = 0; k < n; ++k) accumulate(k);
-            }
-        }
-        // ---- consensus and support (findConsensus, msa.cpp:135-157) ----
+            // staged rows (slot list[i], or slot i) meeting this block, in
+            // list order; up to four rows load together, then add in order
+            auto run_rows = [&](const uint8_t* list, int nrows) {
+                for (int i0 = 0; i0 < nrows; i0 += 32) {
+                    bool hit = false;
+                    if (i0 + lane < nrows) {
+                        const int k = list ? list[i0 + lane] : i0 + lane;
+                        const int cb = abegin + s_beg[k];
+                        hit = cb < c0 + 32 && cb + s_len[k] > c0;
+                    }
+                    unsigned m = __ballot_sync(0xffffffffu, hit);
+                    while (m) {
+                        bool v[4];
+                        uint32_t bb[4];
+                        float ww[4];
+                        int nu = 0;
 #pragma unroll
-        for (int j = 0; j < JB; ++j) {
-            const int col = 32 * (warp + NWARP * j) + lane;
-            if (col < ncols) {
-                uint8_t cs = 0; float cw = wA[j];
-                if (wC[j] > cw) { cs = 1; cw = wC[j]; }
-                if (wG[j] > cw) { cs = 2; cw = wG[j]; }
-                if (wT[j] > cw) { cs = 3; cw = wT[j]; }
-                const float colw = __fadd_rn(__fadd_rn(__fadd_rn(wA[j], wC[j]), wG[j]), wT[j]);
+                        for (int u = 0; u < 4; ++u) {
+                            v[u] = false;
+                            bb[u] = 0u;
+                            ww[u] = 0.0f;
+                            if (m) {                             // warp-uniform
+                                const int i = i0 + __ffs(m) - 1;
+                                m &= m - 1;
+                                ++nu;
+                                const int k = list ? list[i] : i;
+                                const int p = col - (abegin + s_beg[k]);
+                                const bool in = (unsigned)p < (unsigned)s_len[k];
+                                const int pc = in ? p : 0;          // loads stay inside the row
+                                const float w = useQ ? fmul_rn(s_w[k], cand_qweight(k, pc)) : s_w[k];
+                                v[u] = in;
+                                bb[u] = cand_base(k, pc);
+                                ww[u] = in ? w : 0.0f;
+                            }
+                        }
+#pragma unroll
+                        for (int u = 0; u < 4; ++u)
+                            if (u < nu) add(bb[u], ww[u], v[u]);
+                    }
+                }
+            };
+            if (persistent) {
+                if (active) run_rows(s_alive, nalive);
+            } else {
+                // more rows than fit: each chunk is staged (by all warps) per block
+                for (int c = 0; c < nalive; c += nstage) {
+                    const int n = min(nstage, nalive - c);
+                    stage(c, n);
+                    if (active) run_rows(nullptr, n);
+                }
+            }
+            if (active && col < ncols) {
+                uint8_t cs = 0; float cw = wA;
+                if (wC > cw) { cs = 1; cw = wC; }
+                if (wG > cw) { cs = 2; cw = wG; }
+                if (wT > cw) { cs = 3; cw = wT; }
+                const float colw = __fadd_rn(__fadd_rn(__fadd_rn(wA, wC), wG), wT);
                 s_cons[col] = cs;
                 s_support[col] = fdiv_rn(cw, colw);
-                const uint32_t nA = (uint32_t)(cntp[j] & 0xFFFFu), nC = (uint32_t)((cntp[j] >> 16) & 0xFFFFu);
-                const uint32_t nG = (uint32_t)((cntp[j] >> 32) & 0xFFFFu), nT = (uint32_t)(cntp[j] >> 48);
+                const uint32_t nA = cAC & 0xFFFFu, nC = cAC >> 16;
+                const uint32_t nG = cGT & 0xFFFFu, nT = cGT >> 16;
                 s_cov[col] = (uint16_t)(nA + nC + nG + nT);
                 s_cnt[col][0] = (uint16_t)nA; s_cnt[col][1] = (uint16_t)nC;
                 s_cnt[col][2] = (uint16_t)nG; s_cnt[col][3] = (uint16_t)nT;
@@ -626,7 +681,7 @@ msa_anchor(const DevOptions& o, const DevReads& r, uint32_t first, uint32_t ai,
                         const uint32_t ob = s_aelem[p] & 3u;
                         s_fw[p] = colw;
                         s_fw[mlen + p] = cw;
-                        s_fw[2 * mlen + p] = ob == 0 ? wA[j] : ob == 1 ? wC[j] : ob == 2 ? wG[j] : wT[j];
+                        s_fw[2 * mlen + p] = ob == 0 ? wA : ob == 1 ? wC : ob == 2 ? wG : wT;
                     }
                 }
             }
@@ -665,7 +720,7 @@ msa_anchor(const DevOptions& o, const DevReads& r, uint32_t first, uint32_t ai,
             for (int i = tid; i < nalive; i += BLOCK) {
                 const int k = s_alive[i];
                 const int rb = abegin + s_beg[k], re = rb + s_len[k];
-                const int rem = (col >= rb && col < re) ? removes(s_elem[k * mlen + col - rb] & 3) : 0;
+                const int rem = (col >= rb && col < re) ? removes((int)cand_base(k, col - rb)) : 0;
                 nrem += rem;
                 veto |= rem && s_w[k] >= 0.90f;
             }
@@ -696,7 +751,7 @@ msa_anchor(const DevOptions& o, const DevReads& r, uint32_t first, uint32_t ai,
                 if (persistent) {
                     k = s_alive[i];
                     const int rb = abegin + s_beg[k], re = rb + s_len[k];
-                    keep = !((col >= rb && col < re) && removes(s_elem[k * mlen + col - rb] & 3));
+                    keep = !((col >= rb && col < re) && removes((int)cand_base(k, col - rb)));
                 } else {
                     rc = recs[off + i];
                     const int rb = abegin + rc.shift, re = rb + rc.len;
@@ -920,7 +975,7 @@ msa_anchor(const DevOptions& o, const DevReads& r, uint32_t first, uint32_t ai,
 // One CTA per anchor, in `order` (e.g. most candidates first) when given;
 // the hardware block scheduler hands out the anchors.
 template <int BLOCK, int JB, bool EMIT = false>
-__global__ void __launch_bounds__(BLOCK)
+__global__ void __launch_bounds__(BLOCK, 768 / BLOCK)
 k_msa(DevOptions o, DevReads r, uint32_t first, uint32_t count, const uint32_t* __restrict__ order,
       const uint32_t* __restrict__ cand_ids, const uint32_t* __restrict__ seg_off,
       const uint32_t* __restrict__ seg_cnt, const AlignRes* __restrict__ ares,
@@ -934,7 +989,7 @@ k_msa(DevOptions o, DevReads r, uint32_t first, uint32_t count, const uint32_t* 
 // Persistent form: a grid of resident CTAs pulls anchors from a device work
 // queue (an atomic cursor over `order`) until the batch is done.
 template <int BLOCK, int JB, bool EMIT = false>
-__global__ void __launch_bounds__(BLOCK)
+__global__ void __launch_bounds__(BLOCK, 768 / BLOCK)
 k_msa_queue(DevOptions o, DevReads r, uint32_t first, uint32_t count, const uint32_t* __restrict__ order,
             unsigned int* __restrict__ cursor, const uint32_t* __restrict__ cand_ids,
             const uint32_t* __restrict__ seg_off, const uint32_t* __restrict__ seg_cnt,
