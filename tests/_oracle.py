@@ -171,7 +171,7 @@ def opts_from_args(args: str) -> CoOpts:
 class OracleRun:
     """Reads + tables + per-anchor results of the oracle for one input."""
 
-    def __init__(self, files, opts: CoOpts, threads: int = 4):
+    def __init__(self, files, opts: CoOpts, threads: int = 4, first: int = 0, count: int | None = None):
         L = lib()
         self.opts = opts
         arr = (ctypes.c_char_p * len(files))(*[f.encode() for f in files])
@@ -180,7 +180,9 @@ class OracleRun:
             raise RuntimeError("oracle could not read input")
         self.tables = L.co_build_tables(self.reads, ctypes.byref(opts))
         r = self.reads.contents
-        self.res = L.co_correct(self.reads, self.tables, ctypes.byref(opts), 0, r.n, threads)
+        self.first = first
+        self.res = L.co_correct(self.reads, self.tables, ctypes.byref(opts), first,
+                                r.n - first if count is None else count, threads)
 
     def close(self):
         L = lib()
@@ -236,6 +238,26 @@ class OracleRun:
                        ("logit", "<f4"), ("x", "<f4", (NFEAT,))])
         a = raw.view(dt)
         return {k: a[k].copy() for k in dt.names}
+
+    def original(self, rid: int) -> bytes:
+        """Uncorrected (2-bit decoded) sequence of a read."""
+        r = self.reads.contents
+        L = int(r.len[rid])
+        buf = ctypes.create_string_buffer(max(L, 1) + 1)
+        words = ctypes.cast(ctypes.addressof(r.seq.contents) + rid * r.seq_pitch * 4, ctypes.POINTER(ctypes.c_uint32))
+        lib().co_decode_2bit(words, L, buf)
+        return buf.raw[:L]
+
+    def records(self) -> bytes:
+        """The results as the library's record stream (care_b200.shard.encode_records)."""
+        from care_b200.shard import encode_records
+        status, hq, ue, ne, seq = self.anchors()
+        st = (status & 1) | (hq << 1) | (ue << 2)
+        cands, cseq = self.candidates()
+        n = status.shape[0]
+        return encode_records(range(self.first, self.first + n), st, ne, seq,
+                              [c[0] for c in cands], [c[2] for c in cands], [c[3] for c in cands], cseq,
+                              self.lengths(), self.original)
 
     def lengths(self):
         r = self.reads.contents
