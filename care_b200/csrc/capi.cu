@@ -87,6 +87,10 @@ struct care_b200_ctx {
     std::vector<std::vector<uint32_t>> t_off, t_val;
     bool tables_ready = false;
     uint32_t tables_reads = 0;        // storage size the tables were built for
+    // minhash signatures of all reads (n * num_maps keys), resident so the
+    // candidate stage only looks them up
+    DBuf d_sigs;
+    int sigs_maps = 0;                // 0: not computed for the current storage
 
     // batch scratch
     DBuf d_seg_off, d_seg_cnt, d_cand_ids, d_cand_anchor, d_ares, d_recs, d_counters, d_status;
@@ -193,6 +197,24 @@ uint64_t host_murmur64(uint64_t x) {
     return x;
 }
 
+// minhash signatures of every read for `maps` hash functions into d_sigs
+int compute_signatures(care_b200_ctx* ctx, int maps) {
+    DevOptions o = make_dev_options(ctx);
+    o.num_maps = maps;
+    const DevReads r = make_dev_reads(ctx);
+    CK(ctx->d_sigs.ensure((size_t)ctx->n * maps * 8), "alloc signatures");
+    const uint32_t chunk = 1u << 20;
+    for (uint32_t b = 0; b < ctx->n; b += chunk) {
+        const uint32_t cnt = std::min(chunk, ctx->n - b);
+        const int wpb = 8;
+        k_signatures<<<(cnt + wpb - 1) / wpb, 32 * wpb, 0, ctx->stream>>>(
+            o, r, b, cnt, ctx->d_sigs.as<unsigned long long>() + (size_t)b * maps);
+        CK(cudaGetLastError(), "k_signatures");
+    }
+    ctx->sigs_maps = maps;
+    return CARE_B200_OK;
+}
+
 int validate_options(care_b200_ctx* ctx, const care_b200_options& o) {
     // ProgramOptions::isValid, src/options.cpp:387-480, plus this library's limits
     if (o.max_error_rate < 0.f || o.max_error_rate > 1.f) return fail(ctx, CARE_B200_EINVAL, "maxmismatchratio must be in [0,1]");
@@ -294,6 +316,7 @@ int care_b200_upload_reads(care_b200_ctx* ctx, const uint32_t* packed, size_t pi
         CK(ctx->d_qual.ensure((size_t)num_reads * qual_pitch_ints * 4), "alloc qualities");
         CK(cudaMemcpyAsync(ctx->d_qual.p, enc_quals, (size_t)num_reads * qual_pitch_ints * 4, cudaMemcpyHostToDevice, ctx->stream), "upload qualities");
     }
+    ctx->sigs_maps = 0;
     ctx->h_len.assign(lengths, lengths + num_reads);
     ctx->h_ambig.assign(num_reads, 0);
     for (size_t i = 0; i < num_ambiguous; i++) {
@@ -373,18 +396,11 @@ int care_b200_build_tables(care_b200_ctx* ctx) {
     ctx->num_maps = h;
     DevOptions o = make_dev_options(ctx);
     DevReads r = make_dev_reads(ctx);
-    // signatures of all reads on the device (insert, ordinaryminhasher.hpp:376-426)
+    // signatures of all reads on the device (insert, ordinaryminhasher.hpp:376-426),
+    // kept resident for the candidate stage
     std::vector<uint64_t> sig((size_t)ctx->n * h);
-    DBuf d_sig;
-    const uint32_t chunk = 1u << 20;
-    CK(d_sig.ensure((size_t)std::min(ctx->n, chunk) * h * 8), "alloc signatures");
-    for (uint32_t b = 0; b < ctx->n; b += chunk) {
-        const uint32_t cnt = std::min(chunk, ctx->n - b);
-        const int wpb = 8;
-        k_signatures<<<(cnt + wpb - 1) / wpb, 32 * wpb, 0, ctx->stream>>>(o, r, b, cnt, d_sig.as<unsigned long long>());
-        CK(cudaGetLastError(), "k_signatures");
-        CK(cudaMemcpyAsync(sig.data() + (size_t)b * h, d_sig.p, (size_t)cnt * h * 8, cudaMemcpyDeviceToHost, ctx->stream), "signatures");
-    }
+    if (int rc = compute_signatures(ctx, h)) return rc;
+    CK(cudaMemcpyAsync(sig.data(), ctx->d_sigs.p, (size_t)ctx->n * h * 8, cudaMemcpyDeviceToHost, ctx->stream), "signatures");
     CK(cudaStreamSynchronize(ctx->stream), "signatures");
     // group per map: values of one key ascending, buckets with fewer than 2
     // or more than threshold values cleared (groupbykey.hpp:99-249)
@@ -630,7 +646,8 @@ int run_batch(care_b200_ctx* ctx, uint32_t first, uint32_t count, bool timed) {
             }
             EQ(mark(0), "event");
             k_candidates<kCandBlock><<<count, kCandBlock, cand_smem, st>>>(
-                o, r, ctx->d_tdesc.as<TableDesc>(), ctx->d_slots.as<Slot>(), ctx->d_values.as<uint32_t>(), first,
+                o, r, ctx->d_tdesc.as<TableDesc>(), ctx->d_slots.as<Slot>(), ctx->d_values.as<uint32_t>(),
+                ctx->d_sigs.as<unsigned long long>(), first,
                 count, set_log2, ctx->d_cand_ids.as<uint32_t>(), ctx->d_cand_anchor.as<uint32_t>(),
                 ctx->d_seg_off.as<uint32_t>(), ctx->d_seg_cnt.as<uint32_t>(), counters, cap, status);
             EQ(cudaGetLastError(), "k_candidates");
@@ -750,6 +767,8 @@ int correct_impl(care_b200_ctx* ctx, uint32_t first, uint32_t count, care_b200_r
     if (ctx->opt.paired_end && ((first | count) & 1)) return fail(ctx, CARE_B200_EINVAL, "paired-end ranges must be pair aligned");
     if (ctx->opt.correction_type == 1 && !ctx->mlp_set) return fail(ctx, CARE_B200_ESTATE, "correction_type 1 needs care_b200_set_mlp");
     CK(cudaSetDevice(ctx->opt.device), "cudaSetDevice");
+    if (ctx->sigs_maps != ctx->num_maps)
+        if (int rc = compute_signatures(ctx, ctx->num_maps)) return rc;
     ctx->r_fx.clear(); ctx->r_fread.clear(); ctx->r_fmeta.clear(); ctx->r_flogit.clear();
     uint32_t B = ctx->opt.batch_size > 0 ? (uint32_t)ctx->opt.batch_size : (1u << 21);
     if (ctx->opt.paired_end) B &= ~1u;

@@ -47,7 +47,8 @@ struct CandSmem {
 template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK)
 k_candidates(DevOptions o, DevReads r, const TableDesc* __restrict__ td, const Slot* __restrict__ slots,
-             const uint32_t* __restrict__ values, uint32_t first, uint32_t count, int set_log2,
+             const uint32_t* __restrict__ values, const unsigned long long* __restrict__ sig,
+             uint32_t first, uint32_t count, int set_log2,
              uint32_t* __restrict__ cand_ids, uint32_t* __restrict__ cand_anchor,
              uint32_t* __restrict__ seg_off, uint32_t* __restrict__ seg_cnt,
              unsigned long long* __restrict__ arena_count, unsigned long long arena_cap,
@@ -77,40 +78,48 @@ k_candidates(DevOptions o, DevReads r, const TableDesc* __restrict__ td, const S
         if (tid == 0) { seg_off[ai] = 0; seg_cnt[ai] = 0; }
         return;
     }
-    // anchor row into shared memory, two zero words of padding for kmer_at
-    const uint32_t* arow = r.seq + (size_t)a * r.seq_pitch;
-    for (int i = tid; i < r.seq_pitch + 2; i += BLOCK) sseq[i] = i < r.seq_pitch ? __ldg(arow + i) : 0u;
-    __syncthreads();
+    // the anchor's signature: resident (computed once per read storage by
+    // k_signatures), or hashed here
+    if (!sig) {
+        // anchor row into shared memory, two zero words of padding for kmer_at
+        const uint32_t* arow = r.seq + (size_t)a * r.seq_pitch;
+        for (int i = tid; i < r.seq_pitch + 2; i += BLOCK) sseq[i] = i < r.seq_pitch ? __ldg(arow + i) : 0u;
+        __syncthreads();
 
-    // canonical k-mers
-    const int npos = L - o.k + 1;
-    const int rcshift = 64 - 2 * o.k;
-    for (int p = tid; p < npos; p += BLOCK) {
-        const unsigned long long fw = kmer_at(sseq, o.k, p);
-        const unsigned long long rv = revcomp64(fw) >> rcshift;
-        canon[p] = fw < rv ? fw : rv;
-    }
-    __syncthreads();
-
-    // per map: min over k-mers of murmur64(kmer + map)
-    {
-        const int m = tid % h, g = tid / h;
-        if (g < groups) {
-            unsigned long long mn = ~0ull;
-            for (int p = g; p < npos; p += groups) {
-                const unsigned long long v = murmur64(canon[p] + (unsigned long long)m);
-                mn = v < mn ? v : mn;
-            }
-            partial[g * h + m] = mn;
+        // canonical k-mers
+        const int npos = L - o.k + 1;
+        const int rcshift = 64 - 2 * o.k;
+        for (int p = tid; p < npos; p += BLOCK) {
+            const unsigned long long fw = kmer_at(sseq, o.k, p);
+            const unsigned long long rv = revcomp64(fw) >> rcshift;
+            canon[p] = fw < rv ? fw : rv;
         }
+        __syncthreads();
+
+        // per map: min over k-mers of murmur64(kmer + map)
+        {
+            const int m = tid % h, g = tid / h;
+            if (g < groups) {
+                unsigned long long mn = ~0ull;
+                for (int p = g; p < npos; p += groups) {
+                    const unsigned long long v = murmur64(canon[p] + (unsigned long long)m);
+                    mn = v < mn ? v : mn;
+                }
+                partial[g * h + m] = mn;
+            }
+        }
+        __syncthreads();
     }
-    __syncthreads();
 
     // table lookup (linear probing from murmur64(key))
     if (tid < h) {
         unsigned long long key = ~0ull;
-        for (int g = 0; g < groups; ++g) { const unsigned long long v = partial[g * h + tid]; key = v < key ? v : key; }
-        key &= o.kmer_mask;
+        if (sig) {
+            key = __ldg(sig + (size_t)a * h + tid);
+        } else {
+            for (int g = 0; g < groups; ++g) { const unsigned long long v = partial[g * h + tid]; key = v < key ? v : key; }
+            key &= o.kmer_mask;
+        }
         const TableDesc d = td[tid];
         uint32_t pos = (uint32_t)murmur64(key) & d.mask;
         uint32_t off = 0, cnt = 0;
@@ -124,7 +133,6 @@ k_candidates(DevOptions o, DevReads r, const TableDesc* __restrict__ td, const S
         qoff[tid] = (uint32_t)d.value_base + off;
         qcnt[tid] = cnt;
     }
-    for (int i = tid; i < setcap; i += BLOCK) set[i] = kEmpty;
     if (tid == 0) s_unique = 0;
     __syncthreads();
     if (tid == 0) {
@@ -134,23 +142,31 @@ k_candidates(DevOptions o, DevReads r, const TableDesc* __restrict__ td, const S
     }
     __syncthreads();
 
-    // insert all retrieved ids into the shared hash set
+    // the hash set is sized for the ids actually retrieved: a power of two
+    // >= 2 * T (at least 64), within the allocated capacity
     const uint32_t T = qpre[h];
+    int sl2 = 6;
+    while (sl2 < set_log2 && (1u << sl2) < 2 * T) ++sl2;
+    const int scap = 1 << sl2;
+    for (int i = tid; i < scap; i += BLOCK) set[i] = kEmpty;
+    __syncthreads();
+
+    // insert all retrieved ids into the shared hash set
     for (uint32_t e = tid; e < T; e += BLOCK) {
         int lo = 0, hi = h - 1;                     // map of element e
         while (lo < hi) { const int mid = (lo + hi + 1) >> 1; if (qpre[mid] <= e) lo = mid; else hi = mid - 1; }
         const uint32_t id = __ldg(values + qoff[lo] + (e - qpre[lo]));
-        uint32_t pos = (id * 2654435761u) >> (32 - set_log2);
-        for (int probe = 0; probe < setcap; ++probe) {
+        uint32_t pos = (id * 2654435761u) >> (32 - sl2);
+        for (int probe = 0; probe < scap; ++probe) {
             const uint32_t prev = atomicCAS(&set[pos], kEmpty, id);
             if (prev == kEmpty || prev == id) break;
-            pos = (pos + 1) & (setcap - 1);
+            pos = (pos + 1) & (scap - 1);
         }
     }
     __syncthreads();
 
     // unique ids minus the anchor itself and (optionally) ambiguous reads
-    for (int i = tid; i < setcap; i += BLOCK) {
+    for (int i = tid; i < scap; i += BLOCK) {
         const uint32_t v = set[i];
         if (v != kEmpty && v != a && !(o.exclude_ambiguous && r.ambig[v])) list[atomicAdd(&s_unique, 1u)] = v;
     }
