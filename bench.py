@@ -223,6 +223,15 @@ def int_peaks():
     return json.loads(r.stdout) if r.returncode == 0 else None
 
 
+def launches_per_pass(tuning: dict, learned: bool, batches: int = 1) -> int:
+    """Kernels of this library launched by one correction pass: candidates,
+    alignment, MSA; the anchor-order kernels and the pair-order kernel when
+    the mapping uses them; inference, verdicts and edit recount with the
+    learned decision."""
+    k = 3 + (3 if tuning.get("msa_order") else 0) + (1 if tuning.get("pair_order") else 0)
+    return batches * (k + (3 if learned else 0))
+
+
 def base_counts(rs, path):
     """TP/FP/FN/TN of a corrected FASTQ against the true reads."""
     from care_b200 import datagen
@@ -353,6 +362,7 @@ def main():
             tp, fp, fn, tn = base_counts(rs, out)
             counts[name] = {"tp": tp, "fp": fp, "fn": fn, "f1": datagen.f1(tp, fp, fn)}
             os.unlink(out)
+        mcorr_tuning = mcorr.tuning
         mcorr.close()
         mvalue = world * n / (mms / 1e3)
         learned = {"value": mvalue, "unit": "reads/s", "ms_per_step": mms, "ratio_vs_plain": mvalue / value,
@@ -360,7 +370,7 @@ def main():
                                 "classifier": mstage[3]},
                    "network": "24-64-64-1 GELU, bf16 tcgen05 GEMMs, fp32 accumulate",
                    "params": os.path.relpath(MLP_FILE, ROOT),
-                   "base_level": counts, "gpu_launches": 6 * args.steps}
+                   "base_level": counts, "gpu_launches": launches_per_pass(mcorr_tuning, True) * args.steps}
 
     progress("timed steps done")
     # e2e through the C ABI from host buffers
@@ -434,7 +444,7 @@ def main():
                                "peak_source": "care-b200-peaks (measured, registers only)" if ip else None},
         "e2e": {"value": world * n / e2e_t, "unit": "reads/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
-        "gpu_launches": 3 * args.steps,
+        "gpu_launches": launches_per_pass(corr.tuning, False) * args.steps,
         "clocks": clk.summary(),
     }
     if learned is not None:
