@@ -370,7 +370,7 @@ def main():
                                 "classifier": mstage[3]},
                    "network": "24-64-64-1 GELU, bf16 tcgen05 GEMMs, fp32 accumulate",
                    "params": os.path.relpath(MLP_FILE, ROOT),
-                   "base_level": counts, "gpu_launches": launches_per_pass(mcorr_tuning, True) * args.steps}
+                   "base_level": counts, "gpu_launches": launches_per_pass(mcorr_tuning, True, -(-n // (1 << 21))) * args.steps}
 
     progress("timed steps done")
     # e2e through the C ABI from host buffers
@@ -444,7 +444,7 @@ def main():
                                "peak_source": "care-b200-peaks (measured, registers only)" if ip else None},
         "e2e": {"value": world * n / e2e_t, "unit": "reads/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
-        "gpu_launches": launches_per_pass(corr.tuning, False) * args.steps,
+        "gpu_launches": launches_per_pass(corr.tuning, False, -(-n // (1 << 21))) * args.steps,
         "clocks": clk.summary(),
     }
     if learned is not None:
