@@ -23,6 +23,11 @@ src/dispatch_care_correct_cpu.cpp:157-168; reads/s = reads / STEP2 time).
           `python -m care_b200.learned` on three other seeded genomes), and
           base-level TP/FP/FN/F1 of both forms against the true reads.
 
+--workload large : 50 Mbp genome with 5% repeats, 150 bp PE at 50x (~16.7M
+          reads), position-dependent substitutions plus 0.01% single-base
+          indels and 0.1% N bases; -c 50 -k 20 -h 48 -q --qualityScoreBits 2
+          --pairmode PE --excludeAmbiguous; plain and learned forms with
+          base-level counts (network care_b200/data/mlp_pe50x_h48.bin).
 --workload uneven : the batched uneven set instead -- 10 Mbp genome with 8%
           repeats in families of 5-500 copies (0.5-2% divergence), single-end
           reads of 50-250 bp at 40x (~2.7M reads), same error and quality
@@ -50,6 +55,8 @@ sys.path.insert(0, ROOT)
 
 ARGS = "-c 30 -k 20 -h 32 -q --qualityScoreBits 2 --pairmode PE"
 ARGS_UNEVEN = "-c 40 -k 20 -h 32 -q --qualityScoreBits 2 --pairmode SE"
+ARGS_LARGE = "-c 50 -k 20 -h 48 -q --qualityScoreBits 2 --pairmode PE --excludeAmbiguous"
+MLP_FILE_LARGE = os.path.join(ROOT, "care_b200", "data", "mlp_pe50x_h48.bin")
 METRIC = "reads corrected/s on 1 B200: plain vs MLP-classifier form at matched base F1"
 MLP_FILE = os.path.join(ROOT, "care_b200", "data", "mlp_pe30x.bin")
 # k_msa DRAM bytes per anchor: dram__bytes_read.sum + dram__bytes_write.sum of
@@ -61,6 +68,8 @@ L2_BYTES = 126 * 1024 * 1024
 
 def workload(rank: int, genome_size: int, kind: str = "pe"):
     from care_b200 import datagen
+    if kind == "large":
+        return datagen.paired_end_large(seed=5 + 1000 * rank, genome_size=genome_size)
     if kind == "uneven":
         return datagen.single_end_uneven(seed=3 + 1000 * rank, genome_size=genome_size, coverage=40.0)
     # 2% of the genome in 20 copies of one repeat unit (5 kbp at 5 Mbp)
@@ -71,6 +80,8 @@ def workload(rank: int, genome_size: int, kind: str = "pe"):
 
 def write_fastq_fast(rs, path):
     n, W = rs.num_reads, rs.seqs.shape[1]
+    if (rs.lengths == W).all() and n > 2_000_000:
+        return write_fastq_fixed(rs, path)
     lens = rs.lengths
     seqs = rs.seqs.tobytes()
     quals = rs.quals.tobytes()
@@ -82,6 +93,31 @@ def write_fastq_fast(rs, path):
                 o, L = i * W, int(lens[i])
                 parts += [b"@r%d\n" % i, seqs[o:o + L], b"\n+\n", quals[o:o + L], b"\n"]
             f.write(b"".join(parts))
+
+
+def write_fastq_fixed(rs, path, chunk: int = 1_000_000):
+    """Fixed-length reads as 4-line FASTQ records built in bulk: header
+    "@r<id, 10 digits>", sequence, "+", qualities."""
+    n, L = rs.seqs.shape
+    rec = 17 + 2 * L
+    with open(path, "wb") as f:
+        for b in range(0, n, chunk):
+            e = min(n, b + chunk)
+            m = e - b
+            buf = np.empty((m, rec), np.uint8)
+            ids = np.arange(b, e, dtype=np.int64)
+            buf[:, 0] = ord("@")
+            buf[:, 1] = ord("r")
+            for d in range(10):
+                buf[:, 11 - d] = ord("0") + (ids // 10 ** d) % 10
+            buf[:, 12] = ord("\n")
+            buf[:, 13:13 + L] = rs.seqs[b:e]
+            buf[:, 13 + L] = ord("\n")
+            buf[:, 14 + L] = ord("+")
+            buf[:, 15 + L] = ord("\n")
+            buf[:, 16 + L:16 + 2 * L] = rs.quals[b:e]
+            buf[:, 16 + 2 * L] = ord("\n")
+            f.write(buf.tobytes())
 
 
 def encode_quality_2bit(quals: np.ndarray) -> np.ndarray:
@@ -263,17 +299,18 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="care_b200", choices=["care_b200", "reference"])
-    ap.add_argument("--workload", default="pe", choices=["pe", "uneven"])
-    ap.add_argument("--genome", type=int, default=None, help="bp (default 5 Mbp, uneven 10 Mbp)")
+    ap.add_argument("--workload", default="pe", choices=["pe", "uneven", "large"])
+    ap.add_argument("--genome", type=int, default=None, help="bp (default 5 Mbp, uneven 10 Mbp, large 50 Mbp)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned", action="store_true")
     ap.add_argument("--tuning", default="auto", choices=["auto", "default"],
                     help="auto: the committed launch mapping of the workload (care_b200/tuning/)")
     args = ap.parse_args()
     if args.genome is None:
-        args.genome = 10_000_000 if args.workload == "uneven" else 5_000_000
+        args.genome = {"uneven": 10_000_000, "large": 50_000_000}.get(args.workload, 5_000_000)
     uneven = args.workload == "uneven"
-    run_args = ARGS_UNEVEN if uneven else ARGS
+    large = args.workload == "large"
+    run_args = ARGS_UNEVEN if uneven else (ARGS_LARGE if large else ARGS)
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -334,11 +371,12 @@ def main():
     # the learned decision on the same reads: device time of the same steps,
     # then base-level counts of both forms against the true reads
     learned = None
-    if not args.no_learned and not uneven and os.path.exists(MLP_FILE):
+    mlp_file = MLP_FILE_LARGE if large else MLP_FILE
+    if not args.no_learned and not uneven and os.path.exists(mlp_file):
         from care_b200 import learned as lrn, datagen
-        params = lrn.load_params(MLP_FILE)
+        params = lrn.load_params(mlp_file)
         progress("learned form: load + tables")
-        mcorr = care_b200.Corrector(care_b200.options_from_args(ARGS, device=local, correction_type=1))
+        mcorr = care_b200.Corrector(care_b200.options_from_args(run_args, device=local, correction_type=1))
         mcorr.set_mlp(params)
         if tuned:
             mcorr.tuning = tuned
@@ -369,7 +407,7 @@ def main():
                    "stage_ms": {"candidates": mstage[0], "align": mstage[1], "msa": mstage[2],
                                 "classifier": mstage[3]},
                    "network": "24-64-64-1 GELU, bf16 tcgen05 GEMMs, fp32 accumulate",
-                   "params": os.path.relpath(MLP_FILE, ROOT),
+                   "params": os.path.relpath(mlp_file, ROOT),
                    "base_level": counts, "gpu_launches": launches_per_pass(mcorr_tuning, True, -(-n // (1 << 21))) * args.steps}
 
     progress("timed steps done")
@@ -421,6 +459,7 @@ def main():
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded), " + rs.name,
         "config": {"workload": ("se_uneven_%dMbp_40x_50-250bp" % (args.genome // 1_000_000)) if uneven
+                   else ("pe_large_%dMbp_50x_150bp_indels_N" % (args.genome // 1_000_000)) if large
                    else "pe_5Mbp_30x_150bp", "reads_per_gpu": n, "args": run_args,
                    "genome_bp": args.genome, "l2": "flushed between steps (252 MB write); working set > L2",
                    "parallelism": f"replicas x{world} (independent read sets)",
@@ -431,7 +470,7 @@ def main():
         "roofline": {"kernel": "k_msa", "bound": "hbm", "achieved": msa_gbs, "peak": hbm_peak,
                      "bytes_per_pair": per_pair,
                      "unit": "GB/s", "frac": msa_gbs / hbm_peak,
-                     "traffic": None if uneven else MSA_DRAM_BYTES_PER_ANCHOR * n,
+                     "traffic": None if (uneven or large) else MSA_DRAM_BYTES_PER_ANCHOR * n,
                      "traffic_source": "ncu capture of 100,000 anchors scaled by anchors per launch",
                      "peak_source": "measured" if peaks else "fallback"},
         "roofline_alignment": {"kernel": "k_align", "bound": "int", "unit": "word compares/s",
@@ -449,7 +488,7 @@ def main():
     }
     if learned is not None:
         line["learned"] = learned
-    if rank == 0 and world == 1 and not args.no_cpu_baseline and not uneven and os.path.exists(CARE_CPU):
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and args.workload == "pe" and os.path.exists(CARE_CPU):
         threads = host_cores()
         progress(f"e2e done; care-cpu sample on {threads} threads")
         v = care_cpu_sample(tmp, threads)

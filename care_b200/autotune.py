@@ -50,12 +50,15 @@ WORKLOADS = {
 }
 
 
+TUNING_FILES = {"pe": "pe_5Mbp_30x.json", "uneven": "se_uneven_40x.json", "large": "pe_large_50x.json"}
+
+
 def tuning_file(workload: str) -> str:
-    return os.path.join(TUNING_DIR, {"pe": "pe_5Mbp_30x.json", "uneven": "se_uneven_40x.json"}[workload])
+    return os.path.join(TUNING_DIR, TUNING_FILES.get(workload, workload + ".json"))
 
 
 def load(workload: str) -> dict | None:
-    """The committed tuning of a workload, or None."""
+    """The committed tuning of a workload, or None (the default mapping)."""
     p = tuning_file(workload)
     if not os.path.exists(p):
         return None

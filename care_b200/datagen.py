@@ -106,15 +106,18 @@ def _pos_dependent_errors(rng, truth_codes, lengths, lo=0.002, hi=0.015,
     """Substitution rate rising linearly along the read; Q from the rate."""
     n, Lmax = truth_codes.shape
     pos = np.arange(Lmax)[None, :].astype(np.float64)
-    denom = np.maximum(lengths[:, None] - 1, 1).astype(np.float64)
-    p = lo + (hi - lo) * np.minimum(pos / denom, 1.0)
-    p = np.broadcast_to(p, (n, Lmax))
+    # rate and -10 log10(rate) per distinct read length, then per read
+    ulen, inv = np.unique(lengths, return_inverse=True)
+    denom = np.maximum(ulen[:, None] - 1, 1).astype(np.float64)
+    pu = lo + (hi - lo) * np.minimum(pos / denom, 1.0)
+    p = pu[inv.reshape(-1)]
+    qbase = (-10.0 * np.log10(pu))[inv.reshape(-1)]
     err = rng.random((n, Lmax)) < p
     valid = pos < lengths[:, None]
     err &= valid
     codes = truth_codes.copy()
     codes[err] = (codes[err] + rng.integers(1, 4, size=int(err.sum()), dtype=np.uint8)) & 3
-    q = np.rint(-10.0 * np.log10(p) + rng.normal(0.0, qsd, size=(n, Lmax)))
+    q = np.rint(qbase + rng.normal(0.0, qsd, size=(n, Lmax)))
     q = np.clip(q, qmin, qmax).astype(np.uint8)
     return codes, q, valid
 
@@ -173,6 +176,81 @@ def paired_end_repeats(seed: int = 2, genome_size: int = 5_000_000,
     return _finish(codes, truth, q, valid, lengths, True, "pe_repeats")
 
 
+def paired_end_large(seed: int = 5, genome_size: int = 50_000_000, coverage: float = 50.0, L: int = 150,
+                     frag_mean: float = 400.0, frag_sd: float = 40.0, repeat_fraction: float = 0.05,
+                     indel_rate: float = 1e-4, n_rate: float = 1e-3, chunk_pairs: int = 500_000) -> ReadSet:
+    """The large set: repeat families (5 kbp units, 20 copies, 0.5-2%
+    divergence) over `repeat_fraction` of the genome, interleaved 150 bp PE
+    reads, position-dependent substitutions and qualities as in
+    paired_end_repeats, plus single-base insertions and deletions
+    (`indel_rate` per base) and N bases (`n_rate` per base, quality kept).
+    Generated in chunks of pairs, each from its own seeded stream, so memory
+    stays bounded. truth holds the error-free read (the genome without the
+    indel), so an indel counts as residual errors past its position."""
+    rng = np.random.default_rng(seed)
+    genome = random_genome(rng, genome_size)
+    unit, copies = 5000, 20
+    nfam = int(repeat_fraction * genome_size) // (unit * copies)
+    if nfam > 0:
+        place_repeats(rng, genome, [(unit, copies, float(rng.uniform(0.005, 0.02))) for _ in range(nfam)])
+    num_pairs = int(round(coverage * genome_size / (2 * L)))
+    n = 2 * num_pairs
+    seqs = np.empty((n, L), np.uint8)
+    quals = np.empty((n, L), np.uint8)
+    truth = np.empty((n, L), np.uint8)
+    j = np.arange(L)[None, :]
+
+    def chunk(c: int) -> None:
+        b = c * chunk_pairs
+        m = min(chunk_pairs, num_pairs - b)
+        cr = np.random.default_rng([seed, 1 + c])
+        frag = np.clip(np.rint(cr.normal(frag_mean, frag_sd, size=m)), L + 1, None).astype(np.int64)
+        starts = (cr.random(m) * (genome_size - frag + 1)).astype(np.int64)
+        s1 = _extract(genome, starts, L + 1)                          # read orientation, one spare base
+        s2 = revcomp_codes(_extract(genome, starts + frag - L - 1, L + 1))
+        flip = cr.random(m) < 0.5
+        a = np.where(flip[:, None], s2, s1)
+        bseg = np.where(flip[:, None], s1, s2)
+        seg = np.empty((2 * m, L + 1), np.uint8)
+        seg[0::2] = a
+        seg[1::2] = bseg
+        tr = seg[:, :L].copy()
+        # single-base indels: the read takes the segment with one base
+        # dropped (deletion) or one random base inserted
+        rd = seg[:, :L].copy()
+        hit = np.nonzero(cr.random(2 * m) < 1.0 - (1.0 - indel_rate) ** L)[0]
+        if hit.size:
+            pos = cr.integers(1, L, size=hit.size)[:, None]
+            ins = cr.random(hit.size) < 0.5
+            src = np.where(ins[:, None], j - (j > pos), j + (j >= pos))
+            rows = np.take_along_axis(seg[hit], src, axis=1)
+            extra = cr.integers(0, 4, size=hit.size, dtype=np.uint8)
+            rows[ins, pos[ins, 0]] = extra[ins]
+            rd[hit] = rows
+        # the substitution and quality model of _pos_dependent_errors for
+        # fixed-length reads, drawn in float32
+        pr = (0.002 + 0.013 * np.arange(L, dtype=np.float32) / np.float32(L - 1)).astype(np.float32)
+        err = cr.random((2 * m, L), dtype=np.float32) < pr[None, :]
+        codes = rd
+        codes[err] = (codes[err] + cr.integers(1, 4, size=int(err.sum()), dtype=np.uint8)) & 3
+        qb = (-10.0 * np.log10(pr)).astype(np.float32)
+        q = np.clip(np.rint(qb[None, :] + cr.standard_normal((2 * m, L), dtype=np.float32) * np.float32(3.0)),
+                    2, 40).astype(np.uint8)
+        sq = ASCII[codes]
+        sq[cr.random((2 * m, L)) < n_rate] = ord("N")
+        seqs[2 * b:2 * (b + m)] = sq
+        quals[2 * b:2 * (b + m)] = q + 33
+        truth[2 * b:2 * (b + m)] = ASCII[tr]
+
+    # chunks are independent streams writing disjoint rows: run them on threads
+    import concurrent.futures
+    import os
+    nchunks = (num_pairs + chunk_pairs - 1) // chunk_pairs
+    with concurrent.futures.ThreadPoolExecutor(max_workers=min(nchunks, os.cpu_count() or 1)) as ex:
+        list(ex.map(chunk, range(nchunks)))
+    return ReadSet(seqs, quals, truth, np.full(n, L, dtype=np.int32), True, "pe_large")
+
+
 def single_end_uneven(seed: int = 3, genome_size: int = 10_000_000,
                       coverage: float = 40.0, Lmin: int = 50, Lmax: int = 250,
                       repeat_fraction: float = 0.08) -> ReadSet:
@@ -216,6 +294,7 @@ WORKLOADS = {
     "se_uniform": single_end_uniform,
     "pe_repeats": paired_end_repeats,
     "se_uneven": single_end_uneven,
+    "pe_large": paired_end_large,
 }
 
 

@@ -33,6 +33,12 @@ from . import datagen
 
 FP_WEIGHT = 30.0
 DEFAULT_ARGS = "-c 30 -k 20 -h 32 -q --qualityScoreBits 2 --pairmode PE --candidateCorrection"
+# training set models: read generator and the care-cpu options of the runs
+MODELS = {
+    "pe30": ("paired_end_repeats", DEFAULT_ARGS),
+    "large50": ("paired_end_large",
+                "-c 50 -k 20 -h 48 -q --qualityScoreBits 2 --pairmode PE --excludeAmbiguous --candidateCorrection"),
+}
 ACGT = np.frombuffer(b"ACGT", np.uint8)
 
 
@@ -102,7 +108,9 @@ def main(argv=None) -> int:
     ap.add_argument("--genomes", type=int, default=3)
     ap.add_argument("--genome-size", type=int, default=5_000_000)
     ap.add_argument("--seed", type=int, default=1000)
-    ap.add_argument("--args", default=DEFAULT_ARGS, help="care-cpu options of the training runs")
+    ap.add_argument("--model", choices=sorted(MODELS), default="pe30",
+                    help="pe30: the 30x benchmark model; large50: 50x, h48, indels and N bases")
+    ap.add_argument("--args", default=None, help="care-cpu options of the training runs (default: the model's)")
     ap.add_argument("--epochs", type=int, default=30)
     ap.add_argument("--batch", type=int, default=65536)
     ap.add_argument("--lr", type=float, default=1e-3)
@@ -111,9 +119,13 @@ def main(argv=None) -> int:
     a = ap.parse_args(argv)
     t0 = time.time()
     G = a.genome_size
-    sets = [datagen.paired_end_repeats(seed=a.seed + i, genome_size=G, repeat_unit=max(100, G // 1000))
-            for i in range(a.genomes)]
-    x, y, w = training_set(sets, a.args, device=a.gpu, fp_weight=a.fp_weight)
+    gen, margs = MODELS[a.model]
+    if gen == "paired_end_large":
+        sets = [datagen.paired_end_large(seed=a.seed + i, genome_size=G) for i in range(a.genomes)]
+    else:
+        sets = [datagen.paired_end_repeats(seed=a.seed + i, genome_size=G, repeat_unit=max(100, G // 1000))
+                for i in range(a.genomes)]
+    x, y, w = training_set(sets, a.args or margs, device=a.gpu, fp_weight=a.fp_weight)
     print(f"{x.shape[0]} rows, {float(y.mean()):.4f} consensus right, {int((w > 1).sum())} false-positive rows",
           file=sys.stderr)
     params, losses = train(x, y, w, a.epochs, a.batch, a.lr, device=a.gpu)
