@@ -536,7 +536,7 @@ int run_batch(care_b200_ctx* ctx, uint32_t first, uint32_t count, bool timed) {
     const int h = ctx->num_maps;
     // shared hash set for de-duplication: > num_maps * threshold entries
     const size_t tmax = (size_t)h * ctx->threshold;
-    int set_log2 = 4;
+    int set_log2 = 6;                 // at least 64 entries: the set and the sort pad to 64 and 32
     while ((size_t)1 << set_log2 < (tmax * 4 + 2) / 3 + 1) set_log2++;
     const int groups = kCandBlock / h;
     const size_t cand_smem = CandSmem::total(ctx->max_len, groups, h, ctx->seq_pitch, 1 << set_log2);

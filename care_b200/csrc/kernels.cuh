@@ -172,13 +172,16 @@ k_candidates(DevOptions o, DevReads r, const TableDesc* __restrict__ td, const S
     }
     __syncthreads();
     const uint32_t U = s_unique;
-    uint32_t P = 1;
+    uint32_t P = 32;
     while (P < U) P <<= 1;
     for (uint32_t i = U + tid; i < P; i += BLOCK) list[i] = kEmpty;
     __syncthreads();
-    // bitonic sort of list[0..P)
+    // bitonic sort of list[0..P): exchanges across warps (partner distance
+    // >= 32) through shared memory, one barrier each; the exchanges within a
+    // warp (distance < 32) of a merge level in registers with shuffles
+    const int wid = tid >> 5, ln = tid & 31;
     for (uint32_t kk = 2; kk <= P; kk <<= 1) {
-        for (uint32_t j = kk >> 1; j > 0; j >>= 1) {
+        for (uint32_t j = kk >> 1; j >= 32; j >>= 1) {
             for (uint32_t i = tid; i < P; i += BLOCK) {
                 const uint32_t ixj = i ^ j;
                 if (ixj > i) {
@@ -189,6 +192,17 @@ k_candidates(DevOptions o, DevReads r, const TableDesc* __restrict__ td, const S
             }
             __syncthreads();
         }
+        for (uint32_t i0 = 32u * wid; i0 < P; i0 += BLOCK) {      // warp-uniform
+            const uint32_t i = i0 + ln;
+            uint32_t x = list[i];
+            const bool up = (i & kk) == 0;
+            for (uint32_t j = min(kk >> 1, 16u); j > 0; j >>= 1) {
+                const uint32_t y = __shfl_xor_sync(0xffffffffu, x, j);
+                x = (up == ((i & j) == 0)) ? min(x, y) : max(x, y);
+            }
+            list[i] = x;
+        }
+        __syncthreads();
     }
     if (tid == 0) s_base = atomicAdd(arena_count, (unsigned long long)U);
     __syncthreads();

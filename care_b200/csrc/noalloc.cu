@@ -140,7 +140,7 @@ extern "C" int care_b200_correct_range_noalloc(const care_b200_options* opt, con
 
     const int h = o.num_maps;
     const size_t tmax = (size_t)h * o.threshold;
-    int set_log2 = 4;
+    int set_log2 = 6;                 // at least 64 entries: the set and the sort pad to 64 and 32
     while ((size_t)1 << set_log2 < (tmax * 4 + 2) / 3 + 1) set_log2++;
     const size_t cand_smem = CandSmem::total(r.max_len, 128 / h, h, r.seq_pitch, 1 << set_log2);
     if (cand_smem > 227 * 1024) return CARE_B200_ELIMIT;

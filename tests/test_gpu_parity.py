@@ -79,9 +79,13 @@ def test_stage_outputs_match_oracle(golden, case):
     ("pe", "-c 30 -k 20 -h 32 -q --qualityScoreBits 2 --pairmode PE --candidateCorrection"),
     ("se", "-c 30 -k 20 -h 16 --pairmode SE"),
     ("un", "-c 40 -k 20 -h 32 -q --qualityScoreBits 2 --pairmode SE --candidateCorrection"),
+    ("large", "-c 50 -k 20 -h 48 -q --qualityScoreBits 2 --pairmode PE --excludeAmbiguous --candidateCorrection"),
 ])
 def test_medium_sets_match_oracle(tmp_path, workload, args):
-    if workload == "pe":
+    if workload == "large":
+        # the large set's model: 50x, indels, N bases (ambiguous reads excluded)
+        rs = datagen.paired_end_large(seed=24, genome_size=300_000, chunk_pairs=20_000)
+    elif workload == "pe":
         rs = datagen.paired_end_repeats(seed=21, genome_size=300_000, repeat_unit=2000, repeat_copies=6)
     elif workload == "se":
         rs = datagen.single_end_uniform(seed=22, genome_size=200_000, num_reads=60_000)
