@@ -421,12 +421,14 @@ def main():
         corr.upload_reads(packed, lens, quals)
         corr.correct_range_raw(0, n)
     barrier()
-    e2e_s = []
+    e2e_s, up_s = [], []
     for _ in range(args.steps):
         w0 = time.perf_counter()
         corr.upload_reads(packed, lens, quals)
+        w1 = time.perf_counter()
         raw = corr.correct_range_raw(0, n)
         e2e_s.append(time.perf_counter() - w0)
+        up_s.append(w1 - w0)
     barrier()
     d2h = raw.num_anchors * (1 + 4 + raw.max_length) + int(raw.num_candidates) * (13 + raw.max_length)
     e2e_t = float(np.mean(e2e_s))
@@ -482,7 +484,8 @@ def main():
                                        "by k_align (1486 per pair at L=150)", "work_per_step": align_words,
                                "peak_source": "care-b200-peaks (measured, registers only)" if ip else None},
         "e2e": {"value": world * n / e2e_t, "unit": "reads/s", "h2d_bytes_per_step": h2d,
-                "d2h_bytes_per_step": d2h},
+                "d2h_bytes_per_step": d2h, "upload_ms": float(np.mean(up_s)) * 1e3,
+                "correct_ms": (e2e_t - float(np.mean(up_s))) * 1e3},
         "gpu_launches": launches_per_pass(corr.tuning, False, -(-n // (1 << 21))) * args.steps,
         "clocks": clk.summary(),
     }

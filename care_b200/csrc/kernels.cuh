@@ -616,6 +616,7 @@ msa_anchor(const DevOptions& o, const DevReads& r, uint32_t first, uint32_t ai,
         // ---- column sums (anchor first, then candidates in list order) and
         //      consensus (findConsensus, msa.cpp:135-157): each warp takes one
         //      32-column block at a time, lane = column ----
+#pragma unroll 1
         for (int j = 0; j < JB; ++j) {
             const int c0 = 32 * (warp + NWARP * j);
             const int col = c0 + lane;
