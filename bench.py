@@ -483,6 +483,16 @@ def main():
                                "work": "un-pruned: 2 orientations x sum over shifts of ceil(overlap/32), counted per pair "
                                        "by k_align (1486 per pair at L=150)", "work_per_step": align_words,
                                "peak_source": "care-b200-peaks (measured, registers only)" if ip else None},
+        "roofline_msa_compute": {"kernel": "k_msa", "bound": "alu", "unit": "element updates/s",
+                                 "achieved": stats["msa_elements"] / (stage[2] / 1e3),
+                                 "peak": ip["msa_elements_per_s"] if ip else None,
+                                 "frac": (stats["msa_elements"] / (stage[2] / 1e3) / ip["msa_elements_per_s"])
+                                 if ip else None,
+                                 "work": "bases added to column sums (anchor and candidates, every build), "
+                                         "counted by k_msa",
+                                 "work_per_step": stats["msa_elements"],
+                                 "peak_source": "care-b200-peaks k_peak_msa (the per-element update mix in "
+                                                "registers)" if ip else None},
         "e2e": {"value": world * n / e2e_t, "unit": "reads/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "upload_ms": float(np.mean(up_s)) * 1e3,
                 "correct_ms": (e2e_t - float(np.mean(up_s))) * 1e3},

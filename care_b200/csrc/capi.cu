@@ -118,7 +118,7 @@ struct care_b200_ctx {
     // results of the last call (pinned host)
     HBuf r_status, r_nedits, r_seq;
     HBuf r_cid, r_canc, r_cshift, r_cue, r_cseq;
-    uint64_t r_ncand = 0, r_pairs = 0, r_words = 0;
+    uint64_t r_ncand = 0, r_pairs = 0, r_words = 0, r_elems = 0;
     uint32_t r_first = 0, r_count = 0;
     bool r_valid = false;
 };
@@ -615,6 +615,7 @@ int run_batch(care_b200_ctx* ctx, uint32_t first, uint32_t count, bool timed) {
         mo.feat_meta = emit ? ctx->d_fmeta.as<uint32_t>() : nullptr;
         mo.feat_count = counters + 2;
         mo.feat_cap = emit ? fcap : 0;
+        mo.elem_count = counters + 5;
 
         AlignArgs aa{o, r, first, ctx->d_cand_ids.as<uint32_t>(), ctx->d_cand_anchor.as<uint32_t>(),
                      ctx->d_seg_off.as<uint32_t>(), ctx->d_seg_cnt.as<uint32_t>(), counters, cap, status,
@@ -687,10 +688,10 @@ int run_batch(care_b200_ctx* ctx, uint32_t first, uint32_t count, bool timed) {
                 EQ(cudaGetLastError(), "k_clf_recount");
             }
             EQ(mark(4), "event");
-            EQ(cudaMemcpyAsync(ctx->h_small.p, counters, 32, cudaMemcpyDeviceToHost, st), "counters");
-            EQ(cudaMemcpyAsync(ctx->h_small.as<char>() + 32, status, 4, cudaMemcpyDeviceToHost, st), "status");
+            EQ(cudaMemcpyAsync(ctx->h_small.p, counters, 48, cudaMemcpyDeviceToHost, st), "counters");
+            EQ(cudaMemcpyAsync(ctx->h_small.as<char>() + 48, status, 4, cudaMemcpyDeviceToHost, st), "status");
             if (o.clf_mode == 2)
-                EQ(cudaMemcpyAsync(ctx->h_small.as<char>() + 36, ctx->d_mlp_err.p, 4, cudaMemcpyDeviceToHost, st), "status");
+                EQ(cudaMemcpyAsync(ctx->h_small.as<char>() + 52, ctx->d_mlp_err.p, 4, cudaMemcpyDeviceToHost, st), "status");
 #undef EQ
             return CARE_B200_OK;
         };
@@ -719,14 +720,15 @@ int run_batch(care_b200_ctx* ctx, uint32_t first, uint32_t count, bool timed) {
         const unsigned long long corr = ctx->h_small.as<unsigned long long>()[1];
         const unsigned long long nfeat = ctx->h_small.as<unsigned long long>()[2];
         const unsigned long long words = ctx->h_small.as<unsigned long long>()[3];
-        const int stw = *(int*)(ctx->h_small.as<char>() + 32);
+        const unsigned long long elems = ctx->h_small.as<unsigned long long>()[5];
+        const int stw = *(int*)(ctx->h_small.as<char>() + 48);
         if (stw & kStatusColumns) return fail(ctx, CARE_B200_ELIMIT, "MSA wider than the kernel's column capacity");
         bool again = false;
         if ((stw & kStatusCandOverflow) || used > cap) { ctx->cand_cap = used + used / 8 + 1024; again = true; }
         if ((stw & kStatusCorrOverflow) || corr > ccap) { ctx->corr_cap = corr + corr / 8 + 1024; again = true; }
         if (emit && ((stw & kStatusFeatOverflow) || nfeat > fcap)) { ctx->feat_cap = nfeat + nfeat / 8 + 4096; again = true; }
         if (again) continue;
-        if (o.clf_mode == 2 && *(int*)(ctx->h_small.as<char>() + 36))
+        if (o.clf_mode == 2 && *(int*)(ctx->h_small.as<char>() + 52))
             return fail(ctx, CARE_B200_ECUDA, "tensor-core completion wait ran out");
         if (timed) {
             float a = 0, b = 0, c = 0, d = 0;
@@ -754,6 +756,7 @@ int run_batch(care_b200_ctx* ctx, uint32_t first, uint32_t count, bool timed) {
         ctx->r_ncand += corr;
         ctx->r_pairs += used;
         ctx->r_words += words;
+        ctx->r_elems += elems;
         return (int)std::min<unsigned long long>(corr, 0x7fffffff);
     }
     return fail(ctx, CARE_B200_ENOMEM, "arena growth did not converge");
@@ -778,6 +781,7 @@ int correct_impl(care_b200_ctx* ctx, uint32_t first, uint32_t count, care_b200_r
     ctx->r_ncand = 0;
     ctx->r_pairs = 0;
     ctx->r_words = 0;
+    ctx->r_elems = 0;
     ctx->r_valid = false;
     const int L = ctx->max_len;
     if (copy) {
@@ -1007,8 +1011,8 @@ int care_b200_last_timing(const care_b200_ctx* ctx, float* total_ms, float* stag
 
 int care_b200_last_stats(const care_b200_ctx* ctx, uint64_t* stats, int nstats) {
     if (!ctx || !stats) return CARE_B200_EINVAL;
-    const uint64_t v[4] = {ctx->r_count, ctx->r_pairs, ctx->r_ncand, ctx->r_words};
-    for (int i = 0; i < nstats && i < 4; i++) stats[i] = v[i];
+    const uint64_t v[5] = {ctx->r_count, ctx->r_pairs, ctx->r_ncand, ctx->r_words, ctx->r_elems};
+    for (int i = 0; i < nstats && i < 5; i++) stats[i] = v[i];
     return CARE_B200_OK;
 }
 

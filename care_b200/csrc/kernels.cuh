@@ -325,6 +325,9 @@ struct MsaOut {
     uint32_t* feat_meta;
     unsigned long long* feat_count;
     unsigned long long feat_cap;
+    // elements added to column sums (anchor and candidate bases, every
+    // build): the MSA stage's roofline work; may be null
+    unsigned long long* elem_count;
 };
 
 constexpr int kNumFeatures = 24;
@@ -581,30 +584,38 @@ msa_anchor(const DevOptions& o, const DevReads& r, uint32_t first, uint32_t ai,
 
     for (int iter = 0;; ++iter) {
         // ---- MSA geometry (build, msa.cpp:17-33) ----
-        int mn = 0, mx = La;
+        int mn = 0, mx = La, sl = 0;                // sl: bases of the rows (roofline work)
         if (persistent) {
             for (int i = tid; i < nalive; i += BLOCK) {
                 const int k = s_alive[i];
                 mn = min(mn, s_beg[k]);
                 mx = max(mx, s_beg[k] + s_len[k]);
+                sl += s_len[k];
             }
         } else {
             for (int k = tid; k < nalive; k += BLOCK) {
                 const CandRec rc = recs[off + k];
                 mn = min(mn, (int)rc.shift);
                 mx = max(mx, (int)rc.shift + (int)rc.len);
+                sl += rc.len;
             }
         }
 #pragma unroll
         for (int d = 16; d > 0; d >>= 1) {
             mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, d));
             mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, d));
+            sl += __shfl_xor_sync(0xffffffffu, sl, d);
         }
         __syncthreads();
-        if (lane == 0) { s_red[warp][0] = mn; s_red[warp][1] = mx; }
+        if (lane == 0) { s_red[warp][0] = mn; s_red[warp][1] = mx; s_red[warp][2] = sl; }
         __syncthreads();
         mn = 0; mx = La;
         for (int w = 0; w < NWARP; ++w) { mn = min(mn, s_red[w][0]); mx = max(mx, s_red[w][1]); }
+        if (tid == 0 && out.elem_count) {
+            int tot = La;
+            for (int w = 0; w < NWARP; ++w) tot += s_red[w][2];
+            atomicAdd(out.elem_count, (unsigned long long)tot);
+        }
         ncols = mx - mn;
         abegin = -mn;
         aend = abegin + La;

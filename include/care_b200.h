@@ -160,7 +160,9 @@ int care_b200_last_timing(const care_b200_ctx* ctx, float* total_ms, float* stag
 /* Counters of the last correction call: stats[0] anchors, stats[1]
  * (anchor, candidate) pairs aligned, stats[2] candidate corrections,
  * stats[3] un-pruned 32-bit word compares of the alignments (both
- * orientations, every scanned shift: the alignment stage's roofline work). */
+ * orientations, every scanned shift: the alignment stage's roofline work),
+ * stats[4] bases added to MSA column sums (anchor and candidates, every
+ * build including refinement rebuilds: the MSA stage's compute work). */
 int care_b200_last_stats(const care_b200_ctx* ctx, uint64_t* stats, int nstats);
 
 /* ---- correction without allocation ---- */
