@@ -371,6 +371,8 @@ msa_anchor(const DevOptions& o, const DevReads& r, uint32_t first, uint32_t ai,
     __shared__ float s_w[kStageMax];
     __shared__ uint32_t s_id[kStageMax];
     __shared__ uint8_t s_fwd[kStageMax];
+    __shared__ int2 s_bl[kStageMax];         // {begin, length} of staged row k
+    __shared__ float s_wq[kStageMax][4];     // row weight * weight of a 1- or 2-bit quality code
     __shared__ uint8_t s_alive[kStageMax];
     __shared__ int s_red[NWARP][4];
     __shared__ int s_vals[12];
@@ -519,7 +521,11 @@ msa_anchor(const DevOptions& o, const DevReads& r, uint32_t first, uint32_t ai,
     }
 
     // stage candidate rows [c, c+n) of recs into slots 0..n-1: their packed
-    // sequence and quality words, eight rows in flight per lane
+    // sequence and quality words, eight rows in flight per lane; reverse-
+    // complement rows are then turned into the alignment's orientation in
+    // place (bases reversed and complemented, qualities reversed over the
+    // whole quality pitch: reverseQualitiesOfRCAlignments, corrector.hpp:
+    // 1227-1239), so the column sums read every row forward
     auto stage = [&](int c, int n) {
         __syncthreads();
         for (int k = tid; k < n; k += BLOCK) {
@@ -529,6 +535,9 @@ msa_anchor(const DevOptions& o, const DevReads& r, uint32_t first, uint32_t ai,
             s_w[k] = rc.weight;
             s_fwd[k] = rc.orient == 1;
             s_id[k] = rc.id;
+            s_bl[k] = make_int2(rc.shift, rc.len);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) s_wq[k][q] = fmul_rn(rc.weight, s_qwc[q]);
         }
         __syncthreads();
         for (int k0 = warp; k0 < n; k0 += 8 * NWARP) {
@@ -551,24 +560,78 @@ msa_anchor(const DevOptions& o, const DevReads& r, uint32_t first, uint32_t ai,
                 }
             }
         }
+        __syncwarp();
+        // reverse-complement rows: a warp per row, each lane one output word
+        // built from a window of the source words (fetched by shuffle)
+        for (int k = warp; k < n; k += NWARP) {
+            if (s_fwd[k]) continue;                      // warp-uniform
+            uint32_t* row = s_raw + k * rw;
+            {   // bases: 16 per word, MSB first; output base p = complement of source base L-1-p
+                const int L = s_len[k];
+                const uint32_t mine = lane < sp ? row[lane] : 0u;
+                const int s0 = L - 16 - 16 * lane;       // first source base of this lane's word
+                const int wi = s0 >= 0 ? (s0 >> 4) : 0;
+                const uint32_t a = __shfl_sync(0xffffffffu, mine, wi & 31);
+                const uint32_t b = __shfl_sync(0xffffffffu, mine, (wi + 1) & 31);
+                uint32_t win;
+                if (s0 >= 0) win = (s0 & 15) ? __funnelshift_l(b, a, 2 * (s0 & 15)) : a;
+                else win = s0 > -16 ? a >> (-2 * s0) : 0u;
+                win = __brev(win);                           // reverse the 16 codes ...
+                win = ((win >> 1) & 0x55555555u) | ((win & 0x55555555u) << 1);   // ... keeping each code's bits
+                if (lane < sp) row[lane] = ~win;             // complement: A<->T, C<->G
+            }
+            if (useQ) {  // qualities reversed over the quality pitch (mlen characters)
+                uint32_t* qrow = row + sp;
+                if (qbits == 8) {        // 4 per word, little-endian bytes
+                    const uint32_t m0 = lane < qp ? qrow[lane] : 0u;
+                    const uint32_t m1 = lane + 32 < qp ? qrow[lane + 32] : 0u;
+                    __syncwarp();
+                    for (int h = 0; h < 2; ++h) {
+                        const int t = lane + 32 * h;
+                        const int s0 = mlen - 4 - 4 * t;
+                        const int wi = s0 >= 0 ? (s0 >> 2) : 0;
+                        const uint32_t a0 = __shfl_sync(0xffffffffu, m0, wi & 31);
+                        const uint32_t a1 = __shfl_sync(0xffffffffu, m1, wi & 31);
+                        const uint32_t b0 = __shfl_sync(0xffffffffu, m0, (wi + 1) & 31);
+                        const uint32_t b1 = __shfl_sync(0xffffffffu, m1, (wi + 1) & 31);
+                        const uint32_t a = wi < 32 ? a0 : a1, b = wi + 1 < 32 ? b0 : b1;
+                        uint32_t win;
+                        if (s0 >= 0) win = (s0 & 3) ? __funnelshift_r(a, b, 8 * (s0 & 3)) : a;
+                        else win = s0 > -4 ? a << (-8 * s0) : 0u;
+                        if (t < qp) qrow[t] = __byte_perm(win, 0u, 0x0123);
+                    }
+                } else {
+                    const int per = qbits == 2 ? 16 : 32;    // codes per word, MSB first
+                    const uint32_t mine = lane < qp ? qrow[lane] : 0u;
+                    __syncwarp();
+                    const int s0 = mlen - per - per * lane;
+                    const int wi = s0 >= 0 ? s0 / per : 0;
+                    const uint32_t a = __shfl_sync(0xffffffffu, mine, wi & 31);
+                    const uint32_t b = __shfl_sync(0xffffffffu, mine, (wi + 1) & 31);
+                    const int sh = s0 >= 0 ? (s0 % per) * (32 / per) : 0;
+                    uint32_t win;
+                    if (s0 >= 0) win = sh ? __funnelshift_l(b, a, sh) : a;
+                    else win = s0 > -per ? a >> (-s0 * (32 / per)) : 0u;
+                    win = __brev(win);
+                    if (per == 16) win = ((win >> 1) & 0x55555555u) | ((win & 0x55555555u) << 1);
+                    if (lane < qp) qrow[lane] = win;
+                }
+            }
+            __syncwarp();
+        }
         __syncthreads();
     };
     // base (2-bit, in the candidate's aligned orientation) of staged row k at
     // position p < s_len[k]
-    auto cand_base = [&](int k, int p) -> uint32_t {
-        const uint32_t* srow = s_raw + k * rw;
-        if (s_fwd[k]) return base_at(srow, p);
-        return base_at(srow, s_len[k] - 1 - p) ^ 3u;
-    };
-    // quality weight of staged row k at position p; reverse-complement
-    // candidates read their qualities reversed over the whole quality pitch
-    // (reverseQualitiesOfRCAlignments, corrector.hpp:1227-1239)
-    auto cand_qweight = [&](int k, int p) -> float {
+    auto cand_base = [&](int k, int p) -> uint32_t { return base_at(s_raw + k * rw, p); };
+    // weight of staged row k's element at position p: row weight times its
+    // quality weight (the product computed once per row and code for 1- and
+    // 2-bit qualities)
+    auto cand_weight = [&](int k, int p) -> float {
         const uint32_t* qrow = s_raw + k * rw + sp;
-        const int q = s_fwd[k] ? p : mlen - 1 - p;
-        if (qbits == 2) return s_qwc[(qrow[q >> 4] >> (30 - 2 * (q & 15))) & 3u];
-        if (qbits == 8) return s_qw[(qrow[q >> 2] >> (8 * (q & 3))) & 0xFFu];
-        return s_qwc[(qrow[q >> 5] >> (31 - (q & 31))) & 1u];
+        if (qbits == 2) return s_wq[k][(qrow[p >> 4] >> (30 - 2 * (p & 15))) & 3u];
+        if (qbits == 8) return fmul_rn(s_w[k], s_qw[(qrow[p >> 2] >> (8 * (p & 3))) & 0xFFu]);
+        return s_wq[k][(qrow[p >> 5] >> (31 - (p & 31))) & 1u];
     };
 
     const bool persistent = V <= nstage;      // all rows stay staged across rebuilds
@@ -660,8 +723,9 @@ msa_anchor(const DevOptions& o, const DevReads& r, uint32_t first, uint32_t ai,
                     bool hit = false;
                     if (i0 + lane < nrows) {
                         const int k = list ? list[i0 + lane] : i0 + lane;
-                        const int cb = abegin + s_beg[k];
-                        hit = cb < c0 + 32 && cb + s_len[k] > c0;
+                        const int2 bl = s_bl[k];
+                        const int cb = abegin + bl.x;
+                        hit = cb < c0 + 32 && cb + bl.y > c0;
                     }
                     unsigned m = __ballot_sync(0xffffffffu, hit);
                     while (m) {
@@ -679,10 +743,11 @@ msa_anchor(const DevOptions& o, const DevReads& r, uint32_t first, uint32_t ai,
                                 m &= m - 1;
                                 ++nu;
                                 const int k = list ? list[i] : i;
-                                const int p = col - (abegin + s_beg[k]);
-                                const bool in = (unsigned)p < (unsigned)s_len[k];
+                                const int2 bl = s_bl[k];
+                                const int p = col - (abegin + bl.x);
+                                const bool in = (unsigned)p < (unsigned)bl.y;
                                 const int pc = in ? p : 0;          // loads stay inside the row
-                                const float w = useQ ? fmul_rn(s_w[k], cand_qweight(k, pc)) : s_w[k];
+                                const float w = useQ ? cand_weight(k, pc) : s_w[k];
                                 v[u] = in;
                                 bb[u] = cand_base(k, pc);
                                 ww[u] = in ? w : 0.0f;
