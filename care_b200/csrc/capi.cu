@@ -99,6 +99,10 @@ struct care_b200_ctx {
     DBuf d_cid, d_canc, d_cshift, d_cue, d_cseq;
     unsigned long long corr_cap = 0;
     HBuf h_small;
+    // host -> device staging of uploads: two pinned chunks per copy stream
+    HBuf h_stage[2][2];
+    cudaEvent_t stage_ev[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+    cudaStream_t copy_stream = nullptr;
 
     // learned decision: parameters, decision-column rows of a batch
     DBuf d_mlp, d_mlp_err;
@@ -215,6 +219,39 @@ int compute_signatures(care_b200_ctx* ctx, int maps) {
     return CARE_B200_OK;
 }
 
+// Host -> device copy of pageable caller memory through two pinned chunks of
+// staging slot `slot`: host threads fill one chunk while the copy engine
+// drains the other. Asynchronous on `st` (the caller synchronises).
+int staged_upload(care_b200_ctx* ctx, int slot, void* dst, const void* src, size_t bytes, cudaStream_t st) {
+    constexpr size_t kChunk = 16u << 20;
+    if (bytes <= kChunk / 4) {               // small: one pinned copy is not worth it
+        CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st), "upload");
+        CK(cudaStreamSynchronize(st), "upload");
+        return CARE_B200_OK;
+    }
+    for (auto& b : ctx->h_stage[slot]) CK(b.ensure(kChunk), "alloc staging");
+    const unsigned hw = std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
+    size_t off = 0;
+    for (int i = 0; off < bytes; ++i, off += kChunk) {
+        const int b = i & 1;
+        const size_t len = std::min(kChunk, bytes - off);
+        CK(cudaEventSynchronize(ctx->stage_ev[slot][b]), "staging");   // the chunk's previous copy is done
+        char* pin = ctx->h_stage[slot][b].as<char>();
+        const char* from = static_cast<const char*>(src) + off;
+        std::vector<std::thread> th;
+        const size_t part = (len + hw - 1) / hw;
+        for (unsigned t = 0; t < hw; ++t) {
+            const size_t a = t * part;
+            if (a >= len) break;
+            th.emplace_back([=] { std::memcpy(pin + a, from + a, std::min(part, len - a)); });
+        }
+        for (auto& x : th) x.join();
+        CK(cudaMemcpyAsync(static_cast<char*>(dst) + off, pin, len, cudaMemcpyHostToDevice, st), "upload");
+        CK(cudaEventRecord(ctx->stage_ev[slot][b], st), "staging");
+    }
+    return CARE_B200_OK;
+}
+
 int validate_options(care_b200_ctx* ctx, const care_b200_options& o) {
     // ProgramOptions::isValid, src/options.cpp:387-480, plus this library's limits
     if (o.max_error_rate < 0.f || o.max_error_rate > 1.f) return fail(ctx, CARE_B200_EINVAL, "maxmismatchratio must be in [0,1]");
@@ -267,6 +304,9 @@ int care_b200_create(const care_b200_options* opt, care_b200_ctx** out) {
     CK(cudaSetDevice(opt->device), "cudaSetDevice");
     CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking), "cudaStreamCreate");
     for (auto& e : ctx->ev) CK(cudaEventCreate(&e), "cudaEventCreate");
+    CK(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    for (auto& row : ctx->stage_ev)
+        for (auto& e : row) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
     float qw[256];
     quality_weights(qw);
     CK(cudaMemcpyToSymbol(c_qweight, qw, sizeof(qw)), "quality weights");
@@ -280,6 +320,10 @@ int care_b200_destroy(care_b200_ctx* ctx) {
     cudaSetDevice(ctx->opt.device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     for (auto& e : ctx->ev) if (e) cudaEventDestroy(e);
+    if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);
+    for (auto& row : ctx->stage_ev)
+        for (auto& e : row) if (e) cudaEventDestroy(e);
+    if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
     if (ctx->gexec) cudaGraphExecDestroy(ctx->gexec);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
@@ -308,15 +352,20 @@ int care_b200_upload_reads(care_b200_ctx* ctx, const uint32_t* packed, size_t pi
     ctx->qual_pitch = ctx->has_qual ? (int)qual_pitch_ints : 0;
     if (ctx->has_qual && (size_t)quality_ints(mx, ctx->opt.quality_bits) > qual_pitch_ints)
         return fail(ctx, CARE_B200_EINVAL, "qual_pitch_ints too small for the longest read");
+    // packed rows and lengths first; the minhash signatures of the new
+    // storage are computed on the main stream while the quality words upload
+    // on the copy stream
     CK(ctx->d_seq.ensure((size_t)num_reads * pitch_ints * 4), "alloc reads");
-    CK(cudaMemcpyAsync(ctx->d_seq.p, packed, (size_t)num_reads * pitch_ints * 4, cudaMemcpyHostToDevice, ctx->stream), "upload reads");
+    if (int rc = staged_upload(ctx, 0, ctx->d_seq.p, packed, (size_t)num_reads * pitch_ints * 4, ctx->stream)) return rc;
     CK(ctx->d_len.ensure((size_t)num_reads * 4), "alloc lengths");
-    CK(cudaMemcpyAsync(ctx->d_len.p, lengths, (size_t)num_reads * 4, cudaMemcpyHostToDevice, ctx->stream), "upload lengths");
+    if (int rc = staged_upload(ctx, 0, ctx->d_len.p, lengths, (size_t)num_reads * 4, ctx->stream)) return rc;
+    ctx->sigs_maps = 0;
+    if (int rc = compute_signatures(ctx, ctx->num_maps ? ctx->num_maps : ctx->opt.num_maps)) return rc;
     if (ctx->has_qual) {
         CK(ctx->d_qual.ensure((size_t)num_reads * qual_pitch_ints * 4), "alloc qualities");
-        CK(cudaMemcpyAsync(ctx->d_qual.p, enc_quals, (size_t)num_reads * qual_pitch_ints * 4, cudaMemcpyHostToDevice, ctx->stream), "upload qualities");
+        if (int rc = staged_upload(ctx, 1, ctx->d_qual.p, enc_quals, (size_t)num_reads * qual_pitch_ints * 4,
+                                   ctx->copy_stream)) return rc;
     }
-    ctx->sigs_maps = 0;
     ctx->h_len.assign(lengths, lengths + num_reads);
     ctx->h_ambig.assign(num_reads, 0);
     for (size_t i = 0; i < num_ambiguous; i++) {
@@ -325,6 +374,7 @@ int care_b200_upload_reads(care_b200_ctx* ctx, const uint32_t* packed, size_t pi
     }
     CK(ctx->d_ambig.ensure(num_reads), "alloc ambiguous flags");
     CK(cudaMemcpyAsync(ctx->d_ambig.p, ctx->h_ambig.data(), num_reads, cudaMemcpyHostToDevice, ctx->stream), "upload ambiguous flags");
+    CK(cudaStreamSynchronize(ctx->copy_stream), "upload");
     CK(cudaStreamSynchronize(ctx->stream), "upload");
     if (ctx->tables_ready && ctx->t_keys.size() && num_reads != ctx->tables_reads) ctx->tables_ready = false;
     ctx->r_valid = false;
@@ -399,7 +449,8 @@ int care_b200_build_tables(care_b200_ctx* ctx) {
     // signatures of all reads on the device (insert, ordinaryminhasher.hpp:376-426),
     // kept resident for the candidate stage
     std::vector<uint64_t> sig((size_t)ctx->n * h);
-    if (int rc = compute_signatures(ctx, h)) return rc;
+    if (ctx->sigs_maps != h)
+        if (int rc = compute_signatures(ctx, h)) return rc;
     CK(cudaMemcpyAsync(sig.data(), ctx->d_sigs.p, (size_t)ctx->n * h * 8, cudaMemcpyDeviceToHost, ctx->stream), "signatures");
     CK(cudaStreamSynchronize(ctx->stream), "signatures");
     // group per map: values of one key ascending, buckets with fewer than 2
