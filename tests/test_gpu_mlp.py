@@ -260,3 +260,43 @@ def test_trained_network_gains_over_classic_rule(tmp_path):
     print(f"classic TP {tp0} FP {fp0} FN {fn0} F1 {f0:.5f} | network TP {tp1} FP {fp1} FN {fn1} F1 {f1:.5f}")
     assert f1 > f0
     assert fp1 < fp0
+
+
+def test_cli_learned_decision_equals_library(pe_small, tmp_path):
+    """care-b200 --correctionType 1 --ml-mlpfile writes what the library path writes."""
+    import subprocess
+    from care_b200 import learned
+    rs, inp = pe_small
+    params = learned.load_params(os.path.join(os.path.dirname(care_b200.__file__), "data", "mlp_pe30x.bin"))
+    with care_b200.Corrector(care_b200.options_from_args(ARGS, correction_type=1)) as c:
+        c.load_files([inp])
+        c.build_tables()
+        c.set_mlp(params)
+        c.correct_range()
+        lib_out = str(tmp_path / "lib.fq")
+        c.write_output(lib_out)
+    pfile = str(tmp_path / "p.bin")
+    learned.save_params(pfile, params)
+    r = subprocess.run([care_b200.CLI_PATH, "-i", inp, "-d", str(tmp_path), "-o", "cli.fq", "--correctionType", "1",
+                        "--ml-mlpfile", pfile] + ARGS.split(), capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    assert open(tmp_path / "cli.fq", "rb").read() == open(lib_out, "rb").read()
+    # without a parameter file the driver refuses type 1
+    r = subprocess.run([care_b200.CLI_PATH, "-i", inp, "-d", str(tmp_path), "-o", "x.fq", "--correctionType", "1"]
+                       + ARGS.split(), capture_output=True, text=True)
+    assert r.returncode != 0
+
+
+def test_decision_rows_over_several_batches(pe_small):
+    rs, inp = pe_small
+
+    def rows(batch):
+        with care_b200.Corrector(care_b200.options_from_args(ARGS, batch_size=batch)) as c:
+            c.load_files([inp])
+            c.build_tables()
+            return _sorted(c.collect_features())
+
+    a, b = rows(0), rows(2048)
+    for k in ("read_id", "pos", "orig", "cons"):
+        assert np.array_equal(a[k], b[k])
+    assert np.array_equal(a["x"].view(np.uint32), b["x"].view(np.uint32))

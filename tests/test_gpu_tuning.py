@@ -115,3 +115,18 @@ def test_variants_with_the_learned_decision(tmp_path):
         assert np.array_equal(fb[k], fv[k])
     assert np.array_equal(fb["x"].view(np.uint32), fv["x"].view(np.uint32))
     assert np.array_equal(fb["logit"], fv["logit"])
+
+
+def test_autotuner_on_a_sample(uneven):
+    """The tuner walks the knobs, checks every variant's results against the
+    default's and returns a valid mapping no slower than the default."""
+    from care_b200 import autotune
+    rs, inp, d = uneven
+    with care_b200.Corrector(care_b200.options_from_args(UNEVEN_ARGS)) as c:
+        c.load_files([inp])
+        c.build_tables()
+        best, info = autotune.tune(c, c.num_reads, sweeps=1, steps=1, log=lambda m: None)
+        c.tuning = best                                       # accepted by the library
+    assert set(best) == set(autotune.DEFAULT)
+    assert info["best_ms"] <= info["default_ms"]
+    assert len(info["measured"]) >= 1 + sum(len(v) - 1 for v in autotune.KNOBS.values())
