@@ -4,6 +4,7 @@
 #include "hostio.hpp"
 #include "kernels.cuh"
 #include "mlp.hpp"
+#include "tables.hpp"
 
 #include <algorithm>
 #include <cmath>
@@ -35,6 +36,7 @@ struct DBuf {
         if (e == cudaSuccess) bytes = n;
         return e;
     }
+    void adopt(void* q, size_t n) { release(); p = q; bytes = n; }
     template <class T> T* as() const { return static_cast<T*>(p); }
 };
 
@@ -448,9 +450,50 @@ int care_b200_build_tables(care_b200_ctx* ctx) {
     DevReads r = make_dev_reads(ctx);
     // signatures of all reads on the device (insert, ordinaryminhasher.hpp:376-426),
     // kept resident for the candidate stage
-    std::vector<uint64_t> sig((size_t)ctx->n * h);
     if (ctx->sigs_maps != h)
         if (int rc = compute_signatures(ctx, h)) return rc;
+    {
+        // grouping on the device: radix sort, runs, kept keys, slots
+        DeviceTables t = build_tables_device(ctx->d_sigs.as<unsigned long long>(), ctx->n, h,
+                                             ctx->opt.kmerlength, ctx->threshold, ctx->stream);
+        if (t.error == cudaSuccess) {
+            // host copies for care_b200_get_table
+            std::vector<unsigned long long> keys(t.nkeys);
+            std::vector<uint32_t> koff(t.nkeys), vals(t.nvalues);
+            if (t.nkeys) {
+                CK(cudaMemcpyAsync(keys.data(), t.keys.p, (size_t)t.nkeys * 8, cudaMemcpyDeviceToHost, ctx->stream), "tables");
+                CK(cudaMemcpyAsync(koff.data(), t.key_off.p, (size_t)t.nkeys * 4, cudaMemcpyDeviceToHost, ctx->stream), "tables");
+            }
+            if (t.nvalues)
+                CK(cudaMemcpyAsync(vals.data(), t.values.p, (size_t)t.nvalues * 4, cudaMemcpyDeviceToHost, ctx->stream), "tables");
+            CK(cudaStreamSynchronize(ctx->stream), "tables");
+            ctx->num_maps = h;
+            ctx->t_keys.assign(h, {});
+            ctx->t_off.assign(h, {});
+            ctx->t_val.assign(h, {});
+            for (int m = 0; m < h; m++) {
+                const uint32_t f = t.map_first[m], c = t.map_keys[m], vb = t.map_vbase[m], vc = t.map_vcount[m];
+                ctx->t_keys[m].assign(keys.begin() + f, keys.begin() + f + c);
+                auto& off = ctx->t_off[m];
+                off.resize(c + 1);
+                for (uint32_t i = 0; i < c; i++) off[i] = koff[f + i] - vb;
+                off[c] = vc;
+                ctx->t_val[m].assign(vals.begin() + vb, vals.begin() + vb + vc);
+            }
+            const size_t ns = t.total_slots, nv = std::max<size_t>(t.nvalues, 1);
+            ctx->d_slots.adopt(t.slots.release(), ns * sizeof(Slot));
+            ctx->d_values.adopt(t.values.release(), nv * 4);
+            ctx->d_tdesc.adopt(t.desc.release(), (size_t)h * sizeof(TableDesc));
+            ctx->tables_ready = true;
+            ctx->tables_reads = ctx->n;
+            return CARE_B200_OK;
+        }
+        // only a composite key wider than 64 bits (2k + log2(maps)) sends the
+        // grouping to the host; any other failure is an error
+        if (t.error != cudaErrorInvalidValue) return cuda_fail(ctx, t.error, "table build on the device");
+        cudaGetLastError();
+    }
+    std::vector<uint64_t> sig((size_t)ctx->n * h);
     CK(cudaMemcpyAsync(sig.data(), ctx->d_sigs.p, (size_t)ctx->n * h * 8, cudaMemcpyDeviceToHost, ctx->stream), "signatures");
     CK(cudaStreamSynchronize(ctx->stream), "signatures");
     // group per map: values of one key ascending, buckets with fewer than 2
