@@ -324,6 +324,92 @@ CB_HD void shd_scan(uint32_t (&Sh)[NW + 2], uint32_t (&Sl)[NW + 2],
     }
 }
 
+// The forward scan of a pair of reads of equal length L, answering both
+// directions at once: (A, C) with A as anchor and (C, A) with C as anchor.
+// (C, A) at shift -s compares the same bases as (A, C) at s, with the same
+// shift range (same length, same minimum overlap), but scans in the order
+// 0, -1, ..., -(L-minov), 1, ..., L-minov (in A's shifts). Each direction's
+// result is the first shift of its own order among the valid shifts with the
+// minimal score, so the scan keeps every shift whose score can tie the best
+// (limit best - total + 2*ov + 1, direction ended only when no later shift
+// can reach the best) and records the first minimal shift of each order.
+// Shift s < 0 has rank -s in the (C, A) order, s > 0 rank (L-minov) + s.
+template <int NW>
+CB_HD void shd_scan_ties(uint32_t (&Sh)[NW + 2], uint32_t (&Sl)[NW + 2],
+                         const uint32_t (&Oh)[NW + 2], const uint32_t (&Ol)[NW + 2],
+                         int t0, int t1, int sign, int L, int negs, int total,
+                         const int* __restrict__ mextab, int& best, int& shiftA, int& shiftB) {
+    if (t1 < t0) return;
+    bool stop = false;
+#pragma unroll 1
+    for (int w = 0; w <= (t1 >> 5) && !stop; ++w) {
+        const int rb = (w == (t0 >> 5)) ? (t0 & 31) : 0;
+        const int re = (w == (t1 >> 5)) ? (t1 & 31) : 31;
+#pragma unroll 1
+        for (int r = rb; r <= re; ++r) {
+            const int t = 32 * w + r;
+            const int ov = L - t;                       // equal lengths: overlap L - |shift|
+            const int mex = min(mextab[ov], best - total + 2 * ov + 1);
+            if (mex <= 0) { stop = true; break; }
+            uint32_t d0 = (funnel_l(Sh[1], Sh[0], r) ^ Oh[0]) | (funnel_l(Sl[1], Sl[0], r) ^ Ol[0]);
+            uint32_t d1 = (funnel_l(Sh[2], Sh[1], r) ^ Oh[1]) | (funnel_l(Sl[2], Sl[1], r) ^ Ol[1]);
+            if (ov < 64) { d0 &= lead_mask(ov); d1 &= lead_mask(ov - 32); }
+            int mm = popc32(d0) + popc32(d1);
+            if (mm < mex && ov > 64) {
+#pragma unroll
+                for (int j = 2; j < NW; ++j) {
+                    if (32 * j < ov && mm < mex) {
+                        uint32_t dj = (funnel_l(Sh[j + 1], Sh[j], r) ^ Oh[j]) |
+                                      (funnel_l(Sl[j + 1], Sl[j], r) ^ Ol[j]);
+                        dj &= lead_mask(ov - 32 * j);
+                        mm += popc32(dj);
+                    }
+                }
+            }
+            if (mm < mex) {
+                const int sc = mm + total - 2 * ov;
+                const int s = sign * t;
+                if (sc < best) { best = sc; shiftA = s; shiftB = s; }
+                else if (sc == best) {
+                    const int rs = s <= 0 ? -s : negs + s, rb2 = shiftB <= 0 ? -shiftB : negs + shiftB;
+                    if (rs < rb2) shiftB = s;
+                }
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < NW + 1; ++j) { Sh[j] = Sh[j + 1]; Sl[j] = Sl[j + 1]; }
+        Sh[NW + 1] = 0u; Sl[NW + 1] = 0u;
+    }
+}
+
+// Forward alignments of (A, C) and (C, A) for reads of equal length L.
+template <int NW>
+CB_HD void shifted_hamming_pair(const uint32_t (&Ah)[NW + 2], const uint32_t (&Al)[NW + 2],
+                                const uint32_t (&Ch)[NW + 2], const uint32_t (&Cl)[NW + 2], int L, int minov,
+                                const int* __restrict__ mextab, ShdResult& ac, ShdResult& ca) {
+    const int total = 2 * L;
+    int best = total, shiftA = -L, shiftB = -L;
+    uint32_t Sh[NW + 2], Sl[NW + 2];
+#pragma unroll 1
+    for (int dir = 0; dir < 2; ++dir) {
+#pragma unroll
+        for (int j = 0; j < NW + 2; ++j) { Sh[j] = dir ? Ch[j] : Ah[j]; Sl[j] = dir ? Cl[j] : Al[j]; }
+        if (dir == 0) shd_scan_ties<NW>(Sh, Sl, Ch, Cl, 0, L - minov, +1, L, L - minov, total, mextab, best, shiftA, shiftB);
+        else shd_scan_ties<NW>(Sh, Sl, Ah, Al, 1, L - minov, -1, L, L - minov, total, mextab, best, shiftA, shiftB);
+    }
+    auto fill = [&](ShdResult& res, int shift) {
+        res.valid = shift != -L;
+        const int cb = max(-shift, 0);
+        const int ce = min(L, L - shift);
+        res.overlap = ce - cb;
+        res.score = best;
+        res.shift = shift;
+        res.nops = best - total + 2 * res.overlap;
+    };
+    fill(ac, shiftA);
+    fill(ca, shiftB == -L ? -L : -shiftB);
+}
+
 // Sum of ceil(v/32) for v = 1..n (0 for n <= 0).
 CB_HD int words_prefix(int n) {
     if (n <= 0) return 0;

@@ -57,4 +57,26 @@ void hd_canonical_kmers(const uint32_t* seq, int len, int k, unsigned long long*
 unsigned long long hd_murmur64(unsigned long long x) { return murmur64(x); }
 
 int hd_unpruned_words(int la, int lc, int minov) { return unpruned_words(la, lc, minov); }
+
+// forward alignments of (a, c) and (c, a) from one scan (equal lengths);
+// out: score, overlap, shift, nops, valid of (a, c) then of (c, a)
+int hd_shd_pair(const uint32_t* a, const uint32_t* c, int len, int min_overlap, float mer, float ratio, int* out) {
+    constexpr int NW = 8;
+    if (len > 32 * NW) return -1;
+    uint32_t Ah[NW + 2], Al[NW + 2], Ch[NW + 2], Cl[NW + 2];
+    load_planes<NW>(a, len, Ah, Al);
+    load_planes<NW>(c, len, Ch, Cl);
+    int mextab[kMaxLen + 1];
+    for (int i = 0; i <= kMaxLen; i++) mextab[i] = f2i_rz(fmul_rn((float)i, mer));
+    const int lo = f2i_rz(fmul_rn((float)len, ratio));
+    const int minov = min_overlap > lo ? min_overlap : lo;
+    ShdResult ac, ca;
+    shifted_hamming_pair<NW>(Ah, Al, Ch, Cl, len, minov, mextab, ac, ca);
+    const ShdResult* rs[2] = {&ac, &ca};
+    for (int k = 0; k < 2; k++) {
+        out[5 * k + 0] = rs[k]->score; out[5 * k + 1] = rs[k]->overlap; out[5 * k + 2] = rs[k]->shift;
+        out[5 * k + 3] = rs[k]->nops; out[5 * k + 4] = rs[k]->valid;
+    }
+    return 0;
+}
 }

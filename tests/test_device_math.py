@@ -30,6 +30,8 @@ def harness():
     lib.hd_murmur64.argtypes = [ctypes.c_uint64]
     lib.hd_murmur64.restype = ctypes.c_uint64
     lib.hd_unpruned_words.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    lib.hd_shd_pair.argtypes = [P(ctypes.c_uint32), P(ctypes.c_uint32), ctypes.c_int, ctypes.c_int, ctypes.c_float,
+                                ctypes.c_float, P(ctypes.c_int)]
     return lib
 
 
@@ -119,3 +121,36 @@ def test_unpruned_word_count_closed_form():
         la, lc = rng.randint(1, 256), rng.randint(1, 256)
         mo = max(rng.randint(1, 80), int(la * 0.3))
         assert H.hd_unpruned_words(la, lc, mo) == brute(la, lc, mo), (la, lc, mo)
+
+
+def _oracle_shd(a, c, mo, mer, ratio):
+    res = _oracle.CoAlign()
+    O.co_shd(enc(a), len(a), enc(c), len(c), mo, mer, ratio, ctypes.byref(res))
+    return [res.score, res.overlap, res.shift, res.nops, res.valid]
+
+
+@pytest.mark.parametrize("seed", range(200))
+def test_pair_scan_equals_both_directions(seed):
+    """One tie-aware scan of an equal-length pair gives the reference's
+    alignment of (a, c) and of (c, a): random pairs, overlapping pairs with
+    errors, and low-complexity pairs whose scores tie at several shifts."""
+    rng = random.Random(7000 + seed)
+    L = rng.choice([50, 64, 100, 101, 150, 160, 200, 250])
+    kind = seed % 4
+    if kind == 0:
+        a = "".join(rng.choice("ACGT") for _ in range(L))
+        c = "".join(rng.choice("ACGT") for _ in range(L))
+    elif kind == 1:
+        g = "".join(rng.choice("ACGT") for _ in range(2 * L))
+        sh = rng.randint(0, L // 2)
+        a, c = mutate(rng, g[:L], rng.randint(0, 6)), mutate(rng, g[sh:sh + L], rng.randint(0, 6))
+    else:
+        unit = "".join(rng.choice("ACGT") for _ in range(rng.randint(1, 4)))
+        g = (unit * (2 * L))[:2 * L]
+        sh = rng.randint(0, L // 2)
+        a, c = mutate(rng, g[:L], rng.randint(0, 3)), mutate(rng, g[sh:sh + L], rng.randint(0, 3))
+    mo, mer, ratio = 30, 0.2, 0.30
+    out = (ctypes.c_int * 10)()
+    assert H.hd_shd_pair(enc(a), enc(c), L, mo, mer, ratio, out) == 0
+    assert list(out[:5]) == _oracle_shd(a, c, mo, mer, ratio), (a, c)
+    assert list(out[5:]) == _oracle_shd(c, a, mo, mer, ratio), (a, c)
