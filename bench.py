@@ -261,10 +261,11 @@ def int_peaks():
 
 def launches_per_pass(tuning: dict, learned: bool, batches: int = 1) -> int:
     """Kernels of this library launched by one correction pass: candidates,
-    alignment, MSA; the anchor-order kernels and the pair-order kernel when
-    the mapping uses them; inference, verdicts and edit recount with the
+    alignment, MSA; the anchor-order kernels, the pair-order kernel and the
+    mirror work list when the mapping uses them; inference, verdicts and edit recount with the
     learned decision."""
-    k = 3 + (3 if tuning.get("msa_order") else 0) + (1 if tuning.get("pair_order") else 0)
+    k = 3 + (3 if tuning.get("msa_order") else 0) + (1 if tuning.get("pair_order") else 0) + \
+        (1 if tuning.get("pair_mirror") else 0)
     return batches * (k + (3 if learned else 0))
 
 

@@ -117,7 +117,7 @@ struct care_b200_ctx {
 
     // launch mapping (care_b200_set_tuning) and its scratch
     care_b200_tuning tune{0, 0, 4, 128, 0, 0};
-    DBuf d_order, d_bins, d_pair_order;
+    DBuf d_order, d_bins, d_pair_order, d_pair_work;
     cudaGraphExec_t gexec = nullptr;
     int sms = 0;
 
@@ -556,6 +556,7 @@ struct AlignArgs {
     const uint32_t* cand_ids; const uint32_t* cand_anchor; const uint32_t* seg_off; const uint32_t* seg_cnt;
     const unsigned long long* total; unsigned long long cap; const int* status; AlignRes* out;
     unsigned long long* words; const uint32_t* pair_order;
+    const uint2* work; const unsigned int* work_n;
 };
 
 template <int B, int NW>
@@ -563,7 +564,7 @@ cudaError_t align_go(const AlignArgs& a, cudaStream_t st) {
     const unsigned long long blocks = (a.cap + B - 1) / B;
     k_align<B, NW><<<(unsigned)blocks, B, 0, st>>>(a.o, a.r, a.first, a.cand_ids, a.cand_anchor, a.seg_off,
                                                    a.seg_cnt, a.total, a.cap, a.status, a.out, a.words,
-                                                   a.pair_order);
+                                                   a.pair_order, a.work, a.work_n);
     return cudaGetLastError();
 }
 
@@ -677,6 +678,7 @@ int run_batch(care_b200_ctx* ctx, uint32_t first, uint32_t count, bool timed) {
         CK(ctx->d_ares.ensure(cap * sizeof(AlignRes)), "alloc alignments");
         CK(ctx->d_recs.ensure(cap * sizeof(CandRec)), "alloc records");
         if (tu.pair_order) CK(ctx->d_pair_order.ensure(cap * 4), "alloc pair order");
+        if (tu.pair_mirror) CK(ctx->d_pair_work.ensure(cap * 8), "alloc mirror work list");
         const unsigned long long ccap = ctx->corr_cap;
         CK(ctx->d_cid.ensure(ccap * 4), "alloc");
         CK(ctx->d_canc.ensure(ccap * 4), "alloc");
@@ -714,7 +716,9 @@ int run_batch(care_b200_ctx* ctx, uint32_t first, uint32_t count, bool timed) {
         AlignArgs aa{o, r, first, ctx->d_cand_ids.as<uint32_t>(), ctx->d_cand_anchor.as<uint32_t>(),
                      ctx->d_seg_off.as<uint32_t>(), ctx->d_seg_cnt.as<uint32_t>(), counters, cap, status,
                      ctx->d_ares.as<AlignRes>(), counters + 3,
-                     tu.pair_order ? ctx->d_pair_order.as<uint32_t>() : nullptr};
+                     tu.pair_order ? ctx->d_pair_order.as<uint32_t>() : nullptr,
+                     tu.pair_mirror ? ctx->d_pair_work.as<uint2>() : nullptr,
+                     reinterpret_cast<const unsigned int*>(counters + 6)};
         MsaArgs ma{o, r, first, count, tu.msa_order ? ctx->d_order.as<uint32_t>() : nullptr,
                    reinterpret_cast<unsigned int*>(counters + 4), ctx->d_cand_ids.as<uint32_t>(),
                    ctx->d_seg_off.as<uint32_t>(), ctx->d_seg_cnt.as<uint32_t>(), ctx->d_ares.as<AlignRes>(),
@@ -752,6 +756,14 @@ int run_batch(care_b200_ctx* ctx, uint32_t first, uint32_t count, bool timed) {
                                                     ctx->d_seg_cnt.as<uint32_t>(), count, status,
                                                     ctx->d_pair_order.as<uint32_t>());
                 EQ(cudaGetLastError(), "k_pair_order");
+            }
+            if (tu.pair_mirror) {
+                k_pair_mirror<256><<<(unsigned)((cap + 255) / 256), 256, 0, st>>>(
+                    r, first, count, ctx->d_cand_ids.as<uint32_t>(), ctx->d_cand_anchor.as<uint32_t>(),
+                    ctx->d_seg_off.as<uint32_t>(), ctx->d_seg_cnt.as<uint32_t>(), counters, cap, status,
+                    tu.pair_order ? ctx->d_pair_order.as<uint32_t>() : nullptr, ctx->d_pair_work.as<uint2>(),
+                    reinterpret_cast<unsigned int*>(counters + 6));
+                EQ(cudaGetLastError(), "k_pair_mirror");
             }
             EQ(align_dispatch(tu.align_block, nw, aa, st), "k_align");
             EQ(mark(2), "event");
@@ -958,7 +970,7 @@ int care_b200_correct_range_device(care_b200_ctx* ctx, uint32_t first, uint32_t 
 
 int care_b200_default_tuning(care_b200_tuning* t) {
     if (!t) return CARE_B200_EINVAL;
-    *t = care_b200_tuning{0, 0, 4, 128, 0, 0};
+    *t = care_b200_tuning{0, 0, 4, 128, 0, 0, 0};
     return CARE_B200_OK;
 }
 
@@ -966,7 +978,7 @@ int care_b200_set_tuning(care_b200_ctx* ctx, const care_b200_tuning* t) {
     if (!ctx || !t) return CARE_B200_EINVAL;
     if ((t->msa_warps != 4 && t->msa_warps != 8) || (t->align_block != 128 && t->align_block != 256) ||
         (unsigned)t->msa_order > 1 || (unsigned)t->msa_queue > 1 || (unsigned)t->pair_order > 1 ||
-        (unsigned)t->graph > 1)
+        (unsigned)t->graph > 1 || (unsigned)t->pair_mirror > 1)
         return fail(ctx, CARE_B200_EINVAL, "invalid tuning");
     ctx->tune = *t;
     return CARE_B200_OK;

@@ -222,13 +222,84 @@ k_candidates(DevOptions o, DevReads r, const TableDesc* __restrict__ td, const S
 //   chooseBestAlignmentOrientation    include/alignmentorientation.hpp:72-92
 //   computePairFlags                  include/corrector.hpp:763-807 (PE)
 // ---------------------------------------------------------------------------
+constexpr uint32_t kNoMirror = 0xffffffffu;
+
+// Mirror pairs. When candidate c of anchor a is itself an anchor of the
+// batch, has a's length and holds a among its candidates, the pairs (a, c)
+// and (c, a) share their scans: the reverse-complement alignments are the
+// same (same shift, overlap and mismatches) and both forward alignments come
+// from one tie-aware scan (shifted_hamming_pair). The pair with a < c leads
+// and computes both results; its mirror is skipped. Work list: leaders
+// {pair, mirror} from the front, single pairs {pair, kNoMirror} from the
+// back (index total-1 down), counts in work_n[0] and work_n[1].
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK)
+k_pair_mirror(DevReads r, uint32_t first, uint32_t count, const uint32_t* __restrict__ cand_ids,
+              const uint32_t* __restrict__ cand_anchor, const uint32_t* __restrict__ seg_off,
+              const uint32_t* __restrict__ seg_cnt, const unsigned long long* __restrict__ total_ptr,
+              unsigned long long arena_cap, const int* __restrict__ status, const uint32_t* __restrict__ pair_order,
+              uint2* __restrict__ work, unsigned int* __restrict__ work_n) {
+    if (*status & kStatusCandOverflow) return;
+    const unsigned long long total = *total_ptr;
+    if (total > arena_cap) return;
+    const unsigned long long slot = (unsigned long long)blockIdx.x * BLOCK + threadIdx.x;
+    if (slot - (threadIdx.x & 31) >= total) return;          // whole warp past the end
+    int kind = 0;                                            // 1 leader, 2 single
+    uint32_t i = 0, j = kNoMirror;
+    if (slot < total) {
+        i = pair_order ? pair_order[slot] : (uint32_t)slot;
+        const uint32_t a = first + cand_anchor[i];
+        const uint32_t c = cand_ids[i];
+        kind = 2;
+        if (c - first < count && r.len[a] == r.len[c]) {
+            const uint32_t ci = c - first, off = seg_off[ci], cnt = seg_cnt[ci];
+            uint32_t lo = 0, hi = cnt;
+            while (lo < hi) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (cand_ids[off + mid] < a) lo = mid + 1; else hi = mid;
+            }
+            if (lo < cnt && cand_ids[off + lo] == a) {
+                j = off + lo;
+                kind = a < c ? 1 : 0;
+            }
+        }
+    }
+    const unsigned ln = threadIdx.x & 31, below = (1u << ln) - 1u;
+    const unsigned ml = __ballot_sync(0xffffffffu, kind == 1), ms = __ballot_sync(0xffffffffu, kind == 2);
+    unsigned bl = 0, bs = 0;
+    if (ln == 0) {
+        if (ml) bl = atomicAdd(&work_n[0], (unsigned)__popc(ml));
+        if (ms) bs = atomicAdd(&work_n[1], (unsigned)__popc(ms));
+    }
+    bl = __shfl_sync(0xffffffffu, bl, 0);
+    bs = __shfl_sync(0xffffffffu, bs, 0);
+    if (kind == 1) work[bl + __popc(ml & below)] = make_uint2(i, j);
+    if (kind == 2) work[total - 1 - (bs + __popc(ms & below))] = make_uint2(i, kNoMirror);
+}
+
+// Candidate c's pair flag: c's mate is a candidate of the anchor's mate
+// (equivalent to flagPairedCandidates, include/util.hpp:1016-1197).
+__device__ __forceinline__ uint8_t mate_flag(const uint32_t* __restrict__ cand_ids, const uint32_t* __restrict__ seg_off,
+                       const uint32_t* __restrict__ seg_cnt, uint32_t ai, uint32_t c) {
+    const uint32_t mi = ai ^ 1u;
+    const uint32_t moff = seg_off[mi], mcnt = seg_cnt[mi];
+    const uint32_t target = c ^ 1u;
+    uint32_t lo2 = 0, hi2 = mcnt;
+    while (lo2 < hi2) {
+        const uint32_t mid = (lo2 + hi2) >> 1;
+        if (cand_ids[moff + mid] < target) lo2 = mid + 1; else hi2 = mid;
+    }
+    return (lo2 < mcnt && cand_ids[moff + lo2] == target) ? 1 : 0;
+}
+
 template <int BLOCK, int NW>
 __global__ void __launch_bounds__(BLOCK)
 k_align(DevOptions o, DevReads r, uint32_t first, const uint32_t* __restrict__ cand_ids,
         const uint32_t* __restrict__ cand_anchor, const uint32_t* __restrict__ seg_off,
         const uint32_t* __restrict__ seg_cnt, const unsigned long long* __restrict__ total_ptr,
         unsigned long long arena_cap, const int* __restrict__ status, AlignRes* __restrict__ out,
-        unsigned long long* __restrict__ work_count, const uint32_t* __restrict__ pair_order) {
+        unsigned long long* __restrict__ work_count, const uint32_t* __restrict__ pair_order,
+        const uint2* __restrict__ work, const unsigned int* __restrict__ work_n) {
     __shared__ int s_mex[kMaxLen + 1];
     // int(float(ov) * maxErrorRate), the first term of max_errors_excl
     for (int i = threadIdx.x; i <= kMaxLen; i += BLOCK) s_mex[i] = __float2int_rz(__fmul_rn((float)i, o.max_error_rate));
@@ -239,7 +310,17 @@ k_align(DevOptions o, DevReads r, uint32_t first, const uint32_t* __restrict__ c
     const unsigned long long slot = (unsigned long long)blockIdx.x * BLOCK + threadIdx.x;
     const unsigned long long total = *total_ptr;
     if (total > arena_cap || slot >= total) return;
-    const unsigned long long i = pair_order ? pair_order[slot] : slot;
+    unsigned long long i;
+    uint32_t j = kNoMirror;
+    if (work) {                        // mirror work list (k_pair_mirror)
+        const unsigned nl = work_n[0], ns = work_n[1];
+        if (slot >= (unsigned long long)nl + ns) return;
+        const uint2 w = slot < nl ? work[slot] : work[total - 1 - (slot - nl)];
+        i = w.x;
+        j = w.y;
+    } else {
+        i = pair_order ? pair_order[slot] : slot;
+    }
     const uint32_t ai = cand_anchor[i];
     const uint32_t a = first + ai;
     const uint32_t c = cand_ids[i];
@@ -249,38 +330,31 @@ k_align(DevOptions o, DevReads r, uint32_t first, const uint32_t* __restrict__ c
     load_planes<NW>(r.seq + (size_t)c * r.seq_pitch, Lc, Ch, Cl);
     const int lo = __float2int_rz(__fmul_rn((float)La, o.min_overlap_ratio));
     const int minov = o.min_overlap > lo ? o.min_overlap : lo;
-    if (work_count) {                 // un-pruned word compares, both orientations (roofline work)
+    if (work_count) {                 // un-pruned word compares of the scans run here (roofline work)
         const unsigned m = __activemask();
         const unsigned ws = __reduce_add_sync(m, (unsigned)(2 * unpruned_words(La, Lc, minov)));
         if ((int)(threadIdx.x & 31) == __ffs(m) - 1) atomicAdd(work_count, (unsigned long long)ws);
     }
-    const ShdResult f = shifted_hamming<NW>(Ah, Al, La, Ch, Cl, Lc, minov, s_mex);
+    ShdResult f, g;                   // g: forward alignment of the mirror pair (c, a)
+    if (j != kNoMirror) shifted_hamming_pair<NW>(Ah, Al, Ch, Cl, La, minov, s_mex, f, g);
+    else f = shifted_hamming<NW>(Ah, Al, La, Ch, Cl, Lc, minov, s_mex);
     uint32_t Rh[NW + 2], Rl[NW + 2];
     revcomp_planes<NW>(Ch, Cl, Lc, Rh, Rl);
     const ShdResult rc = shifted_hamming<NW>(Ah, Al, La, Rh, Rl, Lc, minov, s_mex);
-    const int orient = choose_orientation(f, rc, La, o.min_overlap_ratio, o.min_overlap,
-                                          __fmul_rn(o.estimated_errorrate, 4.0f));
-    AlignRes res;
-    const ShdResult& b = orient == 2 ? rc : f;
-    res.shift = (int16_t)b.shift;
-    res.overlap = (int16_t)b.overlap;
-    res.nops = (int16_t)b.nops;
-    res.orient = (uint8_t)orient;
-    res.paired = 0;
-    if (o.paired_end) {
-        // candidate c is paired iff c's mate is a candidate of the anchor's mate
-        // (equivalent to flagPairedCandidates, include/util.hpp:1016-1197)
-        const uint32_t mi = ai ^ 1u;
-        const uint32_t moff = seg_off[mi], mcnt = seg_cnt[mi];
-        const uint32_t target = c ^ 1u;
-        uint32_t lo2 = 0, hi2 = mcnt;
-        while (lo2 < hi2) {
-            const uint32_t mid = (lo2 + hi2) >> 1;
-            if (cand_ids[moff + mid] < target) lo2 = mid + 1; else hi2 = mid;
-        }
-        res.paired = (lo2 < mcnt && cand_ids[moff + lo2] == target) ? 1 : 0;
-    }
-    out[i] = res;
+    const float ler = __fmul_rn(o.estimated_errorrate, 4.0f);
+    auto result = [&](const ShdResult& fw, uint32_t anchor_index, uint32_t cand) {
+        const int orient = choose_orientation(fw, rc, La, o.min_overlap_ratio, o.min_overlap, ler);
+        AlignRes res;
+        const ShdResult& b = orient == 2 ? rc : fw;
+        res.shift = (int16_t)b.shift;
+        res.overlap = (int16_t)b.overlap;
+        res.nops = (int16_t)b.nops;
+        res.orient = (uint8_t)orient;
+        res.paired = o.paired_end ? mate_flag(cand_ids, seg_off, seg_cnt, anchor_index, cand) : 0;
+        return res;
+    };
+    out[i] = result(f, ai, c);
+    if (j != kNoMirror) out[j] = result(g, c - first, a);
 }
 
 // ---------------------------------------------------------------------------

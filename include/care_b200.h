@@ -159,8 +159,9 @@ int care_b200_last_timing(const care_b200_ctx* ctx, float* total_ms, float* stag
 
 /* Counters of the last correction call: stats[0] anchors, stats[1]
  * (anchor, candidate) pairs aligned, stats[2] candidate corrections,
- * stats[3] un-pruned 32-bit word compares of the alignments (both
- * orientations, every scanned shift: the alignment stage's roofline work),
+ * stats[3] un-pruned 32-bit word compares of the alignment scans run (both
+ * orientations, every scanned shift; a mirrored pair's shared scans count
+ * once: the alignment stage's roofline work),
  * stats[4] bases added to MSA column sums (anchor and candidates, every
  * build including refinement rebuilds: the MSA stage's compute work). */
 int care_b200_last_stats(const care_b200_ctx* ctx, uint64_t* stats, int nstats);
@@ -316,6 +317,8 @@ typedef struct care_b200_tuning {
     int align_block;   /* threads per CTA of the alignment stage: 128 or 256 */
     int pair_order;    /* 1: alignment pairs packed by candidate length within each anchor */
     int graph;         /* 1: each batch's launches replayed as one CUDA graph */
+    int pair_mirror;   /* 1: pairs (a, c) and (c, a) of equal-length anchors of one batch share
+                          their scans (one scan answers both forward alignments) */
 } care_b200_tuning;
 
 int care_b200_default_tuning(care_b200_tuning* t);

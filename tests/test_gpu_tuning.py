@@ -1,9 +1,10 @@
 """Launch-mapping variants (care_b200_tuning) leave every result unchanged:
 LPT anchor order, the persistent work-queue MSA kernel, 8 warps per anchor,
-256-thread alignment CTAs, length-packed alignment pairs and CUDA-graph
-replay of each batch are byte-identical to the default mapping, through the
-C ABI, on an uneven workload (candidate counts from 1 to thousands) and in
-several batches."""
+256-thread alignment CTAs, length-packed alignment pairs, mirrored pairs
+sharing their scans and CUDA-graph replay of each batch are byte-identical
+to the default mapping, through the C ABI, on an uneven workload (candidate
+counts from 1 to thousands), on equal-length paired-end reads and in several
+batches."""
 import os
 
 import numpy as np
@@ -22,7 +23,10 @@ VARIANTS = [
     {"align_block": 256},
     {"pair_order": 1},
     {"graph": 1},
-    {"msa_order": 1, "msa_queue": 1, "msa_warps": 8, "align_block": 256, "pair_order": 1, "graph": 1},
+    {"pair_mirror": 1},
+    {"pair_mirror": 1, "pair_order": 1},
+    {"msa_order": 1, "msa_queue": 1, "msa_warps": 8, "align_block": 256, "pair_order": 1, "graph": 1,
+     "pair_mirror": 1},
 ]
 
 UNEVEN_ARGS = "-c 40 -k 20 -h 32 -q --qualityScoreBits 2 --pairmode SE --candidateCorrection"
@@ -87,6 +91,36 @@ def test_variant_in_several_batches(uneven, variant):
     from batch to batch (last batch smaller)."""
     rs, inp, d = uneven
     _same(_run(inp, UNEVEN_ARGS), _run(inp, UNEVEN_ARGS, variant, batch_size=4096))
+
+
+@pytest.mark.parametrize("batch_size", [0, 1536], ids=["one-batch", "batches"])
+def test_mirror_pairs_paired_end(tmp_path, batch_size):
+    """Equal-length paired-end reads of a repeat-rich genome (many tied
+    shifts): with pair_mirror most pairs are answered by their mirror's scan,
+    and records, pair flags and the written file are unchanged. With small
+    batches only pairs whose reads are anchors of the same batch mirror."""
+    rs = datagen.paired_end_repeats(seed=63, genome_size=150_000, repeat_unit=600, repeat_copies=8)
+    inp = str(tmp_path / "pe.fq")
+    rs.write_fastq(inp)
+    args = "-c 30 -k 20 -h 32 -q --qualityScoreBits 2 --pairmode PE --candidateCorrection"
+    outs, stats = [], []
+    for tuning in (None, {"pair_mirror": 1}):
+        with care_b200.Corrector(care_b200.options_from_args(args, batch_size=batch_size)) as c:
+            c.load_files([inp])
+            c.build_tables()
+            if tuning:
+                c.tuning = dict(care_b200.Tuning.from_dict({}).as_dict(), **tuning)
+            res = c.correct_range()
+            stats.append(c.last_stats())
+            out = str(tmp_path / f"out{len(outs)}.fq")
+            c.write_output(out)
+        outs.append((res, out))
+    _same(outs[0][0], outs[1][0])
+    assert open(outs[0][1], "rb").read() == open(outs[1][1], "rb").read()
+    assert stats[0]["pairs"] == stats[1]["pairs"]
+    # the scans run: about half of all pairs in one batch, fewer saved in many
+    ratio = stats[1]["word_compares"] / stats[0]["word_compares"]
+    assert ratio < (0.6 if batch_size == 0 else 1.0)
 
 
 def test_variants_with_the_learned_decision(tmp_path):
