@@ -387,6 +387,7 @@ def main():
             mcorr.correct_range_device(0, n)
         barrier()
         mms, mstage, _ = timed_steps(mcorr, n, args.steps, flush)
+        mbatches = mcorr.last_stats()["batches"]
         barrier()
         if world > 1:
             t = torch.tensor([mms], device=f"cuda:{local}")
@@ -409,7 +410,7 @@ def main():
                                 "classifier": mstage[3]},
                    "network": "24-64-64-1 GELU, bf16 tcgen05 GEMMs, fp32 accumulate",
                    "params": os.path.relpath(mlp_file, ROOT),
-                   "base_level": counts, "gpu_launches": launches_per_pass(mcorr_tuning, True, -(-n // (1 << 21))) * args.steps}
+                   "base_level": counts, "gpu_launches": launches_per_pass(mcorr_tuning, True, mbatches) * args.steps}
 
     progress("timed steps done")
     # e2e through the C ABI from host buffers
@@ -497,7 +498,7 @@ def main():
         "e2e": {"value": world * n / e2e_t, "unit": "reads/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "upload_ms": float(np.mean(up_s)) * 1e3,
                 "correct_ms": (e2e_t - float(np.mean(up_s))) * 1e3},
-        "gpu_launches": launches_per_pass(corr.tuning, False, -(-n // (1 << 21))) * args.steps,
+        "gpu_launches": launches_per_pass(corr.tuning, False, stats["batches"]) * args.steps,
         "clocks": clk.summary(),
     }
     if learned is not None:

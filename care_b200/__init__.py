@@ -423,10 +423,10 @@ class Corrector:
         }
 
     def last_stats(self):
-        st = (ctypes.c_uint64 * 5)()
-        self._check(self.lib.care_b200_last_stats(self._ctx, st, 5), "last_stats")
+        st = (ctypes.c_uint64 * 6)()
+        self._check(self.lib.care_b200_last_stats(self._ctx, st, 6), "last_stats")
         return {"anchors": st[0], "pairs": st[1], "candidate_corrections": st[2], "word_compares": st[3],
-                "msa_elements": st[4]}
+                "msa_elements": st[4], "batches": st[5]}
 
     def last_timing(self):
         """(total ms, [candidates, alignment, MSA, classifier] ms) of the last call."""

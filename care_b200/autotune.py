@@ -50,6 +50,7 @@ DEFAULT = {"msa_order": 0, "msa_queue": 0, "msa_warps": 4, "align_block": 128, "
 WORKLOADS = {
     "pe": ("-c 30 -k 20 -h 32 -q --qualityScoreBits 2 --pairmode PE", 5_000_000),
     "uneven": ("-c 40 -k 20 -h 32 -q --qualityScoreBits 2 --pairmode SE", 10_000_000),
+    "large": ("-c 50 -k 20 -h 48 -q --qualityScoreBits 2 --pairmode PE --excludeAmbiguous", 10_000_000),
 }
 
 
@@ -129,6 +130,8 @@ def main(argv=None) -> int:
     t0 = time.time()
     if a.workload == "uneven":
         rs = datagen.single_end_uneven(seed=a.seed, genome_size=G, coverage=40.0)
+    elif a.workload == "large":
+        rs = datagen.paired_end_large(seed=a.seed, genome_size=G)
     else:
         rs = datagen.paired_end_repeats(seed=a.seed, genome_size=G, repeat_unit=max(100, G // 1000))
     with tempfile.TemporaryDirectory() as d:

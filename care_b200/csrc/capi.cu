@@ -65,6 +65,9 @@ constexpr int kMsaBlock = 128;
 
 }  // namespace
 
+// Largest candidate arena of one batch: pair indices and offsets are 32-bit.
+constexpr unsigned long long kMaxBatchPairs = 0xffffffffull;
+
 struct care_b200_ctx {
     care_b200_options opt{};
     std::string err;
@@ -124,7 +127,8 @@ struct care_b200_ctx {
     // results of the last call (pinned host)
     HBuf r_status, r_nedits, r_seq;
     HBuf r_cid, r_canc, r_cshift, r_cue, r_cseq;
-    uint64_t r_ncand = 0, r_pairs = 0, r_words = 0, r_elems = 0;
+    uint64_t r_ncand = 0, r_pairs = 0, r_words = 0, r_elems = 0, r_batches = 0;
+    double pairs_per_anchor = 96.0;   // seen in the last correction call (automatic batch size)
     uint32_t r_first = 0, r_count = 0;
     bool r_valid = false;
 };
@@ -651,7 +655,11 @@ int run_batch(care_b200_ctx* ctx, uint32_t first, uint32_t count, bool timed) {
         CK(ctx->d_order.ensure((size_t)count * 4), "alloc");
         CK(ctx->d_bins.ensure(kLptBins * 4), "alloc");
     }
-    if (ctx->cand_cap < (unsigned long long)count * 96) ctx->cand_cap = (unsigned long long)count * 96;
+    {   // the pairs per anchor seen last, with a margin (96 before the first call)
+        const unsigned long long want = std::min<unsigned long long>(
+            kMaxBatchPairs, (unsigned long long)((double)count * ctx->pairs_per_anchor * 1.1) + 1024);
+        if (ctx->cand_cap < want) ctx->cand_cap = want;
+    }
     if (ctx->corr_cap == 0) ctx->corr_cap = ctx->opt.correct_candidates ? (unsigned long long)count * 16 + 1024 : 1024;
     const bool emit = o.clf_mode != 0;
     if (emit) {
@@ -830,7 +838,13 @@ int run_batch(care_b200_ctx* ctx, uint32_t first, uint32_t count, bool timed) {
         const int stw = *(int*)(ctx->h_small.as<char>() + 48);
         if (stw & kStatusColumns) return fail(ctx, CARE_B200_ELIMIT, "MSA wider than the kernel's column capacity");
         bool again = false;
-        if ((stw & kStatusCandOverflow) || used > cap) { ctx->cand_cap = used + used / 8 + 1024; again = true; }
+        if ((stw & kStatusCandOverflow) || used > cap) {
+            // pair indices and segment offsets are 32-bit
+            if (used + used / 8 + 1024 > kMaxBatchPairs)
+                return fail(ctx, CARE_B200_ELIMIT, "more than 2^32-1 candidate pairs in one batch: set a smaller batch_size");
+            ctx->cand_cap = used + used / 8 + 1024;
+            again = true;
+        }
         if ((stw & kStatusCorrOverflow) || corr > ccap) { ctx->corr_cap = corr + corr / 8 + 1024; again = true; }
         if (emit && ((stw & kStatusFeatOverflow) || nfeat > fcap)) { ctx->feat_cap = nfeat + nfeat / 8 + 4096; again = true; }
         if (again) continue;
@@ -868,6 +882,33 @@ int run_batch(care_b200_ctx* ctx, uint32_t first, uint32_t count, bool timed) {
     return fail(ctx, CARE_B200_ENOMEM, "arena growth did not converge");
 }
 
+// Anchors per batch when the caller leaves it to the library: as many as half
+// of the free device memory holds at the pairs per anchor seen last (96 before
+// the first call) -- one batch for most read sets, so that every candidate is
+// an anchor of the same batch (mirror pairs) and nothing is launched twice --
+// at least 2^20, and few enough for 32-bit pair indices with room to grow.
+uint32_t auto_batch(care_b200_ctx* ctx, uint32_t count) {
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) { cudaGetLastError(); return 1u << 21; }
+    // the batch scratch this context already holds is reused, not added
+    for (const DBuf* d : {&ctx->d_seg_off, &ctx->d_seg_cnt, &ctx->d_cand_ids, &ctx->d_cand_anchor, &ctx->d_ares,
+                          &ctx->d_recs, &ctx->d_st, &ctx->d_ned, &ctx->d_oseq, &ctx->d_cid, &ctx->d_canc,
+                          &ctx->d_cshift, &ctx->d_cue, &ctx->d_cseq, &ctx->d_order, &ctx->d_pair_order,
+                          &ctx->d_pair_work, &ctx->d_fx, &ctx->d_fread, &ctx->d_fmeta, &ctx->d_flogit,
+                          &ctx->d_touched})
+        free_b += d->bytes;
+    const double ppa = ctx->pairs_per_anchor;
+    const double L = ctx->max_len;
+    double per_anchor = ppa * (4 + 4 + sizeof(AlignRes) + sizeof(CandRec) + 8 + 4)   // ids, anchors, alignments,
+                        + 2 * L + 64;                                             // records, work, order; rows
+    if (ctx->opt.correct_candidates) per_anchor += 16 * (13 + L);
+    if (ctx->opt.correction_type == 1) per_anchor += 0.5 * (kNumFeatures * 4 + 12);
+    double b = 0.5 * (double)free_b / per_anchor;
+    b = std::min(b, (double)kMaxBatchPairs / (1.25 * ppa));
+    b = std::max(b, (double)(1u << 20));
+    return (uint32_t)std::min<double>(b, std::max<uint32_t>(count, 2));
+}
+
 int correct_impl(care_b200_ctx* ctx, uint32_t first, uint32_t count, care_b200_results* res, bool copy) {
     if (!ctx) return CARE_B200_EINVAL;
     if (ctx->n == 0) return fail(ctx, CARE_B200_ESTATE, "no reads uploaded");
@@ -879,7 +920,7 @@ int correct_impl(care_b200_ctx* ctx, uint32_t first, uint32_t count, care_b200_r
     if (ctx->sigs_maps != ctx->num_maps)
         if (int rc = compute_signatures(ctx, ctx->num_maps)) return rc;
     ctx->r_fx.clear(); ctx->r_fread.clear(); ctx->r_fmeta.clear(); ctx->r_flogit.clear();
-    uint32_t B = ctx->opt.batch_size > 0 ? (uint32_t)ctx->opt.batch_size : (1u << 21);
+    uint32_t B = ctx->opt.batch_size > 0 ? (uint32_t)ctx->opt.batch_size : auto_batch(ctx, count);
     if (ctx->opt.paired_end) B &= ~1u;
     if (B == 0) B = 2;
     ctx->last_ms = 0.f;
@@ -888,6 +929,7 @@ int correct_impl(care_b200_ctx* ctx, uint32_t first, uint32_t count, care_b200_r
     ctx->r_pairs = 0;
     ctx->r_words = 0;
     ctx->r_elems = 0;
+    ctx->r_batches = 0;
     ctx->r_valid = false;
     const int L = ctx->max_len;
     if (copy) {
@@ -902,6 +944,7 @@ int correct_impl(care_b200_ctx* ctx, uint32_t first, uint32_t count, care_b200_r
         const uint64_t before = ctx->r_ncand;
         const int rc = run_batch(ctx, first + b, cnt, true);
         if (rc < 0) return rc;
+        ctx->r_batches++;
         const uint64_t nc = ctx->r_ncand - before;
         if (copy) {
             CK(cudaMemcpyAsync(ctx->r_status.as<uint8_t>() + b, ctx->d_st.p, cnt, cudaMemcpyDeviceToHost, ctx->stream), "results");
@@ -933,6 +976,7 @@ int correct_impl(care_b200_ctx* ctx, uint32_t first, uint32_t count, care_b200_r
         corr_total += nc;
     }
     ctx->r_ncand = corr_total;
+    if (count) ctx->pairs_per_anchor = std::max(8.0, (double)ctx->r_pairs / count);
     ctx->r_first = first;
     ctx->r_count = count;
     ctx->r_valid = copy;
@@ -1117,8 +1161,8 @@ int care_b200_last_timing(const care_b200_ctx* ctx, float* total_ms, float* stag
 
 int care_b200_last_stats(const care_b200_ctx* ctx, uint64_t* stats, int nstats) {
     if (!ctx || !stats) return CARE_B200_EINVAL;
-    const uint64_t v[5] = {ctx->r_count, ctx->r_pairs, ctx->r_ncand, ctx->r_words, ctx->r_elems};
-    for (int i = 0; i < nstats && i < 5; i++) stats[i] = v[i];
+    const uint64_t v[6] = {ctx->r_count, ctx->r_pairs, ctx->r_ncand, ctx->r_words, ctx->r_elems, ctx->r_batches};
+    for (int i = 0; i < nstats && i < 6; i++) stats[i] = v[i];
     return CARE_B200_OK;
 }
 

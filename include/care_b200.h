@@ -49,7 +49,8 @@ typedef struct care_b200_options {
     int   quality_labels;           /* --correctionQualityLabels */
     int   threads;                  /* host threads for STEP1/STEP3 helpers */
     int   device;                   /* CUDA device ordinal */
-    int   batch_size;               /* anchors per device batch, 0 = automatic */
+    int   batch_size;               /* anchors per device batch, 0 = automatic (as many as half of
+                                       the free device memory holds, at least 2^20) */
     int   clf_min_coverage;         /* learned form: decision columns with a lower
                                        coverage keep the classic rule, default 3 */
 } care_b200_options;
@@ -163,7 +164,8 @@ int care_b200_last_timing(const care_b200_ctx* ctx, float* total_ms, float* stag
  * orientations, every scanned shift; a mirrored pair's shared scans count
  * once: the alignment stage's roofline work),
  * stats[4] bases added to MSA column sums (anchor and candidates, every
- * build including refinement rebuilds: the MSA stage's compute work). */
+ * build including refinement rebuilds: the MSA stage's compute work),
+ * stats[5] device batches the range was split into. */
 int care_b200_last_stats(const care_b200_ctx* ctx, uint64_t* stats, int nstats);
 
 /* ---- correction without allocation ---- */
