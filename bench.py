@@ -259,16 +259,6 @@ def int_peaks():
     return json.loads(r.stdout) if r.returncode == 0 else None
 
 
-def launches_per_pass(tuning: dict, learned: bool, batches: int = 1) -> int:
-    """Kernels of this library launched by one correction pass: candidates,
-    alignment, MSA; the anchor-order kernels, the pair-order kernel and the
-    mirror work list when the mapping uses them; inference, verdicts and edit recount with the
-    learned decision."""
-    k = 3 + (3 if tuning.get("msa_order") else 0) + (1 if tuning.get("pair_order") else 0) + \
-        (1 if tuning.get("pair_mirror") else 0)
-    return batches * (k + (3 if learned else 0))
-
-
 def base_counts(rs, path):
     """TP/FP/FN/TN of a corrected FASTQ against the true reads."""
     from care_b200 import datagen
@@ -387,7 +377,7 @@ def main():
             mcorr.correct_range_device(0, n)
         barrier()
         mms, mstage, _ = timed_steps(mcorr, n, args.steps, flush)
-        mbatches = mcorr.last_stats()["batches"]
+        mlaunches = mcorr.last_stats()["launches"]
         barrier()
         if world > 1:
             t = torch.tensor([mms], device=f"cuda:{local}")
@@ -402,7 +392,6 @@ def main():
             tp, fp, fn, tn = base_counts(rs, out)
             counts[name] = {"tp": tp, "fp": fp, "fn": fn, "f1": datagen.f1(tp, fp, fn)}
             os.unlink(out)
-        mcorr_tuning = mcorr.tuning
         mcorr.close()
         mvalue = world * n / (mms / 1e3)
         learned = {"value": mvalue, "unit": "reads/s", "ms_per_step": mms, "ratio_vs_plain": mvalue / value,
@@ -410,7 +399,7 @@ def main():
                                 "classifier": mstage[3]},
                    "network": "24-64-64-1 GELU, bf16 tcgen05 GEMMs, fp32 accumulate",
                    "params": os.path.relpath(mlp_file, ROOT),
-                   "base_level": counts, "gpu_launches": launches_per_pass(mcorr_tuning, True, mbatches) * args.steps}
+                   "base_level": counts, "gpu_launches": mlaunches * args.steps}
 
     progress("timed steps done")
     # e2e through the C ABI from host buffers
@@ -498,7 +487,7 @@ def main():
         "e2e": {"value": world * n / e2e_t, "unit": "reads/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "upload_ms": float(np.mean(up_s)) * 1e3,
                 "correct_ms": (e2e_t - float(np.mean(up_s))) * 1e3},
-        "gpu_launches": launches_per_pass(corr.tuning, False, stats["batches"]) * args.steps,
+        "gpu_launches": stats["launches"] * args.steps,         # counted by the library per call
         "clocks": clk.summary(),
     }
     if learned is not None:

@@ -88,7 +88,7 @@ class Tuning(ctypes.Structure):
     """care_b200_tuning: launch mapping of a batch (results do not depend on it)."""
     _fields_ = [("msa_order", ctypes.c_int), ("msa_queue", ctypes.c_int), ("msa_warps", ctypes.c_int),
                 ("align_block", ctypes.c_int), ("pair_order", ctypes.c_int), ("graph", ctypes.c_int),
-                ("pair_mirror", ctypes.c_int)]
+                ("pair_mirror", ctypes.c_int), ("cand_set_log2", ctypes.c_int)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -423,10 +423,10 @@ class Corrector:
         }
 
     def last_stats(self):
-        st = (ctypes.c_uint64 * 6)()
-        self._check(self.lib.care_b200_last_stats(self._ctx, st, 6), "last_stats")
+        st = (ctypes.c_uint64 * 8)()
+        self._check(self.lib.care_b200_last_stats(self._ctx, st, 8), "last_stats")
         return {"anchors": st[0], "pairs": st[1], "candidate_corrections": st[2], "word_compares": st[3],
-                "msa_elements": st[4], "batches": st[5]}
+                "msa_elements": st[4], "batches": st[5], "launches": st[6], "spilled_anchors": st[7]}
 
     def last_timing(self):
         """(total ms, [candidates, alignment, MSA, classifier] ms) of the last call."""

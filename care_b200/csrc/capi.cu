@@ -65,6 +65,10 @@ constexpr int kMsaBlock = 128;
 
 }  // namespace
 
+// The launch mapping of a new context: one kernel per stage in anchor order,
+// 4 MSA warps, 128-thread alignment CTAs, a 1024-entry candidate set.
+constexpr care_b200_tuning kDefaultTuning{0, 0, 4, 128, 0, 0, 0, 10};
+
 // Largest candidate arena of one batch: pair indices and offsets are 32-bit.
 constexpr unsigned long long kMaxBatchPairs = 0xffffffffull;
 
@@ -119,15 +123,15 @@ struct care_b200_ctx {
     std::vector<uint32_t> r_fread, r_fmeta;
 
     // launch mapping (care_b200_set_tuning) and its scratch
-    care_b200_tuning tune{0, 0, 4, 128, 0, 0};
-    DBuf d_order, d_bins, d_pair_order, d_pair_work;
+    care_b200_tuning tune = kDefaultTuning;
+    DBuf d_order, d_bins, d_pair_order, d_pair_work, d_spill;
     cudaGraphExec_t gexec = nullptr;
     int sms = 0;
 
     // results of the last call (pinned host)
     HBuf r_status, r_nedits, r_seq;
     HBuf r_cid, r_canc, r_cshift, r_cue, r_cseq;
-    uint64_t r_ncand = 0, r_pairs = 0, r_words = 0, r_elems = 0, r_batches = 0;
+    uint64_t r_ncand = 0, r_pairs = 0, r_words = 0, r_elems = 0, r_batches = 0, r_launches = 0, r_spilled = 0;
     double pairs_per_anchor = 96.0;   // seen in the last correction call (automatic batch size)
     uint32_t r_first = 0, r_count = 0;
     bool r_valid = false;
@@ -640,8 +644,25 @@ int run_batch(care_b200_ctx* ctx, uint32_t first, uint32_t count, bool timed) {
     const int groups = kCandBlock / h;
     const size_t cand_smem = CandSmem::total(ctx->max_len, groups, h, ctx->seq_pitch, 1 << set_log2);
     if (cand_smem > 227 * 1024) return fail(ctx, CARE_B200_ELIMIT, "num_maps * threshold too large for the de-duplication set");
-    CK(cudaFuncSetAttribute(k_candidates<kCandBlock>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cand_smem), "smem attr");
     if (ctx->sms == 0) CK(cudaDeviceGetAttribute(&ctx->sms, cudaDevAttrMultiProcessorCount, ctx->opt.device), "attr");
+    // the main candidate pass uses a set of at most 2^cand_set_log2 entries
+    // (high occupancy); anchors with more unique ids than half of it are
+    // redone by k_candidates_spill with the full set
+    const bool spill = set_log2 > tu.cand_set_log2;
+    const int set_log2_main = spill ? tu.cand_set_log2 : set_log2;
+    const size_t cand_smem_main = CandSmem::total(ctx->max_len, groups, h, ctx->seq_pitch, 1 << set_log2_main);
+    CK(cudaFuncSetAttribute(k_candidates<kCandBlock>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)cand_smem_main), "smem attr");
+    int spill_grid = 0;
+    if (spill) {
+        CK(cudaFuncSetAttribute(k_candidates_spill<kCandBlock>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)cand_smem), "smem attr");
+        int nb = 0;
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_candidates_spill<kCandBlock>, kCandBlock, cand_smem),
+           "occupancy");
+        spill_grid = ctx->sms * std::max(nb, 1);
+        CK(ctx->d_spill.ensure((size_t)count * 4), "alloc");
+    }
 
     CK(ctx->d_seg_off.ensure((size_t)count * 4), "alloc");
     CK(ctx->d_seg_cnt.ensure((size_t)count * 4), "alloc");
@@ -650,7 +671,7 @@ int run_batch(care_b200_ctx* ctx, uint32_t first, uint32_t count, bool timed) {
     CK(ctx->d_st.ensure(count), "alloc");
     CK(ctx->d_ned.ensure((size_t)count * 4), "alloc");
     CK(ctx->d_oseq.ensure((size_t)count * ctx->max_len), "alloc");
-    CK(ctx->h_small.ensure(64), "alloc");
+    CK(ctx->h_small.ensure(80), "alloc");
     if (tu.msa_order) {
         CK(ctx->d_order.ensure((size_t)count * 4), "alloc");
         CK(ctx->d_bins.ensure(kLptBins * 4), "alloc");
@@ -741,7 +762,9 @@ int run_batch(care_b200_ctx* ctx, uint32_t first, uint32_t count, bool timed) {
                          : cudaEventRecord(ctx->ev[k], st);
         };
         // every operation of one attempt, in stream order
+        int launches = 0;                     // kernels of this library enqueued by the attempt
         auto enqueue = [&]() -> int {
+            launches = 0;
 #define EQ(call, where) do { const cudaError_t e_ = (call); if (e_ != cudaSuccess) return cuda_fail(ctx, e_, where); } while (0)
             EQ(cudaMemsetAsync(counters, 0, 64, st), "memset");
             EQ(cudaMemsetAsync(status, 0, 16, st), "memset");
@@ -752,18 +775,31 @@ int run_batch(care_b200_ctx* ctx, uint32_t first, uint32_t count, bool timed) {
                 EQ(cudaMemsetAsync(ctx->d_mlp_err.p, 0, 16, st), "memset");
             }
             EQ(mark(0), "event");
-            k_candidates<kCandBlock><<<count, kCandBlock, cand_smem, st>>>(
+            unsigned int* spill_n = reinterpret_cast<unsigned int*>(counters + 7);
+            k_candidates<kCandBlock><<<count, kCandBlock, cand_smem_main, st>>>(
                 o, r, ctx->d_tdesc.as<TableDesc>(), ctx->d_slots.as<Slot>(), ctx->d_values.as<uint32_t>(),
-                ctx->d_sigs.as<unsigned long long>(), first,
-                count, set_log2, ctx->d_cand_ids.as<uint32_t>(), ctx->d_cand_anchor.as<uint32_t>(),
+                ctx->d_sigs.as<unsigned long long>(), first, count, set_log2_main,
+                spill ? ctx->d_spill.as<uint32_t>() : nullptr, spill ? spill_n : nullptr,
+                ctx->d_cand_ids.as<uint32_t>(), ctx->d_cand_anchor.as<uint32_t>(),
                 ctx->d_seg_off.as<uint32_t>(), ctx->d_seg_cnt.as<uint32_t>(), counters, cap, status);
             EQ(cudaGetLastError(), "k_candidates");
+            ++launches;
+            if (spill) {
+                k_candidates_spill<kCandBlock><<<spill_grid, kCandBlock, cand_smem, st>>>(
+                    o, r, ctx->d_tdesc.as<TableDesc>(), ctx->d_slots.as<Slot>(), ctx->d_values.as<uint32_t>(),
+                    ctx->d_sigs.as<unsigned long long>(), first, set_log2, ctx->d_spill.as<uint32_t>(), spill_n,
+                    ctx->d_cand_ids.as<uint32_t>(), ctx->d_cand_anchor.as<uint32_t>(),
+                    ctx->d_seg_off.as<uint32_t>(), ctx->d_seg_cnt.as<uint32_t>(), counters, cap, status);
+                EQ(cudaGetLastError(), "k_candidates_spill");
+                ++launches;
+            }
             EQ(mark(1), "event");
             if (tu.pair_order) {
                 k_pair_order<<<count, 128, 0, st>>>(r, ctx->d_cand_ids.as<uint32_t>(), ctx->d_seg_off.as<uint32_t>(),
                                                     ctx->d_seg_cnt.as<uint32_t>(), count, status,
                                                     ctx->d_pair_order.as<uint32_t>());
                 EQ(cudaGetLastError(), "k_pair_order");
+                ++launches;
             }
             if (tu.pair_mirror) {
                 k_pair_mirror<256><<<(unsigned)((cap + 255) / 256), 256, 0, st>>>(
@@ -772,8 +808,10 @@ int run_batch(care_b200_ctx* ctx, uint32_t first, uint32_t count, bool timed) {
                     tu.pair_order ? ctx->d_pair_order.as<uint32_t>() : nullptr, ctx->d_pair_work.as<uint2>(),
                     reinterpret_cast<unsigned int*>(counters + 6));
                 EQ(cudaGetLastError(), "k_pair_mirror");
+                ++launches;
             }
             EQ(align_dispatch(tu.align_block, nw, aa, st), "k_align");
+            ++launches;
             EQ(mark(2), "event");
             if (tu.msa_order) {
                 const unsigned g = (unsigned)std::min<uint64_t>(((uint64_t)count + 255) / 256, (uint64_t)ctx->sms * 8);
@@ -783,8 +821,10 @@ int run_batch(care_b200_ctx* ctx, uint32_t first, uint32_t count, bool timed) {
                 k_lpt_scatter<<<g, 256, 0, st>>>(ctx->d_seg_cnt.as<uint32_t>(), count, ctx->d_bins.as<unsigned int>(),
                                                  ctx->d_order.as<uint32_t>());
                 EQ(cudaGetLastError(), "LPT order");
+                launches += 3;
             }
             EQ(msa_dispatch(warps, jb, emit, ma, false, st), "k_msa");
+            ++launches;
             EQ(mark(3), "event");
             if (o.clf_mode == 2) {
                 // the network decides the batch's decision columns (row count
@@ -800,12 +840,13 @@ int run_batch(care_b200_ctx* ctx, uint32_t first, uint32_t count, bool timed) {
                                                                ctx->d_oseq.as<char>(), ctx->d_st.as<uint8_t>(),
                                                                ctx->d_ned.as<int32_t>());
                 EQ(cudaGetLastError(), "k_clf_recount");
+                launches += 3;                   // inference, verdicts, recount
             }
             EQ(mark(4), "event");
-            EQ(cudaMemcpyAsync(ctx->h_small.p, counters, 48, cudaMemcpyDeviceToHost, st), "counters");
-            EQ(cudaMemcpyAsync(ctx->h_small.as<char>() + 48, status, 4, cudaMemcpyDeviceToHost, st), "status");
+            EQ(cudaMemcpyAsync(ctx->h_small.p, counters, 64, cudaMemcpyDeviceToHost, st), "counters");
+            EQ(cudaMemcpyAsync(ctx->h_small.as<char>() + 64, status, 4, cudaMemcpyDeviceToHost, st), "status");
             if (o.clf_mode == 2)
-                EQ(cudaMemcpyAsync(ctx->h_small.as<char>() + 52, ctx->d_mlp_err.p, 4, cudaMemcpyDeviceToHost, st), "status");
+                EQ(cudaMemcpyAsync(ctx->h_small.as<char>() + 68, ctx->d_mlp_err.p, 4, cudaMemcpyDeviceToHost, st), "status");
 #undef EQ
             return CARE_B200_OK;
         };
@@ -830,12 +871,14 @@ int run_batch(care_b200_ctx* ctx, uint32_t first, uint32_t count, bool timed) {
             if (int rc = enqueue()) return rc;
         }
         CK(cudaStreamSynchronize(st), "batch");
+        ctx->r_launches += launches;
         const unsigned long long used = ctx->h_small.as<unsigned long long>()[0];
         const unsigned long long corr = ctx->h_small.as<unsigned long long>()[1];
         const unsigned long long nfeat = ctx->h_small.as<unsigned long long>()[2];
         const unsigned long long words = ctx->h_small.as<unsigned long long>()[3];
         const unsigned long long elems = ctx->h_small.as<unsigned long long>()[5];
-        const int stw = *(int*)(ctx->h_small.as<char>() + 48);
+        const unsigned int spilled = ctx->h_small.as<unsigned int>()[14];     // counters + 7
+        const int stw = *(int*)(ctx->h_small.as<char>() + 64);
         if (stw & kStatusColumns) return fail(ctx, CARE_B200_ELIMIT, "MSA wider than the kernel's column capacity");
         bool again = false;
         if ((stw & kStatusCandOverflow) || used > cap) {
@@ -848,7 +891,7 @@ int run_batch(care_b200_ctx* ctx, uint32_t first, uint32_t count, bool timed) {
         if ((stw & kStatusCorrOverflow) || corr > ccap) { ctx->corr_cap = corr + corr / 8 + 1024; again = true; }
         if (emit && ((stw & kStatusFeatOverflow) || nfeat > fcap)) { ctx->feat_cap = nfeat + nfeat / 8 + 4096; again = true; }
         if (again) continue;
-        if (o.clf_mode == 2 && *(int*)(ctx->h_small.as<char>() + 52))
+        if (o.clf_mode == 2 && *(int*)(ctx->h_small.as<char>() + 68))
             return fail(ctx, CARE_B200_ECUDA, "tensor-core completion wait ran out");
         if (timed) {
             float a = 0, b = 0, c = 0, d = 0;
@@ -877,6 +920,7 @@ int run_batch(care_b200_ctx* ctx, uint32_t first, uint32_t count, bool timed) {
         ctx->r_pairs += used;
         ctx->r_words += words;
         ctx->r_elems += elems;
+        ctx->r_spilled += spilled;
         return (int)std::min<unsigned long long>(corr, 0x7fffffff);
     }
     return fail(ctx, CARE_B200_ENOMEM, "arena growth did not converge");
@@ -895,7 +939,7 @@ uint32_t auto_batch(care_b200_ctx* ctx, uint32_t count) {
                           &ctx->d_recs, &ctx->d_st, &ctx->d_ned, &ctx->d_oseq, &ctx->d_cid, &ctx->d_canc,
                           &ctx->d_cshift, &ctx->d_cue, &ctx->d_cseq, &ctx->d_order, &ctx->d_pair_order,
                           &ctx->d_pair_work, &ctx->d_fx, &ctx->d_fread, &ctx->d_fmeta, &ctx->d_flogit,
-                          &ctx->d_touched})
+                          &ctx->d_touched, &ctx->d_spill})
         free_b += d->bytes;
     const double ppa = ctx->pairs_per_anchor;
     const double L = ctx->max_len;
@@ -930,6 +974,8 @@ int correct_impl(care_b200_ctx* ctx, uint32_t first, uint32_t count, care_b200_r
     ctx->r_words = 0;
     ctx->r_elems = 0;
     ctx->r_batches = 0;
+    ctx->r_launches = 0;
+    ctx->r_spilled = 0;
     ctx->r_valid = false;
     const int L = ctx->max_len;
     if (copy) {
@@ -1014,7 +1060,7 @@ int care_b200_correct_range_device(care_b200_ctx* ctx, uint32_t first, uint32_t 
 
 int care_b200_default_tuning(care_b200_tuning* t) {
     if (!t) return CARE_B200_EINVAL;
-    *t = care_b200_tuning{0, 0, 4, 128, 0, 0, 0};
+    *t = kDefaultTuning;
     return CARE_B200_OK;
 }
 
@@ -1022,7 +1068,7 @@ int care_b200_set_tuning(care_b200_ctx* ctx, const care_b200_tuning* t) {
     if (!ctx || !t) return CARE_B200_EINVAL;
     if ((t->msa_warps != 4 && t->msa_warps != 8) || (t->align_block != 128 && t->align_block != 256) ||
         (unsigned)t->msa_order > 1 || (unsigned)t->msa_queue > 1 || (unsigned)t->pair_order > 1 ||
-        (unsigned)t->graph > 1 || (unsigned)t->pair_mirror > 1)
+        (unsigned)t->graph > 1 || (unsigned)t->pair_mirror > 1 || t->cand_set_log2 < 6 || t->cand_set_log2 > 14)
         return fail(ctx, CARE_B200_EINVAL, "invalid tuning");
     ctx->tune = *t;
     return CARE_B200_OK;
@@ -1161,8 +1207,9 @@ int care_b200_last_timing(const care_b200_ctx* ctx, float* total_ms, float* stag
 
 int care_b200_last_stats(const care_b200_ctx* ctx, uint64_t* stats, int nstats) {
     if (!ctx || !stats) return CARE_B200_EINVAL;
-    const uint64_t v[6] = {ctx->r_count, ctx->r_pairs, ctx->r_ncand, ctx->r_words, ctx->r_elems, ctx->r_batches};
-    for (int i = 0; i < nstats && i < 6; i++) stats[i] = v[i];
+    const uint64_t v[8] = {ctx->r_count, ctx->r_pairs, ctx->r_ncand, ctx->r_words, ctx->r_elems, ctx->r_batches,
+                           ctx->r_launches, ctx->r_spilled};
+    for (int i = 0; i < nstats && i < 8; i++) stats[i] = v[i];
     return CARE_B200_OK;
 }
 

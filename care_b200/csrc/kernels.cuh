@@ -44,19 +44,22 @@ struct CandSmem {
     }
 };
 
+// The candidate list of anchor ai, by one CTA. The de-duplication set has
+// 2^sl2 entries, sl2 the smallest with 2^sl2 >= 2T (T ids retrieved), at most
+// 2^set_log2. With a spill list the capacity is small (most anchors hold a few
+// dozen unique ids among hundreds retrieved) and an anchor with more than
+// half as many unique ids is appended to the list instead: its segment is
+// then written by k_candidates_spill with a set large enough for every id.
 template <int BLOCK>
-__global__ void __launch_bounds__(BLOCK)
-k_candidates(DevOptions o, DevReads r, const TableDesc* __restrict__ td, const Slot* __restrict__ slots,
-             const uint32_t* __restrict__ values, const unsigned long long* __restrict__ sig,
-             uint32_t first, uint32_t count, int set_log2,
-             uint32_t* __restrict__ cand_ids, uint32_t* __restrict__ cand_anchor,
-             uint32_t* __restrict__ seg_off, uint32_t* __restrict__ seg_cnt,
-             unsigned long long* __restrict__ arena_count, unsigned long long arena_cap,
-             int* __restrict__ status) {
-    extern __shared__ __align__(16) unsigned char smem[];
+__device__ __forceinline__ void candidates_of(
+    const DevOptions& o, const DevReads& r, const TableDesc* __restrict__ td, const Slot* __restrict__ slots,
+    const uint32_t* __restrict__ values, const unsigned long long* __restrict__ sig, uint32_t first, uint32_t ai,
+    int set_log2, uint32_t* __restrict__ spill_list, unsigned int* __restrict__ spill_n,
+    uint32_t* __restrict__ cand_ids, uint32_t* __restrict__ cand_anchor, uint32_t* __restrict__ seg_off,
+    uint32_t* __restrict__ seg_cnt, unsigned long long* __restrict__ arena_count, unsigned long long arena_cap,
+    int* __restrict__ status, unsigned char* smem, uint32_t& s_unique, uint32_t& s_ins, uint32_t& s_full,
+    unsigned long long& s_base) {
     const int tid = threadIdx.x;
-    const uint32_t ai = blockIdx.x;
-    if (ai >= count) return;
     const uint32_t a = first + ai;
     const int h = o.num_maps;
     const int groups = BLOCK / h;
@@ -69,8 +72,6 @@ k_candidates(DevOptions o, DevReads r, const TableDesc* __restrict__ td, const S
     uint32_t* qpre = qcnt + kMaxMaps;              // kMaxMaps + 1 entries
     uint32_t* set = (uint32_t*)(smem + CandSmem::set(r.max_len, groups, h, r.seq_pitch));
     uint32_t* list = set + setcap;
-    __shared__ uint32_t s_unique;
-    __shared__ unsigned long long s_base;
 
     const int L = r.len[a];
     const bool skip = (o.exclude_ambiguous && r.ambig[a]) || L < o.k;
@@ -133,12 +134,20 @@ k_candidates(DevOptions o, DevReads r, const TableDesc* __restrict__ td, const S
         qoff[tid] = (uint32_t)d.value_base + off;
         qcnt[tid] = cnt;
     }
-    if (tid == 0) s_unique = 0;
+    if (tid == 0) { s_unique = 0; s_ins = 0; s_full = 0; }
     __syncthreads();
-    if (tid == 0) {
-        uint32_t acc = 0;
-        for (int m = 0; m < h; ++m) { qpre[m] = acc; acc += qcnt[m]; }
-        qpre[h] = acc;
+    if (tid < 32) {                                  // offsets of the maps' runs: warp scan, two maps per lane
+        const uint32_t c0 = tid < h ? qcnt[tid] : 0u, c1 = tid + 32 < h ? qcnt[tid + 32] : 0u;
+        uint32_t s0 = c0, s1 = c1;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t t0 = __shfl_up_sync(0xffffffffu, s0, d), t1 = __shfl_up_sync(0xffffffffu, s1, d);
+            if (tid >= d) { s0 += t0; s1 += t1; }
+        }
+        const uint32_t tot0 = __shfl_sync(0xffffffffu, s0, 31);
+        if (tid < h) qpre[tid] = s0 - c0;
+        if (tid + 32 < h) qpre[tid + 32] = tot0 + s1 - c1;
+        if (tid == 31) qpre[h] = tot0 + s1;
     }
     __syncthreads();
 
@@ -148,22 +157,50 @@ k_candidates(DevOptions o, DevReads r, const TableDesc* __restrict__ td, const S
     int sl2 = 6;
     while (sl2 < set_log2 && (1u << sl2) < 2 * T) ++sl2;
     const int scap = 1 << sl2;
+    // without a spill list the set always has room (2^set_log2 > h * threshold >= T)
+    const uint32_t limit = spill_list ? (uint32_t)scap / 2 : 0xffffffffu;
     for (int i = tid; i < scap; i += BLOCK) set[i] = kEmpty;
     __syncthreads();
 
-    // insert all retrieved ids into the shared hash set
-    for (uint32_t e = tid; e < T; e += BLOCK) {
-        int lo = 0, hi = h - 1;                     // map of element e
-        while (lo < hi) { const int mid = (lo + hi + 1) >> 1; if (qpre[mid] <= e) lo = mid; else hi = mid - 1; }
-        const uint32_t id = __ldg(values + qoff[lo] + (e - qpre[lo]));
-        uint32_t pos = (id * 2654435761u) >> (32 - sl2);
-        for (int probe = 0; probe < scap; ++probe) {
-            const uint32_t prev = atomicCAS(&set[pos], kEmpty, id);
-            if (prev == kEmpty || prev == id) break;
-            pos = (pos + 1) & (scap - 1);
+    // insert all retrieved ids into the shared hash set, eight loads in
+    // flight per thread ahead of their inserts
+    constexpr int kInFlight = 8;
+    for (uint32_t e0 = 0; e0 < T; e0 += BLOCK * kInFlight) {
+        uint32_t ids[kInFlight];
+#pragma unroll
+        for (int k = 0; k < kInFlight; ++k) {
+            const uint32_t e = e0 + (uint32_t)(k * BLOCK + tid);
+            ids[k] = kEmpty;
+            if (e < T) {
+                int lo = 0, hi = h - 1;             // map of element e
+                while (lo < hi) { const int mid = (lo + hi + 1) >> 1; if (qpre[mid] <= e) lo = mid; else hi = mid - 1; }
+                ids[k] = __ldg(values + qoff[lo] + (e - qpre[lo]));
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < kInFlight; ++k) {
+            const uint32_t id = ids[k];                // read ids are < 2^32 - 1: kEmpty marks none
+            if (id == kEmpty || *(volatile uint32_t*)&s_full) continue;
+            uint32_t pos = (id * 2654435761u) >> (32 - sl2);
+            bool placed = false;
+            for (int probe = 0; probe < scap; ++probe) {
+                const uint32_t prev = atomicCAS(&set[pos], kEmpty, id);
+                if (prev == kEmpty) {
+                    placed = true;
+                    if (atomicAdd(&s_ins, 1u) >= limit) s_full = 1;
+                    break;
+                }
+                if (prev == id) { placed = true; break; }
+                pos = (pos + 1) & (scap - 1);
+            }
+            if (!placed) s_full = 1;
         }
     }
     __syncthreads();
+    if (s_full) {                                   // block-uniform: the second pass takes the anchor
+        if (tid == 0) spill_list[atomicAdd(spill_n, 1u)] = ai;
+        return;
+    }
 
     // unique ids minus the anchor itself and (optionally) ambiguous reads
     for (int i = tid; i < scap; i += BLOCK) {
@@ -213,6 +250,48 @@ k_candidates(DevOptions o, DevReads r, const TableDesc* __restrict__ td, const S
         return;
     }
     for (uint32_t i = tid; i < U; i += BLOCK) { cand_ids[base + i] = list[i]; cand_anchor[base + i] = ai; }
+}
+
+// One anchor per CTA, the set capacity 2^set_log2 (small when spill_list is
+// given: the anchors that overflow it are listed for k_candidates_spill).
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK)
+k_candidates(DevOptions o, DevReads r, const TableDesc* __restrict__ td, const Slot* __restrict__ slots,
+             const uint32_t* __restrict__ values, const unsigned long long* __restrict__ sig,
+             uint32_t first, uint32_t count, int set_log2, uint32_t* __restrict__ spill_list,
+             unsigned int* __restrict__ spill_n, uint32_t* __restrict__ cand_ids, uint32_t* __restrict__ cand_anchor,
+             uint32_t* __restrict__ seg_off, uint32_t* __restrict__ seg_cnt,
+             unsigned long long* __restrict__ arena_count, unsigned long long arena_cap,
+             int* __restrict__ status) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ uint32_t s_unique, s_ins, s_full;
+    __shared__ unsigned long long s_base;
+    if (blockIdx.x >= count) return;
+    candidates_of<BLOCK>(o, r, td, slots, values, sig, first, blockIdx.x, set_log2, spill_list, spill_n, cand_ids,
+                         cand_anchor, seg_off, seg_cnt, arena_count, arena_cap, status, smem, s_unique, s_ins,
+                         s_full, s_base);
+}
+
+// The listed anchors with a set for every retrieved id (persistent CTAs).
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK)
+k_candidates_spill(DevOptions o, DevReads r, const TableDesc* __restrict__ td, const Slot* __restrict__ slots,
+                   const uint32_t* __restrict__ values, const unsigned long long* __restrict__ sig, uint32_t first,
+                   int set_log2, const uint32_t* __restrict__ spill_list, const unsigned int* __restrict__ spill_n,
+                   uint32_t* __restrict__ cand_ids, uint32_t* __restrict__ cand_anchor,
+                   uint32_t* __restrict__ seg_off, uint32_t* __restrict__ seg_cnt,
+                   unsigned long long* __restrict__ arena_count, unsigned long long arena_cap,
+                   int* __restrict__ status) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ uint32_t s_unique, s_ins, s_full;
+    __shared__ unsigned long long s_base;
+    const unsigned int n = *spill_n;
+    for (unsigned int k = blockIdx.x; k < n; k += gridDim.x) {
+        candidates_of<BLOCK>(o, r, td, slots, values, sig, first, spill_list[k], set_log2, nullptr, nullptr,
+                             cand_ids, cand_anchor, seg_off, seg_cnt, arena_count, arena_cap, status, smem,
+                             s_unique, s_ins, s_full, s_base);
+        __syncthreads();                            // the next anchor reuses the shared state
+    }
 }
 
 // ---------------------------------------------------------------------------

@@ -148,7 +148,7 @@ extern "C" int care_b200_correct_range_noalloc(const care_b200_options* opt, con
         return CARE_B200_ECUDA;
     k_candidates<128><<<num_anchors, 128, cand_smem, st>>>(
         o, r, static_cast<const TableDesc*>(tables->descs), static_cast<const Slot*>(tables->slots), tables->values,
-        nullptr, first_anchor, num_anchors, set_log2, cand_ids, cand_anchor, seg_off, seg_cnt, counters, kNoAllocMaxPairs,
+        nullptr, first_anchor, num_anchors, set_log2, nullptr, nullptr, cand_ids, cand_anchor, seg_off, seg_cnt, counters, kNoAllocMaxPairs,
         dstatus);
     const unsigned ablocks = (unsigned)((kNoAllocMaxPairs + 127) / 128);
     const int nw = (r.max_len + 31) / 32;

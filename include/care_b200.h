@@ -165,7 +165,9 @@ int care_b200_last_timing(const care_b200_ctx* ctx, float* total_ms, float* stag
  * once: the alignment stage's roofline work),
  * stats[4] bases added to MSA column sums (anchor and candidates, every
  * build including refinement rebuilds: the MSA stage's compute work),
- * stats[5] device batches the range was split into. */
+ * stats[5] device batches the range was split into, stats[6] kernels of
+ * this library launched (every batch and every arena-growth attempt),
+ * stats[7] anchors whose candidate lists took the second, full-set pass. */
 int care_b200_last_stats(const care_b200_ctx* ctx, uint64_t* stats, int nstats);
 
 /* ---- correction without allocation ---- */
@@ -321,6 +323,9 @@ typedef struct care_b200_tuning {
     int graph;         /* 1: each batch's launches replayed as one CUDA graph */
     int pair_mirror;   /* 1: pairs (a, c) and (c, a) of equal-length anchors of one batch share
                           their scans (one scan answers both forward alignments) */
+    int cand_set_log2; /* 6..14: de-duplication set of the main candidate pass, 2^x entries;
+                          anchors with more than 2^(x-1) unique candidates take a second pass
+                          with a set for every retrieved id (default 10) */
 } care_b200_tuning;
 
 int care_b200_default_tuning(care_b200_tuning* t);

@@ -45,3 +45,16 @@ def test_create_without_gpu_fails_cleanly():
         assert "create" in str(e)
     else:
         raise AssertionError("context creation must fail loudly without a GPU")
+
+
+def test_tuning_struct_and_default():
+    """care_b200_tuning: the header's fields in order are the binding's, the
+    library's default mapping is the autotuner's starting point, and every
+    knob the tuner walks is a field."""
+    text = open(os.path.join(ROOT, "include", "care_b200.h")).read()
+    body = re.search(r"typedef struct care_b200_tuning \{(.*?)\} care_b200_tuning;", text, re.S).group(1)
+    fields = re.findall(r"^\s*int\s+(\w+);", body, re.M)
+    assert fields == [k for k, _ in care_b200.Tuning._fields_]
+    from care_b200 import autotune
+    assert care_b200.Tuning.from_dict({}).as_dict() == autotune.DEFAULT
+    assert set(autotune.KNOBS) <= set(fields)

@@ -17,12 +17,14 @@ pytestmark = pytest.mark.gpu
 CASES = sorted(__import__("conftest").manifest()["cases"])
 
 
-def run_gpu(files, args, out=None, **kw):
+def run_gpu(files, args, out=None, stats=None, **kw):
     o = care_b200.options_from_args(args, **kw)
     with care_b200.Corrector(o) as c:
         c.load_files(files)
         c.build_tables()
         res = c.correct_range()
+        if stats is not None:
+            stats.update(c.last_stats())
         if out:
             c.write_output(out)
         tables = [c.get_table(m) for m in range(c.num_maps)]

@@ -25,6 +25,8 @@ VARIANTS = [
     {"graph": 1},
     {"pair_mirror": 1},
     {"pair_mirror": 1, "pair_order": 1},
+    {"cand_set_log2": 8},
+    {"cand_set_log2": 12},
     {"msa_order": 1, "msa_queue": 1, "msa_warps": 8, "align_block": 256, "pair_order": 1, "graph": 1,
      "pair_mirror": 1},
 ]
@@ -121,6 +123,26 @@ def test_mirror_pairs_paired_end(tmp_path, batch_size):
     # the scans run: about half of all pairs in one batch, fewer saved in many
     ratio = stats[1]["word_compares"] / stats[0]["word_compares"]
     assert ratio < (0.6 if batch_size == 0 else 1.0)
+
+
+@pytest.mark.parametrize("log2", [6, 7])
+def test_candidate_spill_pass(uneven, log2):
+    """A main-pass set of 64 or 128 entries sends every anchor with more than
+    32 or 64 unique candidates to the second, full-set pass: the candidate
+    lists, and so every result, equal the default mapping's."""
+    rs, inp, d = uneven
+    base_out, var_out = str(d / "base_sp.fq"), str(d / "var_sp.fq")
+    base = _run(inp, UNEVEN_ARGS, out=base_out)
+    with care_b200.Corrector(care_b200.options_from_args(UNEVEN_ARGS)) as c:
+        c.load_files([inp])
+        c.build_tables()
+        c.tuning = dict(care_b200.Tuning.from_dict({}).as_dict(), cand_set_log2=log2)
+        var = c.correct_range()
+        st = c.last_stats()
+        c.write_output(var_out)
+    assert 0.05 * st["anchors"] < st["spilled_anchors"] < st["anchors"]
+    _same(base, var)
+    assert open(base_out, "rb").read() == open(var_out, "rb").read()
 
 
 def test_variants_with_the_learned_decision(tmp_path):
