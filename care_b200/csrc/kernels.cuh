@@ -503,6 +503,33 @@ __host__ __device__ inline size_t msa_smem_bytes(int max_len, int seq_pitch, int
     return elem + raw + (emit ? (size_t)3 * max_len * 4 : 0);
 }
 
+// One element of a column: weight w added to the sum of its base b (0..3)
+// and one to the base's 8-bit count in c8 (A | C << 8 | G << 16 | T << 24),
+// nothing when the column lies outside the row (in false). IEEE adds
+// (add.rn.f32, no contraction), predicated on (base, in): the sums see the
+// same additions in the same order as an add per element of the base.
+__device__ __forceinline__ void msa_add(float& wA, float& wC, float& wG, float& wT, uint32_t& c8,
+                                        uint32_t b, float w, bool in) {
+    asm("{\n\t"
+        ".reg .pred pin, pa, pc, pg, pt;\n\t"
+        ".reg .b32 sh, inc;\n\t"
+        "setp.ne.b32 pin, %7, 0;\n\t"
+        "setp.eq.and.b32 pa, %6, 0, pin;\n\t"
+        "setp.eq.and.b32 pc, %6, 1, pin;\n\t"
+        "setp.eq.and.b32 pg, %6, 2, pin;\n\t"
+        "setp.eq.and.b32 pt, %6, 3, pin;\n\t"
+        "@pa add.rn.f32 %0, %0, %5;\n\t"
+        "@pc add.rn.f32 %1, %1, %5;\n\t"
+        "@pg add.rn.f32 %2, %2, %5;\n\t"
+        "@pt add.rn.f32 %3, %3, %5;\n\t"
+        "shl.b32 sh, %6, 3;\n\t"
+        "shl.b32 inc, %8, sh;\n\t"
+        "@pin add.u32 %4, %4, inc;\n\t"
+        "}"
+        : "+f"(wA), "+f"(wC), "+f"(wG), "+f"(wT), "+r"(c8)
+        : "f"(w), "r"(b), "r"((uint32_t)in), "r"(1u));
+}
+
 // The whole MSA stage of one anchor (local index ai) for one CTA. Every
 // early return is taken by all threads of the CTA together.
 template <int BLOCK, int JB, bool EMIT>
@@ -849,18 +876,15 @@ msa_anchor(const DevOptions& o, const DevReads& r, uint32_t first, uint32_t ai,
             const int col = c0 + lane;
             const bool active = c0 < ncols;                  // warp-uniform
             uint32_t cAC = 0u, cGT = 0u;                     // 16-bit counts: A | C << 16, G | T << 16
+            uint32_t c8 = 0u;           // the chunk's 8-bit counts A | C << 8 | G << 16 | T << 24
             float wA = 0.0f, wC = 0.0f, wG = 0.0f, wT = 0.0f;
-            // branch-free add of one element; a lane outside the row adds
-            // weight +0.0f (an exact identity on the non-negative sums) and
-            // no count
-            auto add = [&](uint32_t b, float w, bool valid) {
-                const uint32_t inc = valid ? (1u << (16 * (b & 1u))) : 0u;
-                cAC += (b & 2u) ? 0u : inc;
-                cGT += (b & 2u) ? inc : 0u;
-                wA = __fadd_rn(wA, b == 0 ? w : 0.0f);
-                wC = __fadd_rn(wC, b == 1 ? w : 0.0f);
-                wG = __fadd_rn(wG, b == 2 ? w : 0.0f);
-                wT = __fadd_rn(wT, b == 3 ? w : 0.0f);
+            auto add = [&](uint32_t b, float w, bool valid) { msa_add(wA, wC, wG, wT, c8, b, w, valid); };
+            // a chunk adds at most 128 rows and the anchor: its 8-bit counts
+            // cannot overflow before they are moved to the 16-bit ones
+            auto flush = [&]() {
+                cAC += (c8 & 0xFFu) | ((c8 & 0xFF00u) << 8);
+                cGT += ((c8 >> 16) & 0xFFu) | ((c8 >> 24) << 16);
+                c8 = 0u;
             };
             {
                 const int p = col - abegin;
@@ -903,7 +927,7 @@ msa_anchor(const DevOptions& o, const DevReads& r, uint32_t first, uint32_t ai,
                                 const float w = useQ ? cand_weight(k, pc) : s_w[k];
                                 v[u] = in;
                                 bb[u] = cand_base(k, pc);
-                                ww[u] = in ? w : 0.0f;
+                                ww[u] = w;
                             }
                         }
 #pragma unroll
@@ -920,8 +944,10 @@ msa_anchor(const DevOptions& o, const DevReads& r, uint32_t first, uint32_t ai,
                     const int n = min(nstage, nalive - c);
                     stage(c, n);
                     if (active) run_rows(nullptr, n);
+                    flush();
                 }
             }
+            flush();
             if (active && col < ncols) {
                 uint8_t cs = 0; float cw = wA;
                 if (wC > cw) { cs = 1; cw = wC; }
