@@ -20,8 +20,12 @@ DEPS = [SRC, os.path.join(ROOT, "care_b200", "csrc", "device.cuh")]
 def harness():
     os.makedirs(os.path.dirname(OUT), exist_ok=True)
     if not os.path.exists(OUT) or any(os.path.getmtime(d) > os.path.getmtime(OUT) for d in DEPS):
+        # built under a process-private name and renamed into place: test
+        # workers that start together never load a half-written library
+        tmp = f"{OUT}.{os.getpid()}.tmp"
         subprocess.run(["nvcc", "-shared", "-Xcompiler", "-fPIC,-ffp-contract=off", "-O2", "-std=c++17",
-                        "-o", OUT, SRC], check=True, capture_output=True)
+                        "-o", tmp, SRC], check=True, capture_output=True)
+        os.replace(tmp, OUT)
     lib = ctypes.CDLL(OUT)
     P = ctypes.POINTER
     lib.hd_shd.argtypes = [P(ctypes.c_uint32), ctypes.c_int, P(ctypes.c_uint32), ctypes.c_int, ctypes.c_int,
