@@ -74,7 +74,7 @@ EXPORTS = [
     "care_b200_build_tables", "care_b200_get_table", "care_b200_correct_range",
     "care_b200_correct_range_device", "care_b200_serialize_results",
     "care_b200_load_reads_from_files", "care_b200_write_output", "care_b200_last_timing",
-    "care_b200_last_stats", "care_b200_num_reads", "care_b200_max_length", "care_b200_num_maps",
+    "care_b200_last_stats", "care_b200_count_word_compares", "care_b200_num_reads", "care_b200_max_length", "care_b200_num_maps",
     "care_b200_correct_range_noalloc",
     "care_b200_set_mlp", "care_b200_collect_features", "care_b200_mlp_default_train_options",
     "care_b200_mlp_create", "care_b200_mlp_destroy", "care_b200_mlp_last_error", "care_b200_mlp_set_params",
@@ -174,6 +174,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.care_b200_write_output.argtypes = [c_ctx, ctypes.c_char_p]
     lib.care_b200_last_timing.argtypes = [c_ctx, P(ctypes.c_float), P(ctypes.c_float), ctypes.c_int]
     lib.care_b200_last_stats.argtypes = [c_ctx, P(ctypes.c_uint64), ctypes.c_int]
+    lib.care_b200_count_word_compares.argtypes = [c_ctx, ctypes.c_int]
     lib.care_b200_correct_range_noalloc.argtypes = [P(Options), P(DeviceReads), P(DeviceTables), ctypes.c_uint32,
                                                      ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p,
                                                      ctypes.c_void_p, ctypes.c_void_p]
@@ -423,10 +424,16 @@ class Corrector:
         }
 
     def last_stats(self):
-        st = (ctypes.c_uint64 * 8)()
-        self._check(self.lib.care_b200_last_stats(self._ctx, st, 8), "last_stats")
+        st = (ctypes.c_uint64 * 9)()
+        self._check(self.lib.care_b200_last_stats(self._ctx, st, 9), "last_stats")
         return {"anchors": st[0], "pairs": st[1], "candidate_corrections": st[2], "word_compares": st[3],
-                "msa_elements": st[4], "batches": st[5], "launches": st[6], "spilled_anchors": st[7]}
+                "msa_elements": st[4], "batches": st[5], "launches": st[6], "spilled_anchors": st[7],
+                "word_compares_run": st[8]}
+
+    def count_word_compares(self, on: bool = True):
+        """Run the alignment's statistics form in the following calls: it also
+        counts the word compares actually run (last_stats()["word_compares_run"])."""
+        self._check(self.lib.care_b200_count_word_compares(self._ctx, int(bool(on))), "count_word_compares")
 
     def last_timing(self):
         """(total ms, [candidates, alignment, MSA, classifier] ms) of the last call."""

@@ -132,6 +132,8 @@ struct care_b200_ctx {
     HBuf r_status, r_nedits, r_seq;
     HBuf r_cid, r_canc, r_cshift, r_cue, r_cseq;
     uint64_t r_ncand = 0, r_pairs = 0, r_words = 0, r_elems = 0, r_batches = 0, r_launches = 0, r_spilled = 0;
+    uint64_t r_run_words = 0;
+    bool count_words = false;         // the alignment's statistics form (care_b200_count_word_compares)
     double pairs_per_anchor = 96.0;   // seen in the last correction call (automatic batch size)
     uint32_t r_first = 0, r_count = 0;
     bool r_valid = false;
@@ -565,25 +567,30 @@ struct AlignArgs {
     const unsigned long long* total; unsigned long long cap; const int* status; AlignRes* out;
     unsigned long long* words; const uint32_t* pair_order;
     const uint2* work; const unsigned int* work_n;
+    unsigned long long* run_words;             // non-null: the statistics form, counting words run
 };
 
-template <int B, int NW>
+template <int B, int NW, bool CNT>
 cudaError_t align_go(const AlignArgs& a, cudaStream_t st) {
     const unsigned long long blocks = (a.cap + B - 1) / B;
-    k_align<B, NW><<<(unsigned)blocks, B, 0, st>>>(a.o, a.r, a.first, a.cand_ids, a.cand_anchor, a.seg_off,
-                                                   a.seg_cnt, a.total, a.cap, a.status, a.out, a.words,
-                                                   a.pair_order, a.work, a.work_n);
+    k_align<B, NW, CNT><<<(unsigned)blocks, B, 0, st>>>(a.o, a.r, a.first, a.cand_ids, a.cand_anchor, a.seg_off,
+                                                        a.seg_cnt, a.total, a.cap, a.status, a.out, a.words,
+                                                        a.pair_order, a.work, a.work_n, a.run_words);
     return cudaGetLastError();
 }
 
 cudaError_t align_dispatch(int block, int nw, const AlignArgs& a, cudaStream_t st) {
-#define AL(B)                                       \
-    if (nw <= 4) return align_go<B, 4>(a, st);      \
-    if (nw <= 5) return align_go<B, 5>(a, st);      \
-    if (nw <= 6) return align_go<B, 6>(a, st);      \
-    return align_go<B, 8>(a, st);
-    if (block == 256) { AL(256) }
-    AL(128)
+#define AL(B, C)                                        \
+    if (nw <= 4) return align_go<B, 4, C>(a, st);       \
+    if (nw <= 5) return align_go<B, 5, C>(a, st);       \
+    if (nw <= 6) return align_go<B, 6, C>(a, st);       \
+    return align_go<B, 8, C>(a, st);
+    if (a.run_words) {
+        if (block == 256) { AL(256, true) }
+        AL(128, true)
+    }
+    if (block == 256) { AL(256, false) }
+    AL(128, false)
 #undef AL
 }
 
@@ -666,7 +673,7 @@ int run_batch(care_b200_ctx* ctx, uint32_t first, uint32_t count, bool timed) {
 
     CK(ctx->d_seg_off.ensure((size_t)count * 4), "alloc");
     CK(ctx->d_seg_cnt.ensure((size_t)count * 4), "alloc");
-    CK(ctx->d_counters.ensure(64), "alloc");
+    CK(ctx->d_counters.ensure(128), "alloc");
     CK(ctx->d_status.ensure(16), "alloc");
     CK(ctx->d_st.ensure(count), "alloc");
     CK(ctx->d_ned.ensure((size_t)count * 4), "alloc");
@@ -747,7 +754,8 @@ int run_batch(care_b200_ctx* ctx, uint32_t first, uint32_t count, bool timed) {
                      ctx->d_ares.as<AlignRes>(), counters + 3,
                      tu.pair_order ? ctx->d_pair_order.as<uint32_t>() : nullptr,
                      tu.pair_mirror ? ctx->d_pair_work.as<uint2>() : nullptr,
-                     reinterpret_cast<const unsigned int*>(counters + 6)};
+                     reinterpret_cast<const unsigned int*>(counters + 6),
+                     ctx->count_words ? counters + 8 : nullptr};
         MsaArgs ma{o, r, first, count, tu.msa_order ? ctx->d_order.as<uint32_t>() : nullptr,
                    reinterpret_cast<unsigned int*>(counters + 4), ctx->d_cand_ids.as<uint32_t>(),
                    ctx->d_seg_off.as<uint32_t>(), ctx->d_seg_cnt.as<uint32_t>(), ctx->d_ares.as<AlignRes>(),
@@ -766,7 +774,7 @@ int run_batch(care_b200_ctx* ctx, uint32_t first, uint32_t count, bool timed) {
         auto enqueue = [&]() -> int {
             launches = 0;
 #define EQ(call, where) do { const cudaError_t e_ = (call); if (e_ != cudaSuccess) return cuda_fail(ctx, e_, where); } while (0)
-            EQ(cudaMemsetAsync(counters, 0, 64, st), "memset");
+            EQ(cudaMemsetAsync(counters, 0, 128, st), "memset");
             EQ(cudaMemsetAsync(status, 0, 16, st), "memset");
             // rows of anchors that are not corrected read as zero bytes
             EQ(cudaMemsetAsync(ctx->d_oseq.p, 0, (size_t)count * ctx->max_len, st), "memset");
@@ -843,10 +851,10 @@ int run_batch(care_b200_ctx* ctx, uint32_t first, uint32_t count, bool timed) {
                 launches += 3;                   // inference, verdicts, recount
             }
             EQ(mark(4), "event");
-            EQ(cudaMemcpyAsync(ctx->h_small.p, counters, 64, cudaMemcpyDeviceToHost, st), "counters");
-            EQ(cudaMemcpyAsync(ctx->h_small.as<char>() + 64, status, 4, cudaMemcpyDeviceToHost, st), "status");
+            EQ(cudaMemcpyAsync(ctx->h_small.p, counters, 72, cudaMemcpyDeviceToHost, st), "counters");
+            EQ(cudaMemcpyAsync(ctx->h_small.as<char>() + 72, status, 4, cudaMemcpyDeviceToHost, st), "status");
             if (o.clf_mode == 2)
-                EQ(cudaMemcpyAsync(ctx->h_small.as<char>() + 68, ctx->d_mlp_err.p, 4, cudaMemcpyDeviceToHost, st), "status");
+                EQ(cudaMemcpyAsync(ctx->h_small.as<char>() + 76, ctx->d_mlp_err.p, 4, cudaMemcpyDeviceToHost, st), "status");
 #undef EQ
             return CARE_B200_OK;
         };
@@ -878,7 +886,8 @@ int run_batch(care_b200_ctx* ctx, uint32_t first, uint32_t count, bool timed) {
         const unsigned long long words = ctx->h_small.as<unsigned long long>()[3];
         const unsigned long long elems = ctx->h_small.as<unsigned long long>()[5];
         const unsigned int spilled = ctx->h_small.as<unsigned int>()[14];     // counters + 7
-        const int stw = *(int*)(ctx->h_small.as<char>() + 64);
+        const unsigned long long run_words = ctx->h_small.as<unsigned long long>()[8];
+        const int stw = *(int*)(ctx->h_small.as<char>() + 72);
         if (stw & kStatusColumns) return fail(ctx, CARE_B200_ELIMIT, "MSA wider than the kernel's column capacity");
         bool again = false;
         if ((stw & kStatusCandOverflow) || used > cap) {
@@ -891,7 +900,7 @@ int run_batch(care_b200_ctx* ctx, uint32_t first, uint32_t count, bool timed) {
         if ((stw & kStatusCorrOverflow) || corr > ccap) { ctx->corr_cap = corr + corr / 8 + 1024; again = true; }
         if (emit && ((stw & kStatusFeatOverflow) || nfeat > fcap)) { ctx->feat_cap = nfeat + nfeat / 8 + 4096; again = true; }
         if (again) continue;
-        if (o.clf_mode == 2 && *(int*)(ctx->h_small.as<char>() + 68))
+        if (o.clf_mode == 2 && *(int*)(ctx->h_small.as<char>() + 76))
             return fail(ctx, CARE_B200_ECUDA, "tensor-core completion wait ran out");
         if (timed) {
             float a = 0, b = 0, c = 0, d = 0;
@@ -921,6 +930,7 @@ int run_batch(care_b200_ctx* ctx, uint32_t first, uint32_t count, bool timed) {
         ctx->r_words += words;
         ctx->r_elems += elems;
         ctx->r_spilled += spilled;
+        ctx->r_run_words += run_words;
         return (int)std::min<unsigned long long>(corr, 0x7fffffff);
     }
     return fail(ctx, CARE_B200_ENOMEM, "arena growth did not converge");
@@ -976,6 +986,7 @@ int correct_impl(care_b200_ctx* ctx, uint32_t first, uint32_t count, care_b200_r
     ctx->r_batches = 0;
     ctx->r_launches = 0;
     ctx->r_spilled = 0;
+    ctx->r_run_words = 0;
     ctx->r_valid = false;
     const int L = ctx->max_len;
     if (copy) {
@@ -1056,6 +1067,12 @@ int care_b200_correct_range(care_b200_ctx* ctx, uint32_t first, uint32_t count, 
 
 int care_b200_correct_range_device(care_b200_ctx* ctx, uint32_t first, uint32_t count) {
     return correct_impl(ctx, first, count, nullptr, false);
+}
+
+int care_b200_count_word_compares(care_b200_ctx* ctx, int on) {
+    if (!ctx || (unsigned)on > 1) return CARE_B200_EINVAL;
+    ctx->count_words = on != 0;
+    return CARE_B200_OK;
 }
 
 int care_b200_default_tuning(care_b200_tuning* t) {
@@ -1207,9 +1224,9 @@ int care_b200_last_timing(const care_b200_ctx* ctx, float* total_ms, float* stag
 
 int care_b200_last_stats(const care_b200_ctx* ctx, uint64_t* stats, int nstats) {
     if (!ctx || !stats) return CARE_B200_EINVAL;
-    const uint64_t v[8] = {ctx->r_count, ctx->r_pairs, ctx->r_ncand, ctx->r_words, ctx->r_elems, ctx->r_batches,
-                           ctx->r_launches, ctx->r_spilled};
-    for (int i = 0; i < nstats && i < 8; i++) stats[i] = v[i];
+    const uint64_t v[9] = {ctx->r_count, ctx->r_pairs, ctx->r_ncand, ctx->r_words, ctx->r_elems, ctx->r_batches,
+                           ctx->r_launches, ctx->r_spilled, ctx->r_run_words};
+    for (int i = 0; i < nstats && i < 9; i++) stats[i] = v[i];
     return CARE_B200_OK;
 }
 

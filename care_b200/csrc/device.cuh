@@ -270,6 +270,11 @@ CB_HD uint32_t lead_mask(int valid) {
     return valid >= 32 ? 0xFFFFFFFFu : (valid <= 0 ? 0u : ~(0xFFFFFFFFu >> valid));
 }
 
+// Word compares a scan runs (statistics only): WordCount counts them,
+// NoCount compiles to nothing.
+struct NoCount { CB_HD void add(int) {} };
+struct WordCount { int n = 0; CB_HD void add(int k) { n += k; } };
+
 // One scan direction of the shifted Hamming distance. The "shifted" planes S
 // slide by t = t0..t1 bases against the "other" planes O, in the reference's
 // order and with its pruning (src/cpu_alignment.cpp:247-316):
@@ -280,11 +285,12 @@ CB_HD uint32_t lead_mask(int valid) {
 // per plane); further words are only read while the count stays below the
 // limit, which decides the same comparisons as the reference's early exit.
 // mextab[ov] holds int(float(ov) * maxErrorRate).
-template <int NW>
+template <int NW, class Cnt = NoCount>
 CB_HD void shd_scan(uint32_t (&Sh)[NW + 2], uint32_t (&Sl)[NW + 2],
                                          const uint32_t (&Oh)[NW + 2], const uint32_t (&Ol)[NW + 2],
                                          int t0, int t1, int sign, int La, int Lc, int total,
-                                         const int* __restrict__ mextab, int& best, int& bestShift) {
+                                         const int* __restrict__ mextab, int& best, int& bestShift,
+                                         Cnt* cnt = nullptr) {
     if (t1 < t0) return;
     bool stop = false;
 #pragma unroll 1
@@ -301,6 +307,7 @@ CB_HD void shd_scan(uint32_t (&Sh)[NW + 2], uint32_t (&Sl)[NW + 2],
             uint32_t d1 = (funnel_l(Sh[2], Sh[1], r) ^ Oh[1]) | (funnel_l(Sl[2], Sl[1], r) ^ Ol[1]);
             if (ov < 64) { d0 &= lead_mask(ov); d1 &= lead_mask(ov - 32); }
             int mm = popc32(d0) + popc32(d1);
+            if (cnt) cnt->add(2);
             if (mm < mex && ov > 64) {
 #pragma unroll
                 for (int j = 2; j < NW; ++j) {
@@ -309,6 +316,7 @@ CB_HD void shd_scan(uint32_t (&Sh)[NW + 2], uint32_t (&Sl)[NW + 2],
                                       (funnel_l(Sl[j + 1], Sl[j], r) ^ Ol[j]);
                         dj &= lead_mask(ov - 32 * j);
                         mm += popc32(dj);
+                        if (cnt) cnt->add(1);
                     }
                 }
             }
@@ -334,11 +342,12 @@ CB_HD void shd_scan(uint32_t (&Sh)[NW + 2], uint32_t (&Sl)[NW + 2],
 // (limit best - total + 2*ov + 1, direction ended only when no later shift
 // can reach the best) and records the first minimal shift of each order.
 // Shift s < 0 has rank -s in the (C, A) order, s > 0 rank (L-minov) + s.
-template <int NW>
+template <int NW, class Cnt = NoCount>
 CB_HD void shd_scan_ties(uint32_t (&Sh)[NW + 2], uint32_t (&Sl)[NW + 2],
                          const uint32_t (&Oh)[NW + 2], const uint32_t (&Ol)[NW + 2],
                          int t0, int t1, int sign, int L, int negs, int total,
-                         const int* __restrict__ mextab, int& best, int& shiftA, int& shiftB) {
+                         const int* __restrict__ mextab, int& best, int& shiftA, int& shiftB,
+                         Cnt* cnt = nullptr) {
     if (t1 < t0) return;
     bool stop = false;
 #pragma unroll 1
@@ -355,6 +364,7 @@ CB_HD void shd_scan_ties(uint32_t (&Sh)[NW + 2], uint32_t (&Sl)[NW + 2],
             uint32_t d1 = (funnel_l(Sh[2], Sh[1], r) ^ Oh[1]) | (funnel_l(Sl[2], Sl[1], r) ^ Ol[1]);
             if (ov < 64) { d0 &= lead_mask(ov); d1 &= lead_mask(ov - 32); }
             int mm = popc32(d0) + popc32(d1);
+            if (cnt) cnt->add(2);
             if (mm < mex && ov > 64) {
 #pragma unroll
                 for (int j = 2; j < NW; ++j) {
@@ -363,6 +373,7 @@ CB_HD void shd_scan_ties(uint32_t (&Sh)[NW + 2], uint32_t (&Sl)[NW + 2],
                                       (funnel_l(Sl[j + 1], Sl[j], r) ^ Ol[j]);
                         dj &= lead_mask(ov - 32 * j);
                         mm += popc32(dj);
+                        if (cnt) cnt->add(1);
                     }
                 }
             }
@@ -383,10 +394,11 @@ CB_HD void shd_scan_ties(uint32_t (&Sh)[NW + 2], uint32_t (&Sl)[NW + 2],
 }
 
 // Forward alignments of (A, C) and (C, A) for reads of equal length L.
-template <int NW>
+template <int NW, class Cnt = NoCount>
 CB_HD void shifted_hamming_pair(const uint32_t (&Ah)[NW + 2], const uint32_t (&Al)[NW + 2],
                                 const uint32_t (&Ch)[NW + 2], const uint32_t (&Cl)[NW + 2], int L, int minov,
-                                const int* __restrict__ mextab, ShdResult& ac, ShdResult& ca) {
+                                const int* __restrict__ mextab, ShdResult& ac, ShdResult& ca,
+                                Cnt* cnt = nullptr) {
     const int total = 2 * L;
     int best = total, shiftA = -L, shiftB = -L;
     uint32_t Sh[NW + 2], Sl[NW + 2];
@@ -394,8 +406,10 @@ CB_HD void shifted_hamming_pair(const uint32_t (&Ah)[NW + 2], const uint32_t (&A
     for (int dir = 0; dir < 2; ++dir) {
 #pragma unroll
         for (int j = 0; j < NW + 2; ++j) { Sh[j] = dir ? Ch[j] : Ah[j]; Sl[j] = dir ? Cl[j] : Al[j]; }
-        if (dir == 0) shd_scan_ties<NW>(Sh, Sl, Ch, Cl, 0, L - minov, +1, L, L - minov, total, mextab, best, shiftA, shiftB);
-        else shd_scan_ties<NW>(Sh, Sl, Ah, Al, 1, L - minov, -1, L, L - minov, total, mextab, best, shiftA, shiftB);
+        if (dir == 0)
+            shd_scan_ties<NW>(Sh, Sl, Ch, Cl, 0, L - minov, +1, L, L - minov, total, mextab, best, shiftA, shiftB, cnt);
+        else
+            shd_scan_ties<NW>(Sh, Sl, Ah, Al, 1, L - minov, -1, L, L - minov, total, mextab, best, shiftA, shiftB, cnt);
     }
     auto fill = [&](ShdResult& res, int shift) {
         res.valid = shift != -L;
@@ -443,11 +457,11 @@ CB_HD int unpruned_words(int La, int Lc, int minov) {
 // cpuShiftedHammingDistancePopcount2BitHiLo (src/cpu_alignment.cpp:32-323):
 // shifts 0..La-minov (anchor slid against the candidate), then -1..-(Lc-minov)
 // (candidate slid against the anchor).
-template <int NW>
+template <int NW, class Cnt = NoCount>
 CB_HD ShdResult shifted_hamming(const uint32_t (&Ah)[NW + 2], const uint32_t (&Al)[NW + 2],
                                                      int La, const uint32_t (&Ch)[NW + 2],
                                                      const uint32_t (&Cl)[NW + 2], int Lc, int minov,
-                                                     const int* __restrict__ mextab) {
+                                                     const int* __restrict__ mextab, Cnt* cnt = nullptr) {
     const int total = La + Lc;
     int best = total, bestShift = -Lc;
     uint32_t Sh[NW + 2], Sl[NW + 2];
@@ -455,8 +469,8 @@ CB_HD ShdResult shifted_hamming(const uint32_t (&Ah)[NW + 2], const uint32_t (&A
     for (int dir = 0; dir < 2; ++dir) {
 #pragma unroll
         for (int j = 0; j < NW + 2; ++j) { Sh[j] = dir ? Ch[j] : Ah[j]; Sl[j] = dir ? Cl[j] : Al[j]; }
-        if (dir == 0) shd_scan<NW>(Sh, Sl, Ch, Cl, 0, La - minov, +1, La, Lc, total, mextab, best, bestShift);
-        else shd_scan<NW>(Sh, Sl, Ah, Al, 1, Lc - minov, -1, La, Lc, total, mextab, best, bestShift);
+        if (dir == 0) shd_scan<NW>(Sh, Sl, Ch, Cl, 0, La - minov, +1, La, Lc, total, mextab, best, bestShift, cnt);
+        else shd_scan<NW>(Sh, Sl, Ah, Al, 1, Lc - minov, -1, La, Lc, total, mextab, best, bestShift, cnt);
     }
     ShdResult res;
     res.valid = bestShift != -Lc;

@@ -7,6 +7,7 @@
 //   k_msa        : alignment filters, MSA build/refine, consensus
 //                  correction of anchor and candidates (one CTA per anchor)
 #pragma once
+#include <type_traits>
 #include "device.cuh"
 
 namespace careb200 {
@@ -371,14 +372,19 @@ __device__ __forceinline__ uint8_t mate_flag(const uint32_t* __restrict__ cand_i
     return (lo2 < mcnt && cand_ids[moff + lo2] == target) ? 1 : 0;
 }
 
-template <int BLOCK, int NW>
+// CNT: the statistics form, which also adds the 32-bit word compares its
+// scans actually run (after the early exits) to run_count.
+template <int BLOCK, int NW, bool CNT = false>
 __global__ void __launch_bounds__(BLOCK)
 k_align(DevOptions o, DevReads r, uint32_t first, const uint32_t* __restrict__ cand_ids,
         const uint32_t* __restrict__ cand_anchor, const uint32_t* __restrict__ seg_off,
         const uint32_t* __restrict__ seg_cnt, const unsigned long long* __restrict__ total_ptr,
         unsigned long long arena_cap, const int* __restrict__ status, AlignRes* __restrict__ out,
         unsigned long long* __restrict__ work_count, const uint32_t* __restrict__ pair_order,
-        const uint2* __restrict__ work, const unsigned int* __restrict__ work_n) {
+        const uint2* __restrict__ work, const unsigned int* __restrict__ work_n,
+        unsigned long long* __restrict__ run_count) {
+    using Cnt = typename std::conditional<CNT, WordCount, NoCount>::type;
+    Cnt wc;
     __shared__ int s_mex[kMaxLen + 1];
     // int(float(ov) * maxErrorRate), the first term of max_errors_excl
     for (int i = threadIdx.x; i <= kMaxLen; i += BLOCK) s_mex[i] = __float2int_rz(__fmul_rn((float)i, o.max_error_rate));
@@ -415,11 +421,16 @@ k_align(DevOptions o, DevReads r, uint32_t first, const uint32_t* __restrict__ c
         if ((int)(threadIdx.x & 31) == __ffs(m) - 1) atomicAdd(work_count, (unsigned long long)ws);
     }
     ShdResult f, g;                   // g: forward alignment of the mirror pair (c, a)
-    if (j != kNoMirror) shifted_hamming_pair<NW>(Ah, Al, Ch, Cl, La, minov, s_mex, f, g);
-    else f = shifted_hamming<NW>(Ah, Al, La, Ch, Cl, Lc, minov, s_mex);
+    if (j != kNoMirror) shifted_hamming_pair<NW, Cnt>(Ah, Al, Ch, Cl, La, minov, s_mex, f, g, &wc);
+    else f = shifted_hamming<NW, Cnt>(Ah, Al, La, Ch, Cl, Lc, minov, s_mex, &wc);
     uint32_t Rh[NW + 2], Rl[NW + 2];
     revcomp_planes<NW>(Ch, Cl, Lc, Rh, Rl);
-    const ShdResult rc = shifted_hamming<NW>(Ah, Al, La, Rh, Rl, Lc, minov, s_mex);
+    const ShdResult rc = shifted_hamming<NW, Cnt>(Ah, Al, La, Rh, Rl, Lc, minov, s_mex, &wc);
+    if constexpr (CNT) {
+        const unsigned m = __activemask();
+        const unsigned ws = __reduce_add_sync(m, (unsigned)wc.n);
+        if ((int)(threadIdx.x & 31) == __ffs(m) - 1) atomicAdd(run_count, (unsigned long long)ws);
+    }
     const float ler = __fmul_rn(o.estimated_errorrate, 4.0f);
     auto result = [&](const ShdResult& fw, uint32_t anchor_index, uint32_t cand) {
         const int orient = choose_orientation(fw, rc, La, o.min_overlap_ratio, o.min_overlap, ler);

@@ -154,7 +154,7 @@ extern "C" int care_b200_correct_range_noalloc(const care_b200_options* opt, con
     const int nw = (r.max_len + 31) / 32;
 #define LAUNCH_ALIGN(NW)                                                                                    \
     k_align<128, NW><<<ablocks, 128, 0, st>>>(o, r, first_anchor, cand_ids, cand_anchor, seg_off, seg_cnt,  \
-                                              counters, kNoAllocMaxPairs, dstatus, ares, nullptr, nullptr, nullptr, nullptr)
+                                              counters, kNoAllocMaxPairs, dstatus, ares, nullptr, nullptr, nullptr, nullptr, nullptr)
     if (nw <= 4) LAUNCH_ALIGN(4);
     else if (nw <= 5) LAUNCH_ALIGN(5);
     else if (nw <= 6) LAUNCH_ALIGN(6);

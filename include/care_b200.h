@@ -167,8 +167,16 @@ int care_b200_last_timing(const care_b200_ctx* ctx, float* total_ms, float* stag
  * build including refinement rebuilds: the MSA stage's compute work),
  * stats[5] device batches the range was split into, stats[6] kernels of
  * this library launched (every batch and every arena-growth attempt),
- * stats[7] anchors whose candidate lists took the second, full-set pass. */
+ * stats[7] anchors whose candidate lists took the second, full-set pass,
+ * stats[8] 32-bit word compares the alignment scans actually ran after their
+ * early exits (counted only while care_b200_count_word_compares is on, else 0). */
 int care_b200_last_stats(const care_b200_ctx* ctx, uint64_t* stats, int nstats);
+
+/* on = 1: the following correction calls run the alignment's statistics form,
+ * which also counts the word compares its scans run (stats[8]; the reference's
+ * early exit, src/cpu_alignment.cpp:82-98, is what makes this count smaller than
+ * stats[3]). Slower; results unchanged. on = 0 (default) turns it off. */
+int care_b200_count_word_compares(care_b200_ctx* ctx, int on);
 
 /* ---- correction without allocation ---- */
 

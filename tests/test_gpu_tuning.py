@@ -186,3 +186,24 @@ def test_autotuner_on_a_sample(uneven):
     assert set(best) == set(autotune.DEFAULT)
     assert info["best_ms"] <= info["default_ms"]
     assert len(info["measured"]) >= 1 + sum(len(v) - 1 for v in autotune.KNOBS.values())
+
+
+def test_counted_word_compares(uneven):
+    """The alignment's statistics form changes no result and counts between
+    one and all of the un-pruned word compares of the same scans."""
+    rs, inp, d = uneven
+    with care_b200.Corrector(care_b200.options_from_args(UNEVEN_ARGS)) as c:
+        c.load_files([inp])
+        c.build_tables()
+        base = c.correct_range()
+        st0 = c.last_stats()
+        c.count_word_compares(True)
+        counted = c.correct_range()
+        st1 = c.last_stats()
+        c.count_word_compares(False)
+        c.correct_range()
+        st2 = c.last_stats()
+    _same(base, counted)
+    assert st0["word_compares_run"] == 0 and st2["word_compares_run"] == 0
+    assert st1["word_compares"] == st0["word_compares"]
+    assert 0 < st1["word_compares_run"] < st1["word_compares"]
