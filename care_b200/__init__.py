@@ -74,7 +74,8 @@ EXPORTS = [
     "care_b200_build_tables", "care_b200_get_table", "care_b200_correct_range",
     "care_b200_correct_range_device", "care_b200_serialize_results",
     "care_b200_load_reads_from_files", "care_b200_write_output", "care_b200_last_timing",
-    "care_b200_last_stats", "care_b200_count_word_compares", "care_b200_num_reads", "care_b200_max_length", "care_b200_num_maps",
+    "care_b200_last_stats", "care_b200_count_word_compares", "care_b200_load_preprocessed_reads",
+    "care_b200_save_preprocessed_reads", "care_b200_num_reads", "care_b200_max_length", "care_b200_num_maps",
     "care_b200_correct_range_noalloc",
     "care_b200_set_mlp", "care_b200_collect_features", "care_b200_mlp_default_train_options",
     "care_b200_mlp_create", "care_b200_mlp_destroy", "care_b200_mlp_last_error", "care_b200_mlp_set_params",
@@ -175,6 +176,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.care_b200_last_timing.argtypes = [c_ctx, P(ctypes.c_float), P(ctypes.c_float), ctypes.c_int]
     lib.care_b200_last_stats.argtypes = [c_ctx, P(ctypes.c_uint64), ctypes.c_int]
     lib.care_b200_count_word_compares.argtypes = [c_ctx, ctypes.c_int]
+    lib.care_b200_load_preprocessed_reads.argtypes = [c_ctx, ctypes.c_char_p]
+    lib.care_b200_save_preprocessed_reads.argtypes = [c_ctx, ctypes.c_char_p]
     lib.care_b200_correct_range_noalloc.argtypes = [P(Options), P(DeviceReads), P(DeviceTables), ctypes.c_uint32,
                                                      ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p,
                                                      ctypes.c_void_p, ctypes.c_void_p]
@@ -288,6 +291,15 @@ class Corrector:
     def load_files(self, files: Sequence[str]):
         arr = (ctypes.c_char_p * len(files))(*[f.encode() for f in files])
         self._check(self.lib.care_b200_load_reads_from_files(self._ctx, arr, len(files)), "load_reads_from_files")
+
+    def load_preprocessed_reads(self, path: str):
+        """Read storage from a file written by care-cpu --save-preprocessedreads-to
+        (or by save_preprocessed_reads), in place of parsing FASTQ."""
+        self._check(self.lib.care_b200_load_preprocessed_reads(self._ctx, path.encode()), "load_preprocessed_reads")
+
+    def save_preprocessed_reads(self, path: str):
+        """The uploaded read storage in care-cpu's binary read-storage layout."""
+        self._check(self.lib.care_b200_save_preprocessed_reads(self._ctx, path.encode()), "save_preprocessed_reads")
 
     def build_tables(self):
         self._check(self.lib.care_b200_build_tables(self._ctx), "build_tables")

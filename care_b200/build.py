@@ -28,7 +28,7 @@ NVFLAGS = ARCH + ["-O3", "-lineinfo", "--fmad=false", "-std=c++17", "-Xcompiler"
 CXXFLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-Wall", "-Wextra"]
 
 CU_SOURCES = ["capi.cu", "noalloc.cu", "mlp.cu", "tables.cu"]
-CXX_SOURCES = ["hostio.cpp"]
+CXX_SOURCES = ["hostio.cpp", "readfile.cpp"]
 
 
 def nvcc() -> str:

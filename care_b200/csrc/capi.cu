@@ -2,6 +2,7 @@
 // storage and minhash tables, the batched correction pipeline, results.
 #include "../../include/care_b200.h"
 #include "hostio.hpp"
+#include "readfile.hpp"
 #include "kernels.cuh"
 #include "mlp.hpp"
 #include "tables.hpp"
@@ -1193,6 +1194,54 @@ int care_b200_load_reads_from_files(care_b200_ctx* ctx, const char* const* files
     return care_b200_upload_reads(ctx, h.seq.data(), h.seq_pitch, h.len.data(),
                                   h.has_quality ? h.qual.data() : nullptr, h.qual_pitch,
                                   h.ambiguous_ids.data(), h.ambiguous_ids.size(), h.n);
+}
+
+int care_b200_load_preprocessed_reads(care_b200_ctx* ctx, const char* path) {
+    if (!ctx || !path) return CARE_B200_EINVAL;
+    ReadStorageFile f;
+    const std::string e = read_storage_file(path, f);
+    if (!e.empty()) return fail(ctx, CARE_B200_EIO, e);
+    const bool useq = ctx->opt.use_quality != 0;
+    if (useq && !f.has_quality)
+        return fail(ctx, CARE_B200_EINVAL, "quality scores expected in the read-storage file, but none are present");
+    if (useq && f.quality_bits != ctx->opt.quality_bits)
+        return fail(ctx, CARE_B200_EINVAL, "the read-storage file uses " + std::to_string(f.quality_bits) +
+                                               " bits per quality score, the options " +
+                                               std::to_string(ctx->opt.quality_bits));
+    // output records of an earlier care_b200_load_reads_from_files stay in
+    // use for the same reads (care-cpu writes its output from the input files)
+    ctx->have_records = ctx->have_records && ctx->reads.n == f.n;
+    return care_b200_upload_reads(ctx, f.seq.data(), f.seq_pitch, f.len.data(),
+                                  useq ? f.qual.data() : nullptr, f.qual_pitch, f.ambiguous_ids.data(),
+                                  f.ambiguous_ids.size(), (uint32_t)f.n);
+}
+
+int care_b200_save_preprocessed_reads(care_b200_ctx* ctx, const char* path) {
+    if (!ctx || !path) return CARE_B200_EINVAL;
+    if (ctx->n == 0) return fail(ctx, CARE_B200_ESTATE, "no reads uploaded");
+    CK(cudaSetDevice(ctx->opt.device), "cudaSetDevice");
+    ReadStorageFile f;
+    f.n = ctx->n;
+    f.has_quality = ctx->has_qual;
+    f.quality_bits = ctx->opt.quality_bits;
+    f.seq_pitch = (uint64_t)ctx->seq_pitch;
+    f.qual_pitch = ctx->has_qual ? (uint64_t)ctx->qual_pitch : 0;
+    f.seq.resize(f.n * f.seq_pitch);
+    f.len.resize(f.n);
+    CK(cudaStreamSynchronize(ctx->stream), "sync");
+    CK(cudaMemcpy(f.seq.data(), ctx->d_seq.p, f.seq.size() * 4, cudaMemcpyDeviceToHost), "download sequences");
+    CK(cudaMemcpy(f.len.data(), ctx->d_len.p, f.len.size() * 4, cudaMemcpyDeviceToHost), "download lengths");
+    if (f.has_quality) {
+        f.qual.resize(f.n * f.qual_pitch);
+        CK(cudaMemcpy(f.qual.data(), ctx->d_qual.p, f.qual.size() * 4, cudaMemcpyDeviceToHost), "download qualities");
+    }
+    f.min_len = *std::min_element(f.len.begin(), f.len.end());
+    f.max_len = *std::max_element(f.len.begin(), f.len.end());
+    for (uint32_t i = 0; i < ctx->n; ++i)
+        if (ctx->h_ambig[i]) f.ambiguous_ids.push_back(i);
+    const std::string e = write_storage_file(path, f);
+    if (!e.empty()) return fail(ctx, CARE_B200_EIO, e);
+    return CARE_B200_OK;
 }
 
 int care_b200_write_output(care_b200_ctx* ctx, const char* outfile) {

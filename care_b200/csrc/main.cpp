@@ -27,7 +27,8 @@ void usage() {
         "  --minalignmentoverlap N      --maxmismatchratio F     --minalignmentoverlapratio F\n"
         "  --errorfactortuning F        --coveragefactortuning F --pairedFilterThreshold F\n"
         "  --correctionQualityLabels    --batchsize N            -g,--gpu N\n"
-        "  --correctionType 0|1 (1: learned decision)  --ml-mlpfile FILE  --clfMinCoverage N");
+        "  --correctionType 0|1 (1: learned decision)  --ml-mlpfile FILE  --clfMinCoverage N\n"
+        "  --save-preprocessedreads-to FILE  --load-preprocessedreads-from FILE");
 }
 
 bool flag_value(int& i, int argc, char** argv) {
@@ -44,7 +45,7 @@ int main(int argc, char** argv) {
     care_b200_options o;
     care_b200_default_options(&o);
     std::vector<std::string> inputs;
-    std::string outdir, outname, mlpfile;
+    std::string outdir, outname, mlpfile, save_reads, load_reads;
     bool haveCov = false, havePair = false;
     for (int i = 1; i < argc; i++) {
         const std::string a = argv[i];
@@ -90,6 +91,8 @@ int main(int argc, char** argv) {
         else if (a == "--correctionType") o.correction_type = std::atoi(val()) == 1 ? 1 : 0;
         else if (a == "--ml-mlpfile") mlpfile = val();
         else if (a == "--clfMinCoverage") o.clf_min_coverage = std::atoi(val());
+        else if (a == "--save-preprocessedreads-to") save_reads = val();
+        else if (a == "--load-preprocessedreads-from") load_reads = val();
         else if (a == "--help") { usage(); return 0; }
         else { std::fprintf(stderr, "unknown option %s\n", a.c_str()); usage(); return 1; }
     }
@@ -124,6 +127,15 @@ int main(int argc, char** argv) {
     std::vector<const char*> fp;
     for (auto& s : inputs) fp.push_back(s.c_str());
     if (care_b200_load_reads_from_files(ctx, fp.data(), (int)fp.size())) return die("reading input");
+    // as care-cpu: the read storage from the saved file, the output records
+    // from the input files (constructChunkedReadStorageFromFiles,
+    // include/chunkedreadstorageconstruction.hpp:35-42)
+    if (!load_reads.empty() && care_b200_load_preprocessed_reads(ctx, load_reads.c_str()))
+        return die("loading the saved read storage");
+    if (!save_reads.empty()) {
+        std::printf("Saving reads to file %s\n", save_reads.c_str());
+        if (care_b200_save_preprocessed_reads(ctx, save_reads.c_str())) return die("saving the read storage");
+    }
     if (care_b200_build_tables(ctx)) return die("building hash tables");
     const double t1 = now();
     std::printf("Total number of reads: %u\nMaximum sequence length: %d\nUsing %d maps\n",

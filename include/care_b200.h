@@ -150,6 +150,22 @@ int care_b200_serialize_results(care_b200_ctx* ctx, const care_b200_results* res
  * and uploads the read storage. */
 int care_b200_load_reads_from_files(care_b200_ctx* ctx, const char* const* files, int num_files);
 
+/* Read-storage handle, binary file: uploads the read storage that care-cpu
+ * saved with --save-preprocessedreads-to (ChunkedReadStorage::loadFromFile,
+ * include/chunkedreadstorage.hpp:160-243), in place of parsing FASTQ. As in the
+ * reference, a file whose quality bits differ from the options, or without
+ * qualities when the options use them, is rejected; qualities the options do
+ * not use are skipped. The file holds no input records: output records from
+ * an earlier care_b200_load_reads_from_files of the same reads stay in use for
+ * care_b200_write_output (care-cpu, too, writes its output from the input
+ * files); otherwise use care_b200_serialize_results. */
+int care_b200_load_preprocessed_reads(care_b200_ctx* ctx, const char* path);
+
+/* Writes the uploaded read storage in the same layout
+ * (ChunkedReadStorage::saveToFile, include/chunkedreadstorage.hpp:246-398);
+ * ambiguous read ids in ascending order. */
+int care_b200_save_preprocessed_reads(care_b200_ctx* ctx, const char* path);
+
 /* Merges all corrections of the last full-range call with the input reads
  * and writes the output file (correctionresultoutput.cpp:30-440, 730-1020). */
 int care_b200_write_output(care_b200_ctx* ctx, const char* outfile);

@@ -1,0 +1,139 @@
+"""care-cpu's binary read-storage file (--save-preprocessedreads-to), without a
+GPU: the files the reference wrote for two seeded read sets
+(tests/golden/make_preprocessed.py) hold exactly the read storage this
+library's own preprocessing builds from the same FASTQ, and the writer
+reproduces the reference's bytes (the ambiguous ids, which the reference
+writes in the order of a hash set, as a set)."""
+import ctypes
+import gzip
+import os
+import struct
+import subprocess
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GOLD = os.path.join(ROOT, "tests", "golden")
+SRC = [os.path.join(ROOT, "tests", "harness", "readfile_harness.cpp"),
+       os.path.join(ROOT, "care_b200", "csrc", "readfile.cpp"),
+       os.path.join(ROOT, "care_b200", "csrc", "hostio.cpp")]
+DEPS = SRC + [os.path.join(ROOT, "care_b200", "csrc", f) for f in ("readfile.hpp", "hostio.hpp")]
+OUT = os.path.join(ROOT, "tests", "_build", "libreadfile.so")
+CASES = {"pre_pe": (True, 2), "pre_un": (False, 8)}      # paired end, quality bits
+U64 = ctypes.c_ulonglong
+
+
+def harness():
+    os.makedirs(os.path.dirname(OUT), exist_ok=True)
+    if not os.path.exists(OUT) or any(os.path.getmtime(d) > os.path.getmtime(OUT) for d in DEPS):
+        tmp = f"{OUT}.{os.getpid()}.tmp"
+        subprocess.run(["g++", "-shared", "-fPIC", "-O2", "-std=c++17", "-o", tmp] + SRC + ["-lpthread"],
+                       check=True, capture_output=True)
+        os.replace(tmp, OUT)
+    lib = ctypes.CDLL(OUT)
+    lib.rf_load.restype = ctypes.c_void_p
+    lib.rf_load.argtypes = [ctypes.c_char_p, ctypes.POINTER(U64), ctypes.c_char_p, ctypes.c_int]
+    lib.rf_parse.restype = ctypes.c_void_p
+    lib.rf_parse.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(U64), ctypes.c_char_p,
+                             ctypes.c_int]
+    for f in (lib.rf_arrays, lib.rf_parse_arrays):
+        f.argtypes = [ctypes.c_void_p] + [ctypes.c_void_p] * 4
+    lib.rf_free.argtypes = lib.rf_parse_free.argtypes = [ctypes.c_void_p]
+    lib.rf_write.argtypes = [ctypes.c_char_p, U64, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, U64, U64,
+                             ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, U64, ctypes.c_char_p,
+                             ctypes.c_int]
+    return lib
+
+
+H = harness()
+
+
+def unpack(tmp, name):
+    out = {}
+    for ext in ("fq", "bin"):
+        p = os.path.join(tmp, f"{name}.{ext}")
+        with open(p, "wb") as f:
+            f.write(gzip.decompress(open(os.path.join(GOLD, f"{name}.{ext}.gz"), "rb").read()))
+        out[ext] = p
+    return out
+
+
+def storage(handle_fn, arrays_fn, free_fn, *args):
+    info = (U64 * 8)()
+    err = ctypes.create_string_buffer(256)
+    h = handle_fn(*args, info, err, 256)
+    assert h, err.value.decode()
+    n, mn, mx, hasq, qbits, sp, qp, na = list(info)
+    seq = np.zeros(n * sp, np.uint32)
+    ln = np.zeros(n, np.int32)
+    qual = np.zeros(max(n * qp, 1), np.uint32)
+    amb = np.zeros(max(na, 1), np.uint32)
+    arrays_fn(h, seq.ctypes.data, ln.ctypes.data, qual.ctypes.data, amb.ctypes.data)
+    free_fn(h)
+    return dict(n=n, min=mn, max=mx, hasq=hasq, qbits=qbits, sp=sp, qp=qp, seq=seq, len=ln,
+                qual=qual[:n * qp], amb=amb[:na])
+
+
+def load(path):
+    return storage(H.rf_load, H.rf_arrays, H.rf_free, path.encode())
+
+
+def section_end(path):
+    """Offset where the ambiguous-id section starts."""
+    b = open(path, "rb").read()
+    lb, sb, qb, ab = struct.unpack_from("<4Q", b, 21)
+    return 53 + lb + sb + qb, b
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_reference_file_holds_our_preprocessing(tmp_path, name):
+    pe, qbits = CASES[name]
+    p = unpack(str(tmp_path), name)
+    ref = load(p["bin"])
+    ours = storage(H.rf_parse, H.rf_parse_arrays, H.rf_parse_free, p["fq"].encode(), int(pe), qbits)
+    for k in ("n", "min", "max", "sp", "qp", "qbits"):
+        assert ref[k] == ours[k], k
+    assert ref["hasq"] == 1
+    assert np.array_equal(ref["len"], ours["len"])
+    assert np.array_equal(ref["seq"], ours["seq"])
+    assert np.array_equal(ref["qual"], ours["qual"])
+    assert sorted(ref["amb"].tolist()) == sorted(ours["amb"].tolist())
+    if name == "pre_pe":
+        assert len(ref["amb"]) > 0                   # reads with N bases
+    else:
+        assert ref["min"] < ref["max"]               # bit-packed lengths
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_writer_reproduces_reference_bytes(tmp_path, name):
+    p = unpack(str(tmp_path), name)
+    ref = load(p["bin"])
+    amb = np.sort(ref["amb"])
+    out = str(tmp_path / "ours.bin")
+    err = ctypes.create_string_buffer(256)
+    rc = H.rf_write(out.encode(), ref["n"], ref["min"], ref["max"], ref["hasq"], ref["qbits"], ref["sp"], ref["qp"],
+                    ref["seq"].ctypes.data, ref["len"].ctypes.data, ref["qual"].ctypes.data, amb.ctypes.data,
+                    len(amb), err, 256)
+    assert rc == 0, err.value.decode()
+    end_ref, b_ref = section_end(p["bin"])
+    end_out, b_out = section_end(out)
+    assert end_ref == end_out and b_ref[:end_ref] == b_out[:end_out]
+    assert len(b_ref) == len(b_out)
+    ids = lambda b, e: sorted(struct.unpack_from(f"<{struct.unpack_from('<Q', b, e)[0]}I", b, e + 8))
+    assert ids(b_ref, end_ref) == ids(b_out, end_out)
+    back = load(out)
+    for k in ("seq", "len", "qual"):
+        assert np.array_equal(back[k], ref[k])
+
+
+def test_truncated_file_is_rejected(tmp_path):
+    p = unpack(str(tmp_path), "pre_un")
+    b = open(p["bin"], "rb").read()
+    for cut in (10, 60, len(b) // 2, len(b) - 3):
+        q = tmp_path / f"cut{cut}.bin"
+        q.write_bytes(b[:cut])
+        info = (U64 * 8)()
+        err = ctypes.create_string_buffer(256)
+        assert not H.rf_load(str(q).encode(), info, err, 256)
+        assert b"truncated" in err.value or b"inconsistent" in err.value
