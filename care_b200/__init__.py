@@ -75,7 +75,7 @@ EXPORTS = [
     "care_b200_correct_range_device", "care_b200_serialize_results",
     "care_b200_load_reads_from_files", "care_b200_write_output", "care_b200_last_timing",
     "care_b200_last_stats", "care_b200_count_word_compares", "care_b200_load_preprocessed_reads",
-    "care_b200_save_preprocessed_reads", "care_b200_num_reads", "care_b200_max_length", "care_b200_num_maps",
+    "care_b200_save_preprocessed_reads", "care_b200_load_hashtables", "care_b200_save_hashtables", "care_b200_num_reads", "care_b200_max_length", "care_b200_num_maps",
     "care_b200_correct_range_noalloc",
     "care_b200_set_mlp", "care_b200_collect_features", "care_b200_mlp_default_train_options",
     "care_b200_mlp_create", "care_b200_mlp_destroy", "care_b200_mlp_last_error", "care_b200_mlp_set_params",
@@ -178,6 +178,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.care_b200_count_word_compares.argtypes = [c_ctx, ctypes.c_int]
     lib.care_b200_load_preprocessed_reads.argtypes = [c_ctx, ctypes.c_char_p]
     lib.care_b200_save_preprocessed_reads.argtypes = [c_ctx, ctypes.c_char_p]
+    lib.care_b200_load_hashtables.argtypes = [c_ctx, ctypes.c_char_p]
+    lib.care_b200_save_hashtables.argtypes = [c_ctx, ctypes.c_char_p]
     lib.care_b200_correct_range_noalloc.argtypes = [P(Options), P(DeviceReads), P(DeviceTables), ctypes.c_uint32,
                                                      ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p,
                                                      ctypes.c_void_p, ctypes.c_void_p]
@@ -300,6 +302,15 @@ class Corrector:
     def save_preprocessed_reads(self, path: str):
         """The uploaded read storage in care-cpu's binary read-storage layout."""
         self._check(self.lib.care_b200_save_preprocessed_reads(self._ctx, path.encode()), "save_preprocessed_reads")
+
+    def load_hashtables(self, path: str):
+        """Tables from a file written by care-cpu --save-hashtables-to (or by
+        save_hashtables), in place of build_tables."""
+        self._check(self.lib.care_b200_load_hashtables(self._ctx, path.encode()), "load_hashtables")
+
+    def save_hashtables(self, path: str):
+        """The tables in care-cpu's minhash-table layout."""
+        self._check(self.lib.care_b200_save_hashtables(self._ctx, path.encode()), "save_hashtables")
 
     def build_tables(self):
         self._check(self.lib.care_b200_build_tables(self._ctx), "build_tables")

@@ -1244,6 +1244,56 @@ int care_b200_save_preprocessed_reads(care_b200_ctx* ctx, const char* path) {
     return CARE_B200_OK;
 }
 
+int care_b200_load_hashtables(care_b200_ctx* ctx, const char* path) {
+    if (!ctx || !path) return CARE_B200_EINVAL;
+    if (ctx->n == 0) return fail(ctx, CARE_B200_ESTATE, "no reads uploaded");
+    MinhashTablesFile t;
+    const std::string e = read_tables_file(path, t, ctx->opt.num_maps);
+    if (!e.empty()) return fail(ctx, CARE_B200_EIO, e);
+    for (const auto& v : t.values)
+        for (uint32_t id : v)
+            if (id >= ctx->n) return fail(ctx, CARE_B200_EINVAL, "table holds a read id beyond the read storage");
+    // as the reference's loader: k and the per-map result threshold of the file
+    if (t.k != ctx->opt.kmerlength) {
+        ctx->opt.kmerlength = t.k;
+        ctx->sigs_maps = 0;                 // signatures of the storage are hashed again with this k
+    }
+    ctx->threshold = t.threshold;
+    const int maps = (int)t.keys.size();
+    std::vector<const uint64_t*> k(maps);
+    std::vector<const uint32_t*> o(maps), v(maps);
+    std::vector<size_t> nk(maps);
+    for (int m = 0; m < maps; ++m) {
+        k[m] = t.keys[m].data();
+        o[m] = t.offsets[m].data();
+        v[m] = t.values[m].data();
+        nk[m] = t.keys[m].size();
+    }
+    return care_b200_upload_tables(ctx, maps, k.data(), o.data(), v.data(), nk.data());
+}
+
+int care_b200_save_hashtables(care_b200_ctx* ctx, const char* path) {
+    if (!ctx || !path) return CARE_B200_EINVAL;
+    if (!ctx->tables_ready) return fail(ctx, CARE_B200_ESTATE, "no tables uploaded or built");
+    MinhashTablesFile t;
+    t.k = ctx->opt.kmerlength;
+    t.threshold = ctx->threshold;
+    t.load = 0.8f;                          // the reference's default hashtable load factor
+    for (int m = 0; m < ctx->num_maps; ++m) {
+        const uint64_t* keys = nullptr;
+        const uint32_t* offs = nullptr;
+        const uint32_t* vals = nullptr;
+        size_t nk = 0;
+        if (int rc = care_b200_get_table(ctx, m, &keys, &offs, &vals, &nk)) return rc;
+        t.keys.emplace_back(keys, keys + nk);
+        t.offsets.emplace_back(offs, offs + nk + 1);
+        t.values.emplace_back(vals, vals + (nk ? offs[nk] : 0));
+    }
+    const std::string e = write_tables_file(path, t);
+    if (!e.empty()) return fail(ctx, CARE_B200_EIO, e);
+    return CARE_B200_OK;
+}
+
 int care_b200_write_output(care_b200_ctx* ctx, const char* outfile) {
     if (!ctx || !outfile) return CARE_B200_EINVAL;
     if (!ctx->have_records) return fail(ctx, CARE_B200_ESTATE, "reads were not loaded from files");

@@ -28,7 +28,8 @@ void usage() {
         "  --errorfactortuning F        --coveragefactortuning F --pairedFilterThreshold F\n"
         "  --correctionQualityLabels    --batchsize N            -g,--gpu N\n"
         "  --correctionType 0|1 (1: learned decision)  --ml-mlpfile FILE  --clfMinCoverage N\n"
-        "  --save-preprocessedreads-to FILE  --load-preprocessedreads-from FILE");
+        "  --save-preprocessedreads-to FILE  --load-preprocessedreads-from FILE\n"
+        "  --save-hashtables-to FILE         --load-hashtables-from FILE");
 }
 
 bool flag_value(int& i, int argc, char** argv) {
@@ -45,7 +46,7 @@ int main(int argc, char** argv) {
     care_b200_options o;
     care_b200_default_options(&o);
     std::vector<std::string> inputs;
-    std::string outdir, outname, mlpfile, save_reads, load_reads;
+    std::string outdir, outname, mlpfile, save_reads, load_reads, save_tables, load_tables;
     bool haveCov = false, havePair = false;
     for (int i = 1; i < argc; i++) {
         const std::string a = argv[i];
@@ -93,6 +94,8 @@ int main(int argc, char** argv) {
         else if (a == "--clfMinCoverage") o.clf_min_coverage = std::atoi(val());
         else if (a == "--save-preprocessedreads-to") save_reads = val();
         else if (a == "--load-preprocessedreads-from") load_reads = val();
+        else if (a == "--save-hashtables-to") save_tables = val();
+        else if (a == "--load-hashtables-from") load_tables = val();
         else if (a == "--help") { usage(); return 0; }
         else { std::fprintf(stderr, "unknown option %s\n", a.c_str()); usage(); return 1; }
     }
@@ -136,7 +139,15 @@ int main(int argc, char** argv) {
         std::printf("Saving reads to file %s\n", save_reads.c_str());
         if (care_b200_save_preprocessed_reads(ctx, save_reads.c_str())) return die("saving the read storage");
     }
-    if (care_b200_build_tables(ctx)) return die("building hash tables");
+    if (!load_tables.empty()) {
+        if (care_b200_load_hashtables(ctx, load_tables.c_str())) return die("loading the saved hash tables");
+    } else if (care_b200_build_tables(ctx)) {
+        return die("building hash tables");
+    }
+    if (!save_tables.empty()) {
+        std::printf("Saving minhasher to file %s\n", save_tables.c_str());
+        if (care_b200_save_hashtables(ctx, save_tables.c_str())) return die("saving the hash tables");
+    }
     const double t1 = now();
     std::printf("Total number of reads: %u\nMaximum sequence length: %d\nUsing %d maps\n",
                 care_b200_num_reads(ctx), care_b200_max_length(ctx), care_b200_num_maps(ctx));

@@ -1,6 +1,7 @@
 // readfile.cpp -- care-cpu's binary read-storage file (layout in readfile.hpp).
 #include "readfile.hpp"
 
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <fstream>
@@ -33,6 +34,24 @@ bool get_words(std::istream& s, std::vector<uint32_t>& v, uint64_t count) {
     v.resize(count);
     return count == 0 || (bool)s.read(reinterpret_cast<char*>(v.data()), count * 4);
 }
+
+// MurmurHash3's 64-bit finalizer (fmix64), the key hash of the index.
+uint64_t fmix64(uint64_t x) {
+    x ^= x >> 33;
+    x *= 0xff51afd7ed558ccdULL;
+    x ^= x >> 33;
+    x *= 0xc4ceb9fe1a85ec53ULL;
+    x ^= x >> 33;
+    return x;
+}
+
+#pragma pack(push, 1)
+struct IndexSlot {
+    uint64_t key;
+    uint32_t first, count;
+};
+#pragma pack(pop)
+static_assert(sizeof(IndexSlot) == 16, "index slot layout");
 
 }  // namespace
 
@@ -159,6 +178,98 @@ std::string write_storage_file(const std::string& path, const ReadStorageFile& f
 
     put(s, na);
     if (na) s.write(reinterpret_cast<const char*>(f.ambiguous_ids.data()), na * 4);
+    if (!s) return "write failed: " + path;
+    return "";
+}
+
+std::string read_tables_file(const std::string& path, MinhashTablesFile& t, int max_maps) {
+    std::ifstream s(path, std::ios::binary);
+    if (!s) return "cannot open " + path;
+    const std::string trunc = path + ": truncated or not a minhash-table file";
+    int k = 0, thr = 0, maps = 0;
+    float lf = 0.f;
+    if (!get(s, k) || !get(s, thr) || !get(s, lf) || !get(s, maps)) return trunc;
+    if (k < 1 || k > 32 || maps < 1) return path + ": bad header";
+    const int use = std::min(maps, max_maps);
+    t = MinhashTablesFile{};
+    t.k = k;
+    t.threshold = thr;
+    t.load = lf;
+    for (int m = 0; m < use; ++m) {
+        uint64_t nv = 0;
+        std::vector<uint32_t> vals;
+        if (!get(s, nv) || !get_words(s, vals, nv)) return trunc;
+        float load = 0.f;
+        uint64_t nk = 0, probes = 0, size = 0, cap = 0, nslots = 0;
+        if (!get(s, load) || !get(s, nk) || !get(s, probes) || !get(s, size) || !get(s, cap) || !get(s, nslots))
+            return trunc;
+        if (nslots != cap || nk > cap) return path + ": inconsistent key index";
+        std::vector<IndexSlot> slots(nslots);
+        if (nslots && !s.read(reinterpret_cast<char*>(slots.data()), nslots * sizeof(IndexSlot))) return trunc;
+        std::vector<IndexSlot> used;
+        for (const IndexSlot& e : slots) {
+            if (e.key == ~0ull) continue;
+            if ((uint64_t)e.first + e.count > nv) return path + ": key index points past the values";
+            used.push_back(e);
+        }
+        if (used.size() != nk) return path + ": key count differs from the index";
+        std::sort(used.begin(), used.end(), [](const IndexSlot& a, const IndexSlot& b) { return a.key < b.key; });
+        std::vector<uint64_t> keys;
+        std::vector<uint32_t> off{0}, v;
+        for (const IndexSlot& e : used) {
+            keys.push_back(e.key);
+            v.insert(v.end(), vals.begin() + e.first, vals.begin() + e.first + e.count);
+            off.push_back((uint32_t)v.size());
+        }
+        t.keys.push_back(std::move(keys));
+        t.offsets.push_back(std::move(off));
+        t.values.push_back(std::move(v));
+    }
+    return "";
+}
+
+std::string write_tables_file(const std::string& path, const MinhashTablesFile& t) {
+    const int maps = (int)t.keys.size();
+    if (maps < 1 || t.offsets.size() != t.keys.size() || t.values.size() != t.keys.size())
+        return "inconsistent tables";
+    std::ofstream s(path, std::ios::binary | std::ios::trunc);
+    if (!s) return "cannot create " + path;
+    put(s, t.k);
+    put(s, t.threshold);
+    put(s, t.load);
+    put(s, maps);
+    for (int m = 0; m < maps; ++m) {
+        const auto& keys = t.keys[m];
+        const auto& off = t.offsets[m];
+        const uint64_t nv = keys.empty() ? 0 : off[keys.size()];
+        put(s, nv);
+        if (nv) s.write(reinterpret_cast<const char*>(t.values[m].data()), nv * 4);
+        // the key index as the reference builds it: size = keys, capacity
+        // size / load in float, keys inserted in ascending order with linear probing
+        const uint64_t size = keys.size();
+        const uint64_t cap = (uint64_t)((float)size / t.load);
+        if (size > cap) return "load factor above 1";
+        // a free slot: key all ones, value {0, 0} (the reference's
+        // numeric_limits max of a pair value is a value-initialised pair)
+        std::vector<IndexSlot> slots(cap, IndexSlot{~0ull, 0u, 0u});
+        uint64_t probes_max = 0;
+        for (size_t i = 0; i < keys.size(); ++i) {
+            uint64_t pos = fmix64(keys[i]) % cap, probes = 0;
+            while (slots[pos].key != ~0ull) {
+                if (++pos == cap) pos = 0;
+                ++probes;
+            }
+            slots[pos] = IndexSlot{keys[i], off[i], off[i + 1] - off[i]};
+            probes_max = std::max(probes_max, probes);
+        }
+        put(s, t.load);
+        put(s, size);
+        put(s, probes_max);
+        put(s, size);
+        put(s, cap);
+        put(s, cap);
+        if (cap) s.write(reinterpret_cast<const char*>(slots.data()), cap * sizeof(IndexSlot));
+    }
     if (!s) return "write failed: " + path;
     return "";
 }

@@ -41,4 +41,28 @@ std::string read_storage_file(const std::string& path, ReadStorageFile& out);
 // Writes `in` in the reference's layout (ambiguous ids in the order given).
 std::string write_storage_file(const std::string& path, const ReadStorageFile& in);
 
+// The minhash-table file of care-cpu (--save-hashtables-to /
+// --load-hashtables-from; OrdinaryCpuMinhasher::writeToStream / loadFromStream,
+// include/ordinaryminhasher.hpp:303-339; per map CpuReadOnlyMultiValueHashTable
+// and its AoSCpuSingleValueHashTable key index, include/cpuhashtable.hpp:
+// 30-290, 468-685). Layout, little-endian:
+//   i32 k; i32 per-map result threshold; f32 load factor; i32 maps; per map:
+//   u64 values, then the u32 read ids (each key's ids a contiguous ascending
+//   run); the key index: f32 load, u64 keys, u64 longest probe sequence,
+//   u64 size (= keys), u64 capacity (size / load, truncated), u64 slots, then
+//   the slots {u64 key, u32 first value, u32 count}: a key at
+//   MurmurHash3-fmix64(key) mod capacity or the next free slot after it (keys
+//   inserted in ascending order); a free slot has key all ones and value 0.
+struct MinhashTablesFile {
+    int k = 0, threshold = 0;
+    float load = 0.8f;
+    std::vector<std::vector<uint64_t>> keys;       // per map, ascending
+    std::vector<std::vector<uint32_t>> offsets;    // per map, keys + 1 prefix offsets into values
+    std::vector<std::vector<uint32_t>> values;     // per map, read ids
+};
+
+// Reads at most max_maps maps (the reference loads min(file, requested)).
+std::string read_tables_file(const std::string& path, MinhashTablesFile& out, int max_maps);
+std::string write_tables_file(const std::string& path, const MinhashTablesFile& in);
+
 }  // namespace careb200

@@ -166,6 +166,19 @@ int care_b200_load_preprocessed_reads(care_b200_ctx* ctx, const char* path);
  * ambiguous read ids in ascending order. */
 int care_b200_save_preprocessed_reads(care_b200_ctx* ctx, const char* path);
 
+/* Minhasher handle, binary file: uploads the tables care-cpu saved with
+ * --save-hashtables-to (OrdinaryCpuMinhasher::loadFromStream,
+ * include/ordinaryminhasher.hpp:318-339), in place of care_b200_build_tables.
+ * As in the reference, at most num_maps maps are loaded and the file's k-mer
+ * length and per-map result threshold are used. The read storage must be the
+ * one the tables were built from (read ids are checked against its size). */
+int care_b200_load_hashtables(care_b200_ctx* ctx, const char* path);
+
+/* Writes the tables in the same layout, byte for byte what care-cpu writes
+ * for the same tables (OrdinaryCpuMinhasher::writeToStream,
+ * include/ordinaryminhasher.hpp:303-316; load factor 0.8). */
+int care_b200_save_hashtables(care_b200_ctx* ctx, const char* path);
+
 /* Merges all corrections of the last full-range call with the input reads
  * and writes the output file (correctionresultoutput.cpp:30-440, 730-1020). */
 int care_b200_write_output(care_b200_ctx* ctx, const char* outfile);

@@ -77,4 +77,37 @@ void rf_parse_arrays(void* p, uint32_t* seq, int32_t* len, uint32_t* qual, uint3
 
 void rf_parse_free(void* p) { delete static_cast<HostReads*>(p); }
 
+// minhash-table file: info = k, threshold, maps, load factor bits
+void* rt_load(const char* path, int max_maps, unsigned long long* info, char* err, int errlen) {
+    auto* t = new MinhashTablesFile;
+    const std::string e = read_tables_file(path, *t, max_maps);
+    if (!e.empty()) { set_err(e, err, errlen); delete t; return nullptr; }
+    uint32_t lb;
+    std::memcpy(&lb, &t->load, 4);
+    const unsigned long long v[4] = {(unsigned long long)t->k, (unsigned long long)t->threshold, t->keys.size(), lb};
+    std::memcpy(info, v, sizeof(v));
+    return t;
+}
+
+void rt_map_size(void* h, int m, unsigned long long* nkeys, unsigned long long* nvalues) {
+    const auto* t = static_cast<const MinhashTablesFile*>(h);
+    *nkeys = t->keys[m].size();
+    *nvalues = t->values[m].size();
+}
+
+void rt_map(void* h, int m, uint64_t* keys, uint32_t* offsets, uint32_t* values) {
+    const auto* t = static_cast<const MinhashTablesFile*>(h);
+    std::memcpy(keys, t->keys[m].data(), t->keys[m].size() * 8);
+    std::memcpy(offsets, t->offsets[m].data(), t->offsets[m].size() * 4);
+    std::memcpy(values, t->values[m].data(), t->values[m].size() * 4);
+}
+
+int rt_write(void* h, const char* path, char* err, int errlen) {
+    const std::string e = write_tables_file(path, *static_cast<const MinhashTablesFile*>(h));
+    set_err(e, err, errlen);
+    return e.empty() ? 0 : -1;
+}
+
+void rt_free(void* h) { delete static_cast<MinhashTablesFile*>(h); }
+
 }  // extern "C"

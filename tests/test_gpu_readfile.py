@@ -1,7 +1,7 @@
-"""The binary read-storage file on the GPU: storage loaded from the files
-care-cpu saved (tests/golden/make_preprocessed.py) corrects exactly like
-storage parsed from the same FASTQ, a save from the device reproduces the
-reference's file, the CLI's --load-preprocessedreads-from gives the same
+"""The binary read-storage and minhash-table files on the GPU: storage and
+tables loaded from the files care-cpu saved (tests/golden/make_preprocessed.py)
+correct exactly like storage parsed from the same FASTQ and tables built on the
+GPU, saves reproduce the reference's files, the CLI's load flags give the same
 output, and a file with other quality bits is rejected as in the reference."""
 import gzip
 import os
@@ -95,3 +95,58 @@ def test_quality_bits_mismatch_rejected(tmp_path):
     with care_b200.Corrector(care_b200.options_from_args(CASES["pre_un"].replace("Bits 8", "Bits 2"))) as c:
         with pytest.raises(care_b200.CareError, match="bits per quality"):
             c.load_preprocessed_reads(p["bin"])
+
+
+H4 = "-c 50 -k 20 -h 4 -q --qualityScoreBits 2 --pairmode PE --candidateCorrection"
+
+
+def tables_file(tmp):
+    p = os.path.join(tmp, "pre_pe_h4.tables")
+    with open(p, "wb") as f:
+        f.write(gzip.decompress(open(os.path.join(GOLD, "pre_pe_h4.tables.gz"), "rb").read()))
+    return p
+
+
+def test_loaded_tables_correct_like_built_tables(tmp_path):
+    p = unpack(str(tmp_path), "pre_pe")
+    tab = tables_file(str(tmp_path))
+    with care_b200.Corrector(care_b200.options_from_args(H4)) as c:
+        c.load_files([p["fq"]])
+        c.build_tables()
+        built = [c.get_table(m) for m in range(c.num_maps)]
+        a = c.correct_range()
+    with care_b200.Corrector(care_b200.options_from_args(H4)) as c:
+        c.load_preprocessed_reads(p["bin"])
+        c.load_hashtables(tab)
+        assert c.num_maps == 4
+        loaded = [c.get_table(m) for m in range(c.num_maps)]
+        b = c.correct_range()
+    for x, y in zip(built, loaded):
+        for u, v in zip(x, y):
+            assert np.array_equal(u, v)
+    assert (a.status & 1).sum() > 0
+    same(a, b)
+
+
+def test_save_tables_reproduces_reference_file(tmp_path):
+    p = unpack(str(tmp_path), "pre_pe")
+    out = str(tmp_path / "saved.tables")
+    with care_b200.Corrector(care_b200.options_from_args(H4)) as c:
+        c.load_files([p["fq"]])
+        c.build_tables()
+        c.save_hashtables(out)
+    assert open(out, "rb").read() == open(tables_file(str(tmp_path)), "rb").read()
+
+
+def test_cli_load_both_files(tmp_path):
+    p = unpack(str(tmp_path), "pre_pe")
+    tab = tables_file(str(tmp_path))
+    outs = []
+    for extra in ([], ["--load-preprocessedreads-from", p["bin"], "--load-hashtables-from", tab]):
+        d = tmp_path / f"t{len(outs)}"
+        d.mkdir()
+        cmd = [care_b200.CLI_PATH, "-i", p["fq"], "-d", str(d), "-o", "out.fq"] + H4.split() + extra
+        r = subprocess.run(cmd, capture_output=True, text=True, timeout=300)
+        assert r.returncode == 0, r.stderr
+        outs.append((d / "out.fq").read_bytes())
+    assert outs[0] == outs[1] and len(outs[0]) > 0

@@ -1,9 +1,10 @@
-"""care-cpu's binary read-storage file (--save-preprocessedreads-to), without a
-GPU: the files the reference wrote for two seeded read sets
-(tests/golden/make_preprocessed.py) hold exactly the read storage this
-library's own preprocessing builds from the same FASTQ, and the writer
-reproduces the reference's bytes (the ambiguous ids, which the reference
-writes in the order of a hash set, as a set)."""
+"""care-cpu's binary read-storage and minhash-table files
+(--save-preprocessedreads-to, --save-hashtables-to), without a GPU: the files
+the reference wrote for seeded read sets (tests/golden/make_preprocessed.py)
+hold exactly the read storage this library's own preprocessing builds from the
+same FASTQ and the tables the oracle builds, and the writers reproduce the
+reference's bytes (the ambiguous ids, which the reference writes in the order
+of a hash set, as a set)."""
 import ctypes
 import gzip
 import os
@@ -40,6 +41,12 @@ def harness():
     for f in (lib.rf_arrays, lib.rf_parse_arrays):
         f.argtypes = [ctypes.c_void_p] + [ctypes.c_void_p] * 4
     lib.rf_free.argtypes = lib.rf_parse_free.argtypes = [ctypes.c_void_p]
+    lib.rt_load.restype = ctypes.c_void_p
+    lib.rt_load.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(U64), ctypes.c_char_p, ctypes.c_int]
+    lib.rt_map_size.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(U64), ctypes.POINTER(U64)]
+    lib.rt_map.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    lib.rt_write.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int]
+    lib.rt_free.argtypes = [ctypes.c_void_p]
     lib.rf_write.argtypes = [ctypes.c_char_p, U64, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, U64, U64,
                              ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, U64, ctypes.c_char_p,
                              ctypes.c_int]
@@ -137,3 +144,57 @@ def test_truncated_file_is_rejected(tmp_path):
         err = ctypes.create_string_buffer(256)
         assert not H.rf_load(str(q).encode(), info, err, 256)
         assert b"truncated" in err.value or b"inconsistent" in err.value
+
+
+def load_tables(path, max_maps=64):
+    info = (U64 * 4)()
+    err = ctypes.create_string_buffer(256)
+    h = H.rt_load(path.encode(), max_maps, info, err, 256)
+    assert h, err.value.decode()
+    maps = []
+    for m in range(info[2]):
+        nk, nv = U64(), U64()
+        H.rt_map_size(h, m, ctypes.byref(nk), ctypes.byref(nv))
+        keys = np.zeros(max(nk.value, 1), np.uint64)
+        offs = np.zeros(nk.value + 1, np.uint32)
+        vals = np.zeros(max(nv.value, 1), np.uint32)
+        H.rt_map(h, m, keys.ctypes.data, offs.ctypes.data, vals.ctypes.data)
+        maps.append((keys[:nk.value], offs, vals[:nv.value]))
+    return h, list(info), maps
+
+
+def test_reference_tables_equal_the_oracle(tmp_path):
+    import _oracle
+    p = unpack(str(tmp_path), "pre_pe")
+    tab = tmp_path / "pre_pe_h4.tables"
+    tab.write_bytes(gzip.decompress(open(os.path.join(GOLD, "pre_pe_h4.tables.gz"), "rb").read()))
+    h, info, maps = load_tables(str(tab))
+    H.rt_free(h)
+    k, thr, nmaps, _ = info
+    assert (k, thr, nmaps) == (20, 125, 4)
+    run = _oracle.OracleRun([p["fq"]], _oracle.opts_from_args("-c 50 -k 20 -h 4 -q --qualityScoreBits 2 --pairmode PE"),
+                            threads=4)
+    try:
+        for m in range(4):
+            ok, oo, ov = run.table(m)
+            rk, ro, rv = maps[m]
+            assert len(rk) > 50
+            assert np.array_equal(rk, ok) and np.array_equal(ro, oo) and np.array_equal(rv, ov), m
+    finally:
+        run.close()
+
+
+def test_table_writer_reproduces_reference_bytes(tmp_path):
+    ref = tmp_path / "ref.tables"
+    ref.write_bytes(gzip.decompress(open(os.path.join(GOLD, "pre_pe_h4.tables.gz"), "rb").read()))
+    h, info, maps = load_tables(str(ref))
+    out = tmp_path / "ours.tables"
+    err = ctypes.create_string_buffer(256)
+    assert H.rt_write(h, str(out).encode(), err, 256) == 0, err.value.decode()
+    H.rt_free(h)
+    assert out.read_bytes() == ref.read_bytes()
+    h2, _, _ = load_tables(str(ref), max_maps=2)              # the reference loads min(file, requested) maps
+    nk = U64(); nv = U64()
+    H.rt_map_size(h2, 1, ctypes.byref(nk), ctypes.byref(nv))
+    assert nk.value == len(maps[1][0])
+    H.rt_free(h2)
