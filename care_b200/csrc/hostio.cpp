@@ -38,13 +38,12 @@ struct Rec {
     bool fasta;
 };
 
-// One record of a 4-line FASTQ or single-line FASTA file.
-bool next_record(FileBuf& f, Rec& r) {
-    const size_t n = f.data.size();
-    const char* d = f.data.data();
-    while (f.pos < n && d[f.pos] != '@' && d[f.pos] != '>') f.pos++;
-    if (f.pos >= n) return false;
-    r.fasta = d[f.pos] == '>';
+// One record of a 4-line FASTQ or single-line FASTA file, read at `pos`
+// (advanced past it) of the n bytes at d.
+bool next_record_at(const char* d, size_t n, size_t& pos, Rec& r) {
+    while (pos < n && d[pos] != '@' && d[pos] != '>') pos++;
+    if (pos >= n) return false;
+    r.fasta = d[pos] == '>';
     auto line = [&](size_t p, const char*& b, size_t& l) {
         size_t e = p;
         while (e < n && d[e] != '\n') e++;
@@ -53,14 +52,77 @@ bool next_record(FileBuf& f, Rec& r) {
         if (l && b[l - 1] == '\r') l--;
         return e + 1;
     };
-    size_t p = line(f.pos + 1, r.h, r.hl);
+    size_t p = line(pos + 1, r.h, r.hl);
     p = line(p, r.s, r.sl);
-    if (r.fasta) { r.q = ""; r.ql = 0; f.pos = p; return true; }
+    if (r.fasta) { r.q = ""; r.ql = 0; pos = p; return true; }
     const char* plus; size_t pl;
     p = line(p, plus, pl);
     p = line(p, r.q, r.ql);
-    f.pos = p;
+    pos = p;
     return true;
+}
+
+// Start of the first record at or after `from`: a line that starts with '>'
+// (FASTA), or with '@' and has a '+' line two lines below (FASTQ; a quality
+// line that starts with '@' is followed by a header and a sequence line, so it
+// never passes). n when there is none.
+size_t record_start(const char* d, size_t n, size_t from, bool fasta) {
+    auto next_line = [&](size_t p) {
+        while (p < n && d[p] != '\n') p++;
+        return p < n ? p + 1 : n;
+    };
+    size_t p = from;
+    if (p > 0 && d[p - 1] != '\n') p = next_line(p);
+    for (; p < n; p = next_line(p)) {
+        if (fasta) { if (d[p] == '>') return p; continue; }
+        if (d[p] != '@') continue;
+        const size_t l2 = next_line(next_line(p));
+        if (l2 < n && d[l2] == '+') return p;
+    }
+    return n;
+}
+
+// All records of a file, as a scan from its first byte finds them. Up to
+// `threads` threads scan segments that begin at record starts; the segments
+// must chain (each scan ends exactly where the next segment begins), else the
+// file is scanned again from the beginning by one thread.
+std::vector<Rec> scan_file(const FileBuf& f, unsigned threads) {
+    const char* d = f.data.data();
+    const size_t n = f.data.size();
+    std::vector<Rec> all;
+    auto serial = [&]() {
+        all.clear();
+        size_t pos = 0;
+        Rec r;
+        while (next_record_at(d, n, pos, r)) all.push_back(r);
+    };
+    const unsigned T = (unsigned)std::max<size_t>(1, std::min<size_t>(threads, n >> 16));   // >= 64 KB a segment
+    size_t first = 0;
+    while (first < n && d[first] != '@' && d[first] != '>') first++;
+    if (T <= 1 || first >= n) { serial(); return all; }
+    const bool fasta = d[first] == '>';
+    std::vector<size_t> start(T + 1, n);
+    start[0] = first;
+    for (unsigned t = 1; t < T; t++) start[t] = std::max(start[t - 1], record_start(d, n, n / T * t, fasta));
+    std::vector<std::vector<Rec>> part(T);
+    std::vector<size_t> endpos(T, 0);
+    std::vector<std::thread> th;
+    for (unsigned t = 0; t < T; t++) {
+        th.emplace_back([&, t] {
+            size_t pos = start[t];
+            Rec r;
+            while (pos < start[t + 1] && next_record_at(d, n, pos, r)) part[t].push_back(r);
+            endpos[t] = std::max(pos, start[t]);
+        });
+    }
+    for (auto& x : th) x.join();
+    for (unsigned t = 0; t + 1 < T; t++)
+        if (endpos[t] != start[t + 1]) { serial(); return all; }
+    size_t total = 0;
+    for (auto& v : part) total += v.size();
+    all.reserve(total);
+    for (auto& v : part) all.insert(all.end(), v.begin(), v.end());
+    return all;
 }
 
 }  // namespace
@@ -115,7 +177,14 @@ void quality_weights(float* w) {
 
 std::string load_reads(const std::vector<std::string>& files, bool paired_end, bool use_quality,
                        int quality_bits, HostReads& out) {
+    return load_reads_threads(files, paired_end, use_quality, quality_bits, out,
+                              std::max(1u, std::thread::hardware_concurrency()));
+}
+
+std::string load_reads_threads(const std::vector<std::string>& files, bool paired_end, bool use_quality,
+                               int quality_bits, HostReads& out, unsigned threads) {
     if (files.empty() || files.size() > 2) return "expected one or two input files";
+    threads = std::max(1u, threads);
     std::vector<FileBuf> in(files.size());
     for (size_t i = 0; i < files.size(); i++)
         if (!read_whole(files[i], in[i])) return "cannot read input file " + files[i];
@@ -124,26 +193,56 @@ std::string load_reads(const std::vector<std::string>& files, bool paired_end, b
     out.quality_bits = quality_bits;
     std::vector<size_t> fileFirst;      // first read of each SE file (rotation restarts)
     fileFirst.push_back(0);
-    size_t cur = 0;
-    for (;;) {
-        Rec r;
-        if (!next_record(in[cur], r)) {
-            if (files.size() == 2 && !paired_end && cur == 0) {
-                cur = 1;
-                fileFirst.push_back(out.rec_off.size());
-                continue;
+    // records in read order: one file; two SE files one after the other; two
+    // PE files alternating (mate 1, mate 2, ...) until either file ends
+    std::vector<Rec> recs;
+    {
+        std::vector<std::vector<Rec>> per(files.size());
+        for (size_t i = 0; i < files.size(); i++) per[i] = scan_file(in[i], threads);
+        if (files.size() == 1) {
+            recs = std::move(per[0]);
+        } else if (!paired_end) {
+            recs = std::move(per[0]);
+            fileFirst.push_back(recs.size());
+            recs.insert(recs.end(), per[1].begin(), per[1].end());
+        } else {
+            for (size_t i = 0;; i++) {
+                if (i >= per[0].size()) break;
+                recs.push_back(per[0][i]);
+                if (i >= per[1].size()) break;
+                recs.push_back(per[1][i]);
             }
-            break;
         }
-        out.fasta |= r.fasta;
-        out.rec_off.push_back(out.text.size());
-        out.len.push_back((int32_t)r.sl);
-        out.text.insert(out.text.end(), r.h, r.h + r.hl); out.text.push_back(0);
-        out.text.insert(out.text.end(), r.s, r.s + r.sl); out.text.push_back(0);
-        out.text.insert(out.text.end(), r.q, r.q + r.ql); out.text.push_back(0);
-        if (files.size() == 2 && paired_end) cur ^= 1;
     }
-    const size_t n = out.rec_off.size();
+    const size_t n = recs.size();
+    // the records' text, NUL separated: header, sequence, quality
+    out.rec_off.resize(n);
+    out.len.resize(n);
+    size_t tsize = 0;
+    for (size_t i = 0; i < n; i++) {
+        const Rec& r = recs[i];
+        out.fasta |= r.fasta;
+        out.rec_off[i] = tsize;
+        out.len[i] = (int32_t)r.sl;
+        tsize += r.hl + r.sl + r.ql + 3;
+    }
+    out.text.resize(tsize);
+    {
+        const unsigned T = (unsigned)std::max<size_t>(1, std::min<size_t>(threads, n / 4096));
+        std::vector<std::thread> th;
+        for (unsigned t = 0; t < T; t++) {
+            th.emplace_back([&, t] {
+                for (size_t i = n * t / T; i < n * (t + 1) / T; i++) {
+                    const Rec& r = recs[i];
+                    char* o = out.text.data() + out.rec_off[i];
+                    std::memcpy(o, r.h, r.hl); o += r.hl; *o++ = 0;
+                    std::memcpy(o, r.s, r.sl); o += r.sl; *o++ = 0;
+                    std::memcpy(o, r.q, r.ql); o += r.ql; *o++ = 0;
+                }
+            });
+        }
+        for (auto& x : th) x.join();
+    }
     if (n >= 0xFFFFFFFFu) return "too many reads";
     out.n = (uint32_t)n;
     out.has_quality = use_quality && !out.fasta;
@@ -194,7 +293,7 @@ std::string load_reads(const std::vector<std::string>& files, bool paired_end, b
         }
     };
     const size_t nb = batches.size();
-    const unsigned nt = std::max(1u, std::min<unsigned>(std::thread::hardware_concurrency(), (unsigned)nb));
+    const unsigned nt = std::max(1u, std::min<unsigned>(threads, (unsigned)nb));
     std::vector<std::thread> th;
     for (unsigned t = 0; t < nt; t++) th.emplace_back(batch_work, nb * t / nt, nb * (t + 1) / nt);
     for (auto& x : th) x.join();

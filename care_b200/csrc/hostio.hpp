@@ -29,6 +29,9 @@ struct HostReads {
 // Returns an empty string on success, else an error message.
 std::string load_reads(const std::vector<std::string>& files, bool paired_end, bool use_quality,
                        int quality_bits, HostReads& out);
+// The same with at most `threads` threads (1: a single sequential scan).
+std::string load_reads_threads(const std::vector<std::string>& files, bool paired_end, bool use_quality,
+                               int quality_bits, HostReads& out, unsigned threads);
 
 void encode_2bit(const char* s, int len, uint32_t* out);
 void encode_quality(const char* q, int len, int bits, uint32_t* out);

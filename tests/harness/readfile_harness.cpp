@@ -77,6 +77,33 @@ void rf_parse_arrays(void* p, uint32_t* seq, int32_t* len, uint32_t* qual, uint3
 
 void rf_parse_free(void* p) { delete static_cast<HostReads*>(p); }
 
+// FNV-1a digest of everything this library's preprocessing produces for one
+// or two files with `threads` threads: read count, record text and offsets,
+// lengths, 2-bit rows, quality rows, ambiguous ids
+int rf_parse_digest(const char* f0, const char* f1, int paired_end, int quality_bits, unsigned threads,
+                    unsigned long long* digest, unsigned long long* nreads, char* err, int errlen) {
+    HostReads h;
+    std::vector<std::string> files{f0};
+    if (f1) files.push_back(f1);
+    const std::string e = load_reads_threads(files, paired_end != 0, true, quality_bits, h, threads);
+    if (!e.empty()) { set_err(e, err, errlen); return -1; }
+    unsigned long long x = 1469598103934665603ull;
+    auto mix = [&](const void* p, size_t bytes) {
+        const unsigned char* c = static_cast<const unsigned char*>(p);
+        for (size_t i = 0; i < bytes; i++) { x ^= c[i]; x *= 1099511628211ull; }
+    };
+    mix(&h.n, sizeof(h.n));
+    mix(h.text.data(), h.text.size());
+    mix(h.rec_off.data(), h.rec_off.size() * sizeof(size_t));
+    mix(h.len.data(), h.len.size() * 4);
+    mix(h.seq.data(), h.seq.size() * 4);
+    mix(h.qual.data(), h.qual.size() * 4);
+    mix(h.ambiguous_ids.data(), h.ambiguous_ids.size() * 4);
+    *digest = x;
+    *nreads = h.n;
+    return 0;
+}
+
 // minhash-table file: info = k, threshold, maps, load factor bits
 void* rt_load(const char* path, int max_maps, unsigned long long* info, char* err, int errlen) {
     auto* t = new MinhashTablesFile;

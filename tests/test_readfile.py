@@ -41,6 +41,8 @@ def harness():
     for f in (lib.rf_arrays, lib.rf_parse_arrays):
         f.argtypes = [ctypes.c_void_p] + [ctypes.c_void_p] * 4
     lib.rf_free.argtypes = lib.rf_parse_free.argtypes = [ctypes.c_void_p]
+    lib.rf_parse_digest.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_uint,
+                                    ctypes.POINTER(U64), ctypes.POINTER(U64), ctypes.c_char_p, ctypes.c_int]
     lib.rt_load.restype = ctypes.c_void_p
     lib.rt_load.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(U64), ctypes.c_char_p, ctypes.c_int]
     lib.rt_map_size.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(U64), ctypes.POINTER(U64)]
@@ -198,3 +200,65 @@ def test_table_writer_reproduces_reference_bytes(tmp_path):
     H.rt_map_size(h2, 1, ctypes.byref(nk), ctypes.byref(nv))
     assert nk.value == len(maps[1][0])
     H.rt_free(h2)
+
+
+def digest(f0, f1=None, pe=False, qbits=2, threads=1):
+    d, n = U64(), U64()
+    err = ctypes.create_string_buffer(256)
+    rc = H.rf_parse_digest(f0.encode(), f1.encode() if f1 else None, int(pe), qbits, threads, ctypes.byref(d),
+                           ctypes.byref(n), err, 256)
+    assert rc == 0, err.value.decode()
+    return d.value, n.value
+
+
+def _records(rng, n, L=120, at_quality=False, fasta=False, crlf=False, n_bases=False):
+    eol = "\r\n" if crlf else "\n"
+    out = []
+    for i in range(n):
+        s = "".join(rng.choice("ACGT") for _ in range(L))
+        if n_bases and i % 7 == 0:
+            s = s[:5] + "N" + s[6:]
+        if fasta:
+            out.append(f">r{i}{eol}{s}{eol}")
+        else:
+            q = "".join(rng.choice("#+5?@AEI") for _ in range(L))
+            if at_quality:
+                q = "@" + q[1:]                        # quality lines that begin like a header
+            out.append(f"@r{i} x{eol}{s}{eol}+{eol}{q}{eol}")
+    return out
+
+
+@pytest.mark.parametrize("kind", ["fastq", "at_quality", "fasta", "crlf", "pe2", "se2"])
+def test_parallel_scan_equals_sequential(tmp_path, kind):
+    """The threaded record scan gives exactly the single-threaded result."""
+    import random
+    rng = random.Random(hash(kind) & 0xffff)
+    recs = _records(rng, 12000, at_quality=(kind == "at_quality"), fasta=(kind == "fasta"),
+                    crlf=(kind == "crlf"), n_bases=True)
+    f0 = tmp_path / "a.fq"
+    f1 = None
+    if kind in ("pe2", "se2"):
+        f1 = tmp_path / "b.fq"
+        f0.write_text("".join(recs[0::2]))
+        f1.write_text("".join(recs[1::2] + (recs[-1:] if kind == "se2" else [])))
+    else:
+        f0.write_text("".join(recs))
+    pe = kind in ("pe2", "fastq", "at_quality", "crlf")
+    args = (str(f0), str(f1) if f1 else None, pe)
+    ref = digest(*args, threads=1)
+    assert ref[1] > 0
+    for t in (2, 3, 8, 16):
+        assert digest(*args, threads=t) == ref, t
+
+
+def test_parallel_scan_falls_back_on_irregular_files(tmp_path):
+    """A file whose records do not chain at the segment starts (here: records
+    with a missing quality line) is scanned sequentially, with the same result."""
+    import random
+    rng = random.Random(5)
+    recs = _records(rng, 8000)
+    broken = [r if i % 997 else "@bad{}\nACGT\n".format(i) for i, r in enumerate(recs)]
+    f = tmp_path / "irregular.fq"
+    f.write_text("".join(broken))
+    ref = digest(str(f), threads=1)
+    assert digest(str(f), threads=8) == ref
