@@ -306,26 +306,19 @@ std::string write_corrected(const HostReads& reads, const HostCorrections& c, bo
     std::FILE* fp = std::fopen(path.c_str(), "wb");
     if (!fp) return "cannot open output file " + path;
     const int dp = c.max_len;
-    // candidate corrections grouped by read id
-    std::vector<uint64_t> order(c.ncand);
-    std::iota(order.begin(), order.end(), 0);
-    std::sort(order.begin(), order.end(), [&](uint64_t x, uint64_t y) {
-        return c.cand_id[x] != c.cand_id[y] ? c.cand_id[x] < c.cand_id[y] : x < y;
-    });
-    std::vector<char> dec((size_t)reads.max_len + 1), m0((size_t)reads.max_len + 1),
-        m1((size_t)reads.max_len + 1), outseq((size_t)reads.max_len + 1);
-    auto decode = [&](uint32_t id, int L) {
-        const uint32_t* row = reads.seq.data() + (size_t)id * reads.seq_pitch;
-        for (int p = 0; p < L; p++) dec[p] = "ACGT"[(row[p >> 4] >> (30 - 2 * (p & 15))) & 3u];
-    };
-    // the sequence the combiner writes for one result: edits applied to the
-    // input read, or the stored full sequence
-    auto materialize = [&](const char* orig, const char* seq, int L, bool useEdits, char* o) {
-        if (useEdits) {
-            std::memcpy(o, orig, (size_t)L);
-            for (int i = 0; i < L; i++) if (seq[i] != dec[i]) o[i] = seq[i];
-        } else std::memcpy(o, seq, (size_t)L);
-    };
+    const uint32_t n = reads.n;
+    // candidate corrections grouped by read id, in stored order within a read
+    // (a stable counting sort); read i's are order[cstart[i] .. cstart[i+1])
+    std::vector<uint64_t> cstart((size_t)n + 1, 0), order;
+    for (uint64_t k = 0; k < c.ncand; k++)
+        if (c.cand_id[k] < n) cstart[c.cand_id[k] + 1]++;
+    for (uint32_t i = 0; i < n; i++) cstart[i + 1] += cstart[i];
+    order.resize(cstart[n]);
+    {
+        std::vector<uint64_t> fill(cstart.begin(), cstart.end() - 1);
+        for (uint64_t k = 0; k < c.ncand; k++)
+            if (c.cand_id[k] < n) order[fill[c.cand_id[k]]++] = k;
+    }
     // The reference's merge (correctionresultoutput.cpp:30-440) combines --
     // and labels -- only reads up to the last read id with a stored result;
     // later reads are copied unchanged. Stored results: anchor results that
@@ -341,59 +334,91 @@ std::string write_corrected(const HostReads& reads, const HostCorrections& c, bo
         const bool hqAnchor = id >= c.first && id < c.first + c.count && (c.status[id - c.first] & 3) == 3;
         if (!hqAnchor) last = std::max<int64_t>(last, id);
     }
-    std::string buf;
-    buf.reserve(1 << 22);
-    uint64_t ci = 0;
-    for (uint32_t i = 0; i < reads.n; i++) {
-        const char* h = reads.text.data() + reads.rec_off[i];
-        const char* s = h + std::strlen(h) + 1;
-        const char* q = s + std::strlen(s) + 1;
-        const int L = reads.len[i];
-        std::memcpy(outseq.data(), s, (size_t)L);
-        const uint64_t cb = ci;
-        while (ci < c.ncand && c.cand_id[order[ci]] == i) ci++;
-        const uint64_t ncand = ci - cb;
-        int label = 0;
-        bool corrected = false;
-        if (i >= c.first && i < c.first + c.count) {
-            const uint32_t k = i - c.first;
-            const uint8_t st = c.status[k];
-            const bool isCorr = st & 1, hq = st & 2, useEdits = st & 4;
-            // correct_cpu.cpp:263-264 save filter: HQ edit lists with no edit
-            // are not stored
-            const bool stored = isCorr && !(hq && useEdits && c.nedits[k] == 0);
-            if (stored) {
-                const char* aseq = c.seq + (size_t)k * dp;
-                decode(i, L);
-                if (hq) {
-                    materialize(s, aseq, L, useEdits, outseq.data());
-                    corrected = true; label = 3;
-                } else if (1 + ncand >= 3) {
-                    materialize(s, aseq, L, useEdits, m0.data());
-                    bool same = true;
-                    for (uint64_t x = cb; x < ci && same; x++) {
-                        const uint64_t idx = order[x];
-                        materialize(s, c.cand_seq + idx * dp, L, c.cand_use_edits[idx], m1.data());
-                        if (std::memcmp(m0.data(), m1.data(), (size_t)L) != 0) same = false;
+
+    // the output records of reads [b, e) appended to buf
+    auto format = [&](uint32_t b, uint32_t e, std::string& buf) {
+        std::vector<char> dec((size_t)reads.max_len + 1), m0((size_t)reads.max_len + 1),
+            m1((size_t)reads.max_len + 1), outseq((size_t)reads.max_len + 1);
+        auto decode = [&](uint32_t id, int L) {
+            const uint32_t* row = reads.seq.data() + (size_t)id * reads.seq_pitch;
+            for (int p = 0; p < L; p++) dec[p] = "ACGT"[(row[p >> 4] >> (30 - 2 * (p & 15))) & 3u];
+        };
+        // the sequence the combiner writes for one result: edits applied to
+        // the input read, or the stored full sequence
+        auto materialize = [&](const char* orig, const char* seq, int L, bool useEdits, char* o) {
+            if (useEdits) {
+                std::memcpy(o, orig, (size_t)L);
+                for (int i = 0; i < L; i++) if (seq[i] != dec[i]) o[i] = seq[i];
+            } else std::memcpy(o, seq, (size_t)L);
+        };
+        for (uint32_t i = b; i < e; i++) {
+            const char* h = reads.text.data() + reads.rec_off[i];
+            const char* s = h + std::strlen(h) + 1;
+            const char* q = s + std::strlen(s) + 1;
+            const int L = reads.len[i];
+            std::memcpy(outseq.data(), s, (size_t)L);
+            const uint64_t cb = cstart[i], ce = cstart[i + 1];
+            const uint64_t ncand = ce - cb;
+            int label = 0;
+            bool corrected = false;
+            if (i >= c.first && i < c.first + c.count) {
+                const uint32_t k = i - c.first;
+                const uint8_t st = c.status[k];
+                const bool isCorr = st & 1, hq = st & 2, useEdits = st & 4;
+                // correct_cpu.cpp:263-264 save filter: HQ edit lists with no
+                // edit are not stored
+                const bool stored = isCorr && !(hq && useEdits && c.nedits[k] == 0);
+                if (stored) {
+                    const char* aseq = c.seq + (size_t)k * dp;
+                    decode(i, L);
+                    if (hq) {
+                        materialize(s, aseq, L, useEdits, outseq.data());
+                        corrected = true; label = 3;
+                    } else if (1 + ncand >= 3) {
+                        materialize(s, aseq, L, useEdits, m0.data());
+                        bool same = true;
+                        for (uint64_t x = cb; x < ce && same; x++) {
+                            const uint64_t idx = order[x];
+                            materialize(s, c.cand_seq + idx * dp, L, c.cand_use_edits[idx], m1.data());
+                            if (std::memcmp(m0.data(), m1.data(), (size_t)L) != 0) same = false;
+                        }
+                        if (same) { std::memcpy(outseq.data(), m0.data(), (size_t)L); corrected = true; label = 2; }
+                    } else {
+                        materialize(s, aseq, L, useEdits, outseq.data());
+                        corrected = true; label = 1;
                     }
-                    if (same) { std::memcpy(outseq.data(), m0.data(), (size_t)L); corrected = true; label = 2; }
-                } else {
-                    materialize(s, aseq, L, useEdits, outseq.data());
-                    corrected = true; label = 1;
                 }
             }
+            buf.push_back(reads.fasta ? '>' : '@');
+            buf.append(h);
+            if (quality_labels && (int64_t)i <= last) { buf.append(" care:q="); buf.push_back((char)('0' + (corrected ? label : 0))); }
+            buf.push_back('\n');
+            buf.append(outseq.data(), (size_t)L);
+            buf.push_back('\n');
+            if (!reads.fasta) { buf.append("+\n"); buf.append(q); buf.push_back('\n'); }
         }
-        buf.push_back(reads.fasta ? '>' : '@');
-        buf.append(h);
-        if (quality_labels && (int64_t)i <= last) { buf.append(" care:q="); buf.push_back((char)('0' + (corrected ? label : 0))); }
-        buf.push_back('\n');
-        buf.append(outseq.data(), (size_t)L);
-        buf.push_back('\n');
-        if (!reads.fasta) { buf.append("+\n"); buf.append(q); buf.push_back('\n'); }
-        if (buf.size() > (1u << 22)) { std::fwrite(buf.data(), 1, buf.size(), fp); buf.clear(); }
+    };
+    // blocks of reads formatted by threads, written in read order
+    const unsigned T = std::max(1u, std::thread::hardware_concurrency());
+    const uint32_t block = 1u << 20;
+    std::vector<std::string> bufs(T);
+    bool ok = true;
+    for (uint32_t b0 = 0; b0 < n && ok; b0 += block) {
+        const uint32_t b1 = (uint32_t)std::min<uint64_t>((uint64_t)b0 + block, n);
+        const unsigned use = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(T, (b1 - b0) / 1024));
+        std::vector<std::thread> th;
+        for (unsigned t = 0; t < use; t++) {
+            th.emplace_back([&, t] {
+                bufs[t].clear();
+                format(b0 + (uint32_t)((uint64_t)(b1 - b0) * t / use), b0 + (uint32_t)((uint64_t)(b1 - b0) * (t + 1) / use),
+                       bufs[t]);
+            });
+        }
+        for (auto& x : th) x.join();
+        for (unsigned t = 0; t < use && ok; t++)
+            ok = std::fwrite(bufs[t].data(), 1, bufs[t].size(), fp) == bufs[t].size();
     }
-    std::fwrite(buf.data(), 1, buf.size(), fp);
-    const bool ok = std::fclose(fp) == 0;
+    ok = (std::fclose(fp) == 0) && ok;
     return ok ? "" : "write error on " + path;
 }
 
