@@ -1196,7 +1196,20 @@ int care_b200_load_reads_from_files(care_b200_ctx* ctx, const char* const* files
                                   h.ambiguous_ids.data(), h.ambiguous_ids.size(), h.n);
 }
 
+static int care_b200_load_preprocessed_reads_impl(care_b200_ctx* ctx, const char* path);
+
+// The file formats are parsed with std::vector: an allocation failure is
+// returned as an error code, nothing is thrown across the C ABI.
 int care_b200_load_preprocessed_reads(care_b200_ctx* ctx, const char* path) {
+    if (!ctx || !path) return CARE_B200_EINVAL;
+    try {
+        return care_b200_load_preprocessed_reads_impl(ctx, path);
+    } catch (const std::exception& e) {
+        return fail(ctx, CARE_B200_ENOMEM, std::string("load_preprocessed_reads: ") + e.what());
+    }
+}
+
+static int care_b200_load_preprocessed_reads_impl(care_b200_ctx* ctx, const char* path) {
     if (!ctx || !path) return CARE_B200_EINVAL;
     ReadStorageFile f;
     const std::string e = read_storage_file(path, f);
@@ -1216,7 +1229,20 @@ int care_b200_load_preprocessed_reads(care_b200_ctx* ctx, const char* path) {
                                   f.ambiguous_ids.size(), (uint32_t)f.n);
 }
 
+static int care_b200_save_preprocessed_reads_impl(care_b200_ctx* ctx, const char* path);
+
+// The file formats are parsed with std::vector: an allocation failure is
+// returned as an error code, nothing is thrown across the C ABI.
 int care_b200_save_preprocessed_reads(care_b200_ctx* ctx, const char* path) {
+    if (!ctx || !path) return CARE_B200_EINVAL;
+    try {
+        return care_b200_save_preprocessed_reads_impl(ctx, path);
+    } catch (const std::exception& e) {
+        return fail(ctx, CARE_B200_ENOMEM, std::string("save_preprocessed_reads: ") + e.what());
+    }
+}
+
+static int care_b200_save_preprocessed_reads_impl(care_b200_ctx* ctx, const char* path) {
     if (!ctx || !path) return CARE_B200_EINVAL;
     if (ctx->n == 0) return fail(ctx, CARE_B200_ESTATE, "no reads uploaded");
     CK(cudaSetDevice(ctx->opt.device), "cudaSetDevice");
@@ -1244,7 +1270,20 @@ int care_b200_save_preprocessed_reads(care_b200_ctx* ctx, const char* path) {
     return CARE_B200_OK;
 }
 
+static int care_b200_load_hashtables_impl(care_b200_ctx* ctx, const char* path);
+
+// The file formats are parsed with std::vector: an allocation failure is
+// returned as an error code, nothing is thrown across the C ABI.
 int care_b200_load_hashtables(care_b200_ctx* ctx, const char* path) {
+    if (!ctx || !path) return CARE_B200_EINVAL;
+    try {
+        return care_b200_load_hashtables_impl(ctx, path);
+    } catch (const std::exception& e) {
+        return fail(ctx, CARE_B200_ENOMEM, std::string("load_hashtables: ") + e.what());
+    }
+}
+
+static int care_b200_load_hashtables_impl(care_b200_ctx* ctx, const char* path) {
     if (!ctx || !path) return CARE_B200_EINVAL;
     if (ctx->n == 0) return fail(ctx, CARE_B200_ESTATE, "no reads uploaded");
     MinhashTablesFile t;
@@ -1272,7 +1311,20 @@ int care_b200_load_hashtables(care_b200_ctx* ctx, const char* path) {
     return care_b200_upload_tables(ctx, maps, k.data(), o.data(), v.data(), nk.data());
 }
 
+static int care_b200_save_hashtables_impl(care_b200_ctx* ctx, const char* path);
+
+// The file formats are parsed with std::vector: an allocation failure is
+// returned as an error code, nothing is thrown across the C ABI.
 int care_b200_save_hashtables(care_b200_ctx* ctx, const char* path) {
+    if (!ctx || !path) return CARE_B200_EINVAL;
+    try {
+        return care_b200_save_hashtables_impl(ctx, path);
+    } catch (const std::exception& e) {
+        return fail(ctx, CARE_B200_ENOMEM, std::string("save_hashtables: ") + e.what());
+    }
+}
+
+static int care_b200_save_hashtables_impl(care_b200_ctx* ctx, const char* path) {
     if (!ctx || !path) return CARE_B200_EINVAL;
     if (!ctx->tables_ready) return fail(ctx, CARE_B200_ESTATE, "no tables uploaded or built");
     MinhashTablesFile t;

@@ -30,7 +30,18 @@ bool get(std::istream& s, T& v) { return (bool)s.read(reinterpret_cast<char*>(&v
 template <class T>
 void put(std::ostream& s, const T& v) { s.write(reinterpret_cast<const char*>(&v), sizeof(T)); }
 
+// Bytes left in the stream: sizes read from a file are checked against it
+// before anything is allocated.
+uint64_t remaining(std::istream& s) {
+    const auto here = s.tellg();
+    s.seekg(0, std::ios::end);
+    const auto end = s.tellg();
+    s.seekg(here);
+    return (here < 0 || end < here) ? 0 : (uint64_t)(end - here);
+}
+
 bool get_words(std::istream& s, std::vector<uint32_t>& v, uint64_t count) {
+    if (count > remaining(s) / 4) return false;
     v.resize(count);
     return count == 0 || (bool)s.read(reinterpret_cast<char*>(v.data()), count * 4);
 }
@@ -64,7 +75,7 @@ std::string read_storage_file(const std::string& path, ReadStorageFile& f) {
     uint8_t hasq = 0;
     if (!get(s, n) || !get(s, hi) || !get(s, lo) || !get(s, hasq) || !get(s, qbits)) return trunc;
     for (auto& b : bytes) if (!get(s, b)) return trunc;
-    if (n == 0 || n > std::numeric_limits<uint32_t>::max()) return path + ": read count out of range";
+    if (n == 0 || n > std::numeric_limits<uint32_t>::max() || n > remaining(s)) return path + ": read count out of range";
 
     // lengths
     int word_bits = 0, bits = 0, mn = 0, mx = 0;
@@ -95,7 +106,7 @@ std::string read_storage_file(const std::string& path, ReadStorageFile& f) {
     // sequences
     uint64_t sp = 0, sn = 0;
     if (!get(s, sp) || !get(s, sn)) return trunc;
-    if (sp == 0 || sn != n * sp || (uint64_t)mx > 16 * sp) return path + ": inconsistent sequence section";
+    if (sp == 0 || sp > (1u << 20) || sn != n * sp || (uint64_t)mx > 16 * sp) return path + ": inconsistent sequence section";
     if (!get_words(s, f.seq, sn)) return trunc;
 
     // qualities
@@ -104,7 +115,7 @@ std::string read_storage_file(const std::string& path, ReadStorageFile& f) {
     if (hasq) {
         if (qbits != 1 && qbits != 2 && qbits != 8) return path + ": quality bits must be 1, 2 or 8";
         const uint64_t per = 32 / qbits;
-        if (qn != n * qp || (uint64_t)mx > per * qp) return path + ": inconsistent quality section";
+        if (qp > (1u << 20) || qn != n * qp || (uint64_t)mx > per * qp) return path + ": inconsistent quality section";
         if (!get_words(s, f.qual, qn)) return trunc;
     } else {
         if (qn != 0) s.seekg((std::streamoff)(qn * 4), std::ios::cur);
@@ -203,7 +214,7 @@ std::string read_tables_file(const std::string& path, MinhashTablesFile& t, int 
         uint64_t nk = 0, probes = 0, size = 0, cap = 0, nslots = 0;
         if (!get(s, load) || !get(s, nk) || !get(s, probes) || !get(s, size) || !get(s, cap) || !get(s, nslots))
             return trunc;
-        if (nslots != cap || nk > cap) return path + ": inconsistent key index";
+        if (nslots != cap || nk > cap || nslots > remaining(s) / sizeof(IndexSlot)) return path + ": inconsistent key index";
         std::vector<IndexSlot> slots(nslots);
         if (nslots && !s.read(reinterpret_cast<char*>(slots.data()), nslots * sizeof(IndexSlot))) return trunc;
         std::vector<IndexSlot> used;

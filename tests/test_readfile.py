@@ -262,3 +262,29 @@ def test_parallel_scan_falls_back_on_irregular_files(tmp_path):
     f.write_text("".join(broken))
     ref = digest(str(f), threads=1)
     assert digest(str(f), threads=8) == ref
+
+
+def test_sizes_beyond_the_file_are_rejected(tmp_path):
+    """Counts in a damaged header that the file cannot hold are rejected
+    before anything is allocated."""
+    p = unpack(str(tmp_path), "pre_un")
+    b = bytearray(open(p["bin"], "rb").read())
+    for off, val in ((0, 2 ** 32 - 1), (0, 10 ** 9)):                 # read count
+        bad = bytearray(b)
+        struct.pack_into("<Q", bad, off, val)
+        q = tmp_path / "bad.bin"
+        q.write_bytes(bytes(bad))
+        info = (U64 * 8)()
+        err = ctypes.create_string_buffer(256)
+        assert not H.rf_load(str(q).encode(), info, err, 256)
+    t = bytearray(gzip.decompress(open(os.path.join(GOLD, "pre_pe_h4.tables.gz"), "rb").read()))
+    nv = struct.unpack_from("<Q", t, 16)[0]
+    slots_at = 16 + 8 + 4 * nv + 4 + 8 * 4                             # u64 slots of map 0's index
+    struct.pack_into("<Q", t, slots_at, 2 ** 40)
+    struct.pack_into("<Q", t, slots_at - 8, 2 ** 40)                   # capacity to match
+    q = tmp_path / "bad.tables"
+    q.write_bytes(bytes(t))
+    info = (U64 * 4)()
+    err = ctypes.create_string_buffer(256)
+    assert not H.rt_load(str(q).encode(), 64, info, err, 256)
+    assert b"inconsistent key index" in err.value
