@@ -303,7 +303,19 @@ void care_b200_default_options(care_b200_options* o) {
     o->clf_min_coverage = 3;
 }
 
+static int care_b200_create_impl(const care_b200_options* opt, care_b200_ctx** out);
+
+// host allocations that fail are returned as CARE_B200_ENOMEM: nothing is
+// thrown across the C ABI
 int care_b200_create(const care_b200_options* opt, care_b200_ctx** out) {
+    try {
+        return care_b200_create_impl(opt, out);
+    } catch (const std::exception&) {
+        return CARE_B200_ENOMEM;
+    }
+}
+
+static int care_b200_create_impl(const care_b200_options* opt, care_b200_ctx** out) {
     if (!opt || !out) return CARE_B200_EINVAL;
     *out = nullptr;
     auto c = std::make_unique<care_b200_ctx>();
@@ -347,7 +359,23 @@ const char* care_b200_last_error(const care_b200_ctx* ctx) {
     return ctx ? ctx->err.c_str() : "no context";
 }
 
+static int care_b200_upload_reads_impl(care_b200_ctx* ctx, const uint32_t* packed, size_t pitch_ints,
+                           const int32_t* lengths, const uint32_t* enc_quals, size_t qual_pitch_ints,
+                           const uint32_t* ambiguous_ids, size_t num_ambiguous, uint32_t num_reads);
+
+// host allocations that fail are returned as CARE_B200_ENOMEM: nothing is
+// thrown across the C ABI
 int care_b200_upload_reads(care_b200_ctx* ctx, const uint32_t* packed, size_t pitch_ints,
+                           const int32_t* lengths, const uint32_t* enc_quals, size_t qual_pitch_ints,
+                           const uint32_t* ambiguous_ids, size_t num_ambiguous, uint32_t num_reads) {
+    try {
+        return care_b200_upload_reads_impl(ctx, packed, pitch_ints, lengths, enc_quals, qual_pitch_ints, ambiguous_ids, num_ambiguous, num_reads);
+    } catch (const std::exception& e) {
+        return ctx ? fail(ctx, CARE_B200_ENOMEM, std::string("care_b200_upload_reads: ") + e.what()) : CARE_B200_ENOMEM;
+    }
+}
+
+static int care_b200_upload_reads_impl(care_b200_ctx* ctx, const uint32_t* packed, size_t pitch_ints,
                            const int32_t* lengths, const uint32_t* enc_quals, size_t qual_pitch_ints,
                            const uint32_t* ambiguous_ids, size_t num_ambiguous, uint32_t num_reads) {
     if (!ctx) return CARE_B200_EINVAL;
@@ -394,7 +422,23 @@ int care_b200_upload_reads(care_b200_ctx* ctx, const uint32_t* packed, size_t pi
     return CARE_B200_OK;
 }
 
+static int care_b200_upload_tables_impl(care_b200_ctx* ctx, int num_maps, const uint64_t* const* keys,
+                            const uint32_t* const* offsets, const uint32_t* const* values,
+                            const size_t* nkeys);
+
+// host allocations that fail are returned as CARE_B200_ENOMEM: nothing is
+// thrown across the C ABI
 int care_b200_upload_tables(care_b200_ctx* ctx, int num_maps, const uint64_t* const* keys,
+                            const uint32_t* const* offsets, const uint32_t* const* values,
+                            const size_t* nkeys) {
+    try {
+        return care_b200_upload_tables_impl(ctx, num_maps, keys, offsets, values, nkeys);
+    } catch (const std::exception& e) {
+        return ctx ? fail(ctx, CARE_B200_ENOMEM, std::string("care_b200_upload_tables: ") + e.what()) : CARE_B200_ENOMEM;
+    }
+}
+
+static int care_b200_upload_tables_impl(care_b200_ctx* ctx, int num_maps, const uint64_t* const* keys,
                             const uint32_t* const* offsets, const uint32_t* const* values,
                             const size_t* nkeys) {
     if (!ctx) return CARE_B200_EINVAL;
@@ -451,7 +495,19 @@ int care_b200_upload_tables(care_b200_ctx* ctx, int num_maps, const uint64_t* co
     return CARE_B200_OK;
 }
 
+static int care_b200_build_tables_impl(care_b200_ctx* ctx);
+
+// host allocations that fail are returned as CARE_B200_ENOMEM: nothing is
+// thrown across the C ABI
 int care_b200_build_tables(care_b200_ctx* ctx) {
+    try {
+        return care_b200_build_tables_impl(ctx);
+    } catch (const std::exception& e) {
+        return ctx ? fail(ctx, CARE_B200_ENOMEM, std::string("care_b200_build_tables: ") + e.what()) : CARE_B200_ENOMEM;
+    }
+}
+
+static int care_b200_build_tables_impl(care_b200_ctx* ctx) {
     if (!ctx) return CARE_B200_EINVAL;
     if (ctx->n == 0) return fail(ctx, CARE_B200_ESTATE, "no reads uploaded");
     CK(cudaSetDevice(ctx->opt.device), "cudaSetDevice");
@@ -545,7 +601,21 @@ int care_b200_build_tables(care_b200_ctx* ctx) {
     return care_b200_upload_tables(ctx, h, kp.data(), op.data(), vp.data(), nk.data());
 }
 
+static int care_b200_get_table_impl(care_b200_ctx* ctx, int map, const uint64_t** keys, const uint32_t** offsets,
+                        const uint32_t** values, size_t* nkeys);
+
+// host allocations that fail are returned as CARE_B200_ENOMEM: nothing is
+// thrown across the C ABI
 int care_b200_get_table(care_b200_ctx* ctx, int map, const uint64_t** keys, const uint32_t** offsets,
+                        const uint32_t** values, size_t* nkeys) {
+    try {
+        return care_b200_get_table_impl(ctx, map, keys, offsets, values, nkeys);
+    } catch (const std::exception& e) {
+        return ctx ? fail(ctx, CARE_B200_ENOMEM, std::string("care_b200_get_table: ") + e.what()) : CARE_B200_ENOMEM;
+    }
+}
+
+static int care_b200_get_table_impl(care_b200_ctx* ctx, int map, const uint64_t** keys, const uint32_t** offsets,
                         const uint32_t** values, size_t* nkeys) {
     if (!ctx) return CARE_B200_EINVAL;
     if (!ctx->tables_ready || map < 0 || map >= ctx->num_maps) return fail(ctx, CARE_B200_EINVAL, "no such table");
@@ -1062,11 +1132,35 @@ int correct_impl(care_b200_ctx* ctx, uint32_t first, uint32_t count, care_b200_r
 
 extern "C" {
 
+static int care_b200_correct_range_impl(care_b200_ctx* ctx, uint32_t first, uint32_t count, care_b200_results* res);
+
+// host allocations that fail are returned as CARE_B200_ENOMEM: nothing is
+// thrown across the C ABI
 int care_b200_correct_range(care_b200_ctx* ctx, uint32_t first, uint32_t count, care_b200_results* res) {
+    try {
+        return care_b200_correct_range_impl(ctx, first, count, res);
+    } catch (const std::exception& e) {
+        return ctx ? fail(ctx, CARE_B200_ENOMEM, std::string("care_b200_correct_range: ") + e.what()) : CARE_B200_ENOMEM;
+    }
+}
+
+static int care_b200_correct_range_impl(care_b200_ctx* ctx, uint32_t first, uint32_t count, care_b200_results* res) {
     return correct_impl(ctx, first, count, res, true);
 }
 
+static int care_b200_correct_range_device_impl(care_b200_ctx* ctx, uint32_t first, uint32_t count);
+
+// host allocations that fail are returned as CARE_B200_ENOMEM: nothing is
+// thrown across the C ABI
 int care_b200_correct_range_device(care_b200_ctx* ctx, uint32_t first, uint32_t count) {
+    try {
+        return care_b200_correct_range_device_impl(ctx, first, count);
+    } catch (const std::exception& e) {
+        return ctx ? fail(ctx, CARE_B200_ENOMEM, std::string("care_b200_correct_range_device: ") + e.what()) : CARE_B200_ENOMEM;
+    }
+}
+
+static int care_b200_correct_range_device_impl(care_b200_ctx* ctx, uint32_t first, uint32_t count) {
     return correct_impl(ctx, first, count, nullptr, false);
 }
 
@@ -1098,7 +1192,19 @@ int care_b200_get_tuning(const care_b200_ctx* ctx, care_b200_tuning* t) {
     return CARE_B200_OK;
 }
 
+static int care_b200_set_mlp_impl(care_b200_ctx* ctx, const float* params);
+
+// host allocations that fail are returned as CARE_B200_ENOMEM: nothing is
+// thrown across the C ABI
 int care_b200_set_mlp(care_b200_ctx* ctx, const float* params) {
+    try {
+        return care_b200_set_mlp_impl(ctx, params);
+    } catch (const std::exception& e) {
+        return ctx ? fail(ctx, CARE_B200_ENOMEM, std::string("care_b200_set_mlp: ") + e.what()) : CARE_B200_ENOMEM;
+    }
+}
+
+static int care_b200_set_mlp_impl(care_b200_ctx* ctx, const float* params) {
     if (!ctx || !params) return CARE_B200_EINVAL;
     for (int i = 0; i < kMlpFloats; i++)
         if (!std::isfinite(params[i])) return fail(ctx, CARE_B200_EINVAL, "non-finite network parameter");
@@ -1109,7 +1215,21 @@ int care_b200_set_mlp(care_b200_ctx* ctx, const float* params) {
     return CARE_B200_OK;
 }
 
+static int care_b200_collect_features_impl(care_b200_ctx* ctx, uint32_t first, uint32_t count, care_b200_results* res,
+                               care_b200_features* feats);
+
+// host allocations that fail are returned as CARE_B200_ENOMEM: nothing is
+// thrown across the C ABI
 int care_b200_collect_features(care_b200_ctx* ctx, uint32_t first, uint32_t count, care_b200_results* res,
+                               care_b200_features* feats) {
+    try {
+        return care_b200_collect_features_impl(ctx, first, count, res, feats);
+    } catch (const std::exception& e) {
+        return ctx ? fail(ctx, CARE_B200_ENOMEM, std::string("care_b200_collect_features: ") + e.what()) : CARE_B200_ENOMEM;
+    }
+}
+
+static int care_b200_collect_features_impl(care_b200_ctx* ctx, uint32_t first, uint32_t count, care_b200_results* res,
                                care_b200_features* feats) {
     if (!ctx || !feats) return CARE_B200_EINVAL;
     ctx->collect = true;
@@ -1125,7 +1245,21 @@ int care_b200_collect_features(care_b200_ctx* ctx, uint32_t first, uint32_t coun
     return CARE_B200_OK;
 }
 
+static int care_b200_serialize_results_impl(care_b200_ctx* ctx, const care_b200_results* res, uint8_t* out,
+                                size_t capacity, size_t* needed);
+
+// host allocations that fail are returned as CARE_B200_ENOMEM: nothing is
+// thrown across the C ABI
 int care_b200_serialize_results(care_b200_ctx* ctx, const care_b200_results* res, uint8_t* out,
+                                size_t capacity, size_t* needed) {
+    try {
+        return care_b200_serialize_results_impl(ctx, res, out, capacity, needed);
+    } catch (const std::exception& e) {
+        return ctx ? fail(ctx, CARE_B200_ENOMEM, std::string("care_b200_serialize_results: ") + e.what()) : CARE_B200_ENOMEM;
+    }
+}
+
+static int care_b200_serialize_results_impl(care_b200_ctx* ctx, const care_b200_results* res, uint8_t* out,
                                 size_t capacity, size_t* needed) {
     if (!ctx || !res || !needed) return CARE_B200_EINVAL;
     size_t pos = 0;
@@ -1182,7 +1316,19 @@ int care_b200_serialize_results(care_b200_ctx* ctx, const care_b200_results* res
     return CARE_B200_OK;
 }
 
+static int care_b200_load_reads_from_files_impl(care_b200_ctx* ctx, const char* const* files, int num_files);
+
+// host allocations that fail are returned as CARE_B200_ENOMEM: nothing is
+// thrown across the C ABI
 int care_b200_load_reads_from_files(care_b200_ctx* ctx, const char* const* files, int num_files) {
+    try {
+        return care_b200_load_reads_from_files_impl(ctx, files, num_files);
+    } catch (const std::exception& e) {
+        return ctx ? fail(ctx, CARE_B200_ENOMEM, std::string("care_b200_load_reads_from_files: ") + e.what()) : CARE_B200_ENOMEM;
+    }
+}
+
+static int care_b200_load_reads_from_files_impl(care_b200_ctx* ctx, const char* const* files, int num_files) {
     if (!ctx || !files || num_files < 1 || num_files > 2) return CARE_B200_EINVAL;
     std::vector<std::string> fs;
     for (int i = 0; i < num_files; i++) fs.emplace_back(files[i]);
@@ -1346,7 +1492,19 @@ static int care_b200_save_hashtables_impl(care_b200_ctx* ctx, const char* path) 
     return CARE_B200_OK;
 }
 
+static int care_b200_write_output_impl(care_b200_ctx* ctx, const char* outfile);
+
+// host allocations that fail are returned as CARE_B200_ENOMEM: nothing is
+// thrown across the C ABI
 int care_b200_write_output(care_b200_ctx* ctx, const char* outfile) {
+    try {
+        return care_b200_write_output_impl(ctx, outfile);
+    } catch (const std::exception& e) {
+        return ctx ? fail(ctx, CARE_B200_ENOMEM, std::string("care_b200_write_output: ") + e.what()) : CARE_B200_ENOMEM;
+    }
+}
+
+static int care_b200_write_output_impl(care_b200_ctx* ctx, const char* outfile) {
     if (!ctx || !outfile) return CARE_B200_EINVAL;
     if (!ctx->have_records) return fail(ctx, CARE_B200_ESTATE, "reads were not loaded from files");
     if (!ctx->r_valid) return fail(ctx, CARE_B200_ESTATE, "no correction results");

@@ -577,7 +577,19 @@ void care_b200_mlp_default_train_options(care_b200_mlp_train_options* o) {
     o->seed = 1;
 }
 
+static int care_b200_mlp_create_impl(int device, care_b200_mlp** out);
+
+// host allocations that fail are returned as CARE_B200_ENOMEM: nothing is
+// thrown across the C ABI
 int care_b200_mlp_create(int device, care_b200_mlp** out) {
+    try {
+        return care_b200_mlp_create_impl(device, out);
+    } catch (const std::exception&) {
+        return CARE_B200_ENOMEM;
+    }
+}
+
+static int care_b200_mlp_create_impl(int device, care_b200_mlp** out) {
     if (!out) return CARE_B200_EINVAL;
     *out = nullptr;
     auto h = std::make_unique<care_b200_mlp>();
@@ -653,7 +665,21 @@ int care_b200_mlp_init(care_b200_mlp* m, uint64_t seed) {
     return care_b200_mlp_set_params(m, p.data());
 }
 
+static int care_b200_mlp_set_data_impl(care_b200_mlp* m, const float* x, const float* labels, const float* weights, uint64_t n,
+                           int set_norm);
+
+// host allocations that fail are returned as CARE_B200_ENOMEM: nothing is
+// thrown across the C ABI
 int care_b200_mlp_set_data(care_b200_mlp* m, const float* x, const float* labels, const float* weights, uint64_t n,
+                           int set_norm) {
+    try {
+        return care_b200_mlp_set_data_impl(m, x, labels, weights, n, set_norm);
+    } catch (const std::exception& e) {
+        return m ? mfail(m, CARE_B200_ENOMEM, std::string("care_b200_mlp_set_data: ") + e.what()) : CARE_B200_ENOMEM;
+    }
+}
+
+static int care_b200_mlp_set_data_impl(care_b200_mlp* m, const float* x, const float* labels, const float* weights, uint64_t n,
                            int set_norm) {
     if (!m || !x || !labels || n == 0) return CARE_B200_EINVAL;
     if (n > 0xFFFFFFFFull) return mfail(m, CARE_B200_ELIMIT, "more than 2^32 rows");
@@ -694,7 +720,21 @@ int care_b200_mlp_set_data(care_b200_mlp* m, const float* x, const float* labels
     return CARE_B200_OK;
 }
 
+static int care_b200_mlp_gradient_impl(care_b200_mlp* m, const float* x, const float* labels, const float* weights, uint64_t n,
+                           float* grad, float* loss);
+
+// host allocations that fail are returned as CARE_B200_ENOMEM: nothing is
+// thrown across the C ABI
 int care_b200_mlp_gradient(care_b200_mlp* m, const float* x, const float* labels, const float* weights, uint64_t n,
+                           float* grad, float* loss) {
+    try {
+        return care_b200_mlp_gradient_impl(m, x, labels, weights, n, grad, loss);
+    } catch (const std::exception& e) {
+        return m ? mfail(m, CARE_B200_ENOMEM, std::string("care_b200_mlp_gradient: ") + e.what()) : CARE_B200_ENOMEM;
+    }
+}
+
+static int care_b200_mlp_gradient_impl(care_b200_mlp* m, const float* x, const float* labels, const float* weights, uint64_t n,
                            float* grad, float* loss) {
     if (!m || !x || !labels || n == 0 || !grad) return CARE_B200_EINVAL;
     MCK(cudaSetDevice(m->device), "cudaSetDevice");
@@ -709,7 +749,21 @@ int care_b200_mlp_gradient(care_b200_mlp* m, const float* x, const float* labels
     return CARE_B200_OK;
 }
 
+static int care_b200_mlp_train_step_impl(care_b200_mlp* m, const float* x, const float* labels, const float* weights,
+                             uint64_t n, const care_b200_mlp_train_options* o, float* loss);
+
+// host allocations that fail are returned as CARE_B200_ENOMEM: nothing is
+// thrown across the C ABI
 int care_b200_mlp_train_step(care_b200_mlp* m, const float* x, const float* labels, const float* weights,
+                             uint64_t n, const care_b200_mlp_train_options* o, float* loss) {
+    try {
+        return care_b200_mlp_train_step_impl(m, x, labels, weights, n, o, loss);
+    } catch (const std::exception& e) {
+        return m ? mfail(m, CARE_B200_ENOMEM, std::string("care_b200_mlp_train_step: ") + e.what()) : CARE_B200_ENOMEM;
+    }
+}
+
+static int care_b200_mlp_train_step_impl(care_b200_mlp* m, const float* x, const float* labels, const float* weights,
                              uint64_t n, const care_b200_mlp_train_options* o, float* loss) {
     if (!m || !x || !labels || n == 0 || !o) return CARE_B200_EINVAL;
     MCK(cudaSetDevice(m->device), "cudaSetDevice");
@@ -726,7 +780,21 @@ int care_b200_mlp_train_step(care_b200_mlp* m, const float* x, const float* labe
     return CARE_B200_OK;
 }
 
+static int care_b200_mlp_train_impl(care_b200_mlp* m, const care_b200_mlp_train_options* o, float* losses,
+                        uint64_t loss_capacity, uint64_t* num_steps);
+
+// host allocations that fail are returned as CARE_B200_ENOMEM: nothing is
+// thrown across the C ABI
 int care_b200_mlp_train(care_b200_mlp* m, const care_b200_mlp_train_options* o, float* losses,
+                        uint64_t loss_capacity, uint64_t* num_steps) {
+    try {
+        return care_b200_mlp_train_impl(m, o, losses, loss_capacity, num_steps);
+    } catch (const std::exception& e) {
+        return m ? mfail(m, CARE_B200_ENOMEM, std::string("care_b200_mlp_train: ") + e.what()) : CARE_B200_ENOMEM;
+    }
+}
+
+static int care_b200_mlp_train_impl(care_b200_mlp* m, const care_b200_mlp_train_options* o, float* losses,
                         uint64_t loss_capacity, uint64_t* num_steps) {
     if (!m || !o || o->epochs < 1 || o->batch < 1) return CARE_B200_EINVAL;
     if (m->n_train == 0) return mfail(m, CARE_B200_ESTATE, "no training rows");
@@ -778,7 +846,19 @@ int care_b200_mlp_train(care_b200_mlp* m, const care_b200_mlp_train_options* o, 
     return CARE_B200_OK;
 }
 
+static int care_b200_mlp_forward_impl(care_b200_mlp* m, const float* x, uint64_t n, float* logits);
+
+// host allocations that fail are returned as CARE_B200_ENOMEM: nothing is
+// thrown across the C ABI
 int care_b200_mlp_forward(care_b200_mlp* m, const float* x, uint64_t n, float* logits) {
+    try {
+        return care_b200_mlp_forward_impl(m, x, n, logits);
+    } catch (const std::exception& e) {
+        return m ? mfail(m, CARE_B200_ENOMEM, std::string("care_b200_mlp_forward: ") + e.what()) : CARE_B200_ENOMEM;
+    }
+}
+
+static int care_b200_mlp_forward_impl(care_b200_mlp* m, const float* x, uint64_t n, float* logits) {
     if (!m || !x || !logits) return CARE_B200_EINVAL;
     if (n == 0) return CARE_B200_OK;
     MCK(cudaSetDevice(m->device), "cudaSetDevice");
