@@ -58,3 +58,20 @@ def test_tuning_struct_and_default():
     from care_b200 import autotune
     assert care_b200.Tuning.from_dict({}).as_dict() == autotune.DEFAULT
     assert set(autotune.KNOBS) <= set(fields)
+
+
+def test_cli_lists_care_cpu_options():
+    """The drop-in binary accepts care-cpu's option names (the usage text, no
+    GPU needed) and rejects unknown options."""
+    out = subprocess.run([care_b200.CLI_PATH, "--help"], capture_output=True, text=True)
+    assert out.returncode == 0
+    text = out.stdout + out.stderr
+    for opt in ("--kmerlength", "--hashmaps", "--useQualityScores", "--qualityScoreBits", "--excludeAmbiguous",
+                "--candidateCorrection", "--candidateCorrectionNewColumns", "--minalignmentoverlap",
+                "--maxmismatchratio", "--minalignmentoverlapratio", "--errorfactortuning", "--coveragefactortuning",
+                "--pairedFilterThreshold", "--correctionQualityLabels", "--correctionType",
+                "--save-preprocessedreads-to", "--load-preprocessedreads-from", "--save-hashtables-to",
+                "--load-hashtables-from"):
+        assert opt in text, opt
+    bad = subprocess.run([care_b200.CLI_PATH, "--no-such-option"], capture_output=True, text=True)
+    assert bad.returncode != 0 and "unknown option" in bad.stderr
