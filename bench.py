@@ -16,8 +16,10 @@ src/dispatch_care_correct_cpu.cpp:157-168; reads/s = reads / STEP2 time).
           storage (care_b200_upload_reads) + correction with the results
           copied back to host memory (care_b200_correct_range), wall clock.
   --impl reference : the reference's care-cpu (built from its sources by
-          oracle/Makefile) on all host cores, on a bounded sample of the
-          workload (same model, 1.25 Mbp genome, 250,000 reads).
+          oracle/Makefile) on all host cores, on the same read set and
+          options; one care-cpu run per step (~15 s on 16 cores).
+  parity : the plain method's corrected FASTQ (untimed, after the timed
+          steps) against care-cpu's output of the same file, by SHA-256.
   learned : the same steps with the learned decision (correction_type 1,
           network parameters care_b200/data/mlp_pe30x.bin, trained by
           `python -m care_b200.learned` on three other seeded genomes), and
@@ -76,48 +78,6 @@ def workload(rank: int, genome_size: int, kind: str = "pe"):
     rs = datagen.paired_end_repeats(seed=2 + 1000 * rank, genome_size=genome_size,
                                     repeat_unit=max(100, genome_size // 1000))
     return rs
-
-
-def write_fastq_fast(rs, path):
-    n, W = rs.num_reads, rs.seqs.shape[1]
-    if (rs.lengths == W).all() and n > 2_000_000:
-        return write_fastq_fixed(rs, path)
-    lens = rs.lengths
-    seqs = rs.seqs.tobytes()
-    quals = rs.quals.tobytes()
-    with open(path, "wb") as f:
-        chunk = 100_000
-        for b in range(0, n, chunk):
-            parts = []
-            for i in range(b, min(n, b + chunk)):
-                o, L = i * W, int(lens[i])
-                parts += [b"@r%d\n" % i, seqs[o:o + L], b"\n+\n", quals[o:o + L], b"\n"]
-            f.write(b"".join(parts))
-
-
-def write_fastq_fixed(rs, path, chunk: int = 1_000_000):
-    """Fixed-length reads as 4-line FASTQ records built in bulk: header
-    "@r<id, 10 digits>", sequence, "+", qualities."""
-    n, L = rs.seqs.shape
-    rec = 17 + 2 * L
-    with open(path, "wb") as f:
-        for b in range(0, n, chunk):
-            e = min(n, b + chunk)
-            m = e - b
-            buf = np.empty((m, rec), np.uint8)
-            ids = np.arange(b, e, dtype=np.int64)
-            buf[:, 0] = ord("@")
-            buf[:, 1] = ord("r")
-            for d in range(10):
-                buf[:, 11 - d] = ord("0") + (ids // 10 ** d) % 10
-            buf[:, 12] = ord("\n")
-            buf[:, 13:13 + L] = rs.seqs[b:e]
-            buf[:, 13 + L] = ord("\n")
-            buf[:, 14 + L] = ord("+")
-            buf[:, 15 + L] = ord("\n")
-            buf[:, 16 + L:16 + 2 * L] = rs.quals[b:e]
-            buf[:, 16 + 2 * L] = ord("\n")
-            f.write(buf.tobytes())
 
 
 def encode_quality_2bit(quals: np.ndarray) -> np.ndarray:
@@ -208,48 +168,73 @@ def cpu_model() -> str:
     return "unknown"
 
 
-def care_cpu_sample(tmpdir: str, threads: int, genome: int = 1_250_000):
-    """care-cpu on the bounded sample (the bench model on a `genome`-bp
-    genome, 250,000 reads at the default size); returns reads/s from its
-    STEP2 line."""
+def care_cpu_run(fq: str, tmpdir: str, threads: int, args: str, out: str = "cpu_out.fq"):
+    """One care-cpu run on the FASTQ `fq` with `threads` threads; returns
+    (reads/s of its STEP2 throughput line, path of its corrected output)."""
+    cmd = [CARE_CPU, "-i", fq, "-d", tmpdir, "-o", out, "-t", str(threads)] + args.split()
+    r = subprocess.run(cmd, capture_output=True, text=True, timeout=1200)
+    if r.returncode != 0:
+        raise RuntimeError("care-cpu failed: " + r.stderr[-500:])
+    m = re.search(r"Correction throughput : ~([0-9.e+]+) reads/second", r.stdout)
+    return float(m.group(1)), os.path.join(tmpdir, out)
+
+
+def care_cpu_sample(tmpdir: str, threads: int, genome: int = 250_000):
+    """care-cpu on a small sample of the paired-end model (`genome`-bp genome,
+    50,000 reads at the default size): the one-thread rate."""
     from care_b200 import datagen
     path = os.path.join(tmpdir, f"sample_{genome}.fq")
     if not os.path.exists(path):
         rs = datagen.paired_end_repeats(seed=7, genome_size=genome, repeat_unit=max(250, genome // 1000))
-        write_fastq_fast(rs, path)
-    cmd = [CARE_CPU, "-i", path, "-d", tmpdir, "-o", "sample_out.fq", "-t", str(threads)] + ARGS.split()
-    try:
-        r = subprocess.run(cmd, capture_output=True, text=True, timeout=180)
-    except subprocess.TimeoutExpired:
-        # one run of this sample takes seconds; a stalled run is retried once
-        r = subprocess.run(cmd, capture_output=True, text=True, timeout=180)
-    if r.returncode != 0:
-        raise RuntimeError("care-cpu failed: " + r.stderr[-500:])
-    m = re.search(r"Correction throughput : ~([0-9.e+]+) reads/second", r.stdout)
-    return float(m.group(1))
+        datagen.write_fastq_fast(rs, path)
+    return care_cpu_run(path, tmpdir, threads, ARGS, out="sample_out.fq")[0]
+
+
+def workload_config(args) -> dict:
+    """The `config` keys both arms share: the workload, its reads and options."""
+    run_args = {"uneven": ARGS_UNEVEN, "large": ARGS_LARGE}.get(args.workload, ARGS)
+    g = args.genome
+    size = f"{g // 1_000_000}Mbp" if g % 1_000_000 == 0 else f"{g // 1000}kbp"
+    name = {"uneven": "se_uneven_%s_40x_50-250bp", "large": "pe_large_%s_50x_150bp_indels_N"}.get(
+        args.workload, "pe_%s_30x_150bp") % size
+    return {"workload": name, "args": run_args, "genome_bp": args.genome}
 
 
 def run_reference(args, rank, world):
+    """The reference's own care-cpu on all host cores, on the same read set
+    and options as the GPU arm (rank 0's set); one care-cpu run per step,
+    its STEP2 throughput line (src/dispatch_care_correct_cpu.cpp:168)."""
     if rank != 0:
         return
     threads = host_cores()
-    cfg = {"workload": "pe_5Mbp_30x_150bp (sample: 1.25 Mbp genome, 250,000 reads, same model)",
-           "args": ARGS, "reads_per_step": 250_000, "threads": threads}
+    cfg = workload_config(args)
     if not os.path.exists(CARE_CPU):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/care-cpu not built (make -C oracle ref)"}))
         return
+    from care_b200 import datagen
     with tempfile.TemporaryDirectory() as tmp:
-        for _ in range(args.warmup):
-            care_cpu_sample(tmp, threads)
-        vals = [care_cpu_sample(tmp, threads) for _ in range(args.steps)]
+        progress("generating reads")
+        rs = workload(0, args.genome, args.workload)
+        n = rs.num_reads
+        fq = os.path.join(tmp, "reads.fq")
+        datagen.write_fastq_fast(rs, fq)
+        del rs
+        cfg["reads_per_gpu"] = n
+        for w in range(args.warmup):
+            care_cpu_run(fq, tmp, threads, cfg["args"])
+            progress(f"care-cpu warm-up run {w} done")
+        vals = []
+        for s in range(args.steps):
+            vals.append(care_cpu_run(fq, tmp, threads, cfg["args"])[0])
+            progress(f"care-cpu timed run {s}: {vals[-1]:.0f} reads/s")
     v = float(np.median(vals))                    # median of the timed runs
+    sample = f"the whole workload ({n} reads), care-cpu -t {threads}, one run per step; median of {len(vals)} runs"
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "reads/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 250_000 / v * 1e3,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": n / v * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
             "data": "synthetic (seeded)", "config": cfg,
             "cpu_baseline": {"value": v, "unit": "reads/s", "cores": threads, "kind": "reference",
-                             "sample": cfg["workload"] + f"; median of {len(vals)} runs", "runs": vals,
-                             "cpu_model": cpu_model()},
+                             "sample": sample, "runs": vals, "cpu_model": cpu_model()},
             "e2e": {"value": v, "unit": "reads/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
 
@@ -279,6 +264,15 @@ def base_counts(rs, path):
     data = open(path, "rb").read().split(b"\n")
     corr = np.frombuffer(b"".join(data[1:4 * n:4]), np.uint8).reshape(n, L)
     return datagen.base_level_counts(rs.seqs, corr, rs.truth, rs.lengths)
+
+
+def sha256_file(path: str) -> str:
+    import hashlib
+    h = hashlib.sha256()
+    with open(path, "rb") as f:
+        for block in iter(lambda: f.read(1 << 24), b""):
+            h.update(block)
+    return h.hexdigest()
 
 
 def timed_steps(corr, n, steps, flush):
@@ -341,7 +335,8 @@ def main():
     rs = workload(rank, args.genome, args.workload)
     n = rs.num_reads
     fq = os.path.join(tmp, "reads.fq")
-    write_fastq_fast(rs, fq)
+    from care_b200 import datagen
+    datagen.write_fastq_fast(rs, fq)
 
     opts = care_b200.options_from_args(run_args, device=local)
     corr = care_b200.Corrector(opts)
@@ -378,6 +373,14 @@ def main():
         ms = float(t.item())
     value = world * n / (ms / 1e3)
 
+    # the corrected FASTQ of the plain method (untimed): its digest for the
+    # comparison with care-cpu's output of the same file, and its base counts
+    progress("plain output")
+    corr.correct_range(0, n)
+    plain_out = os.path.join(tmp, "plain.fq")
+    corr.write_output(plain_out)
+    plain_sha = sha256_file(plain_out)
+
     # the learned decision on the same reads: device time of the same steps,
     # then base-level counts of both forms against the true reads
     learned = None
@@ -405,12 +408,15 @@ def main():
         progress("learned form timed; base-level counts")
         counts = {}
         for name, c in (("plain", corr), ("learned", mcorr)):
-            c.correct_range(0, n)
-            out = os.path.join(tmp, f"{name}.fq")
-            c.write_output(out)
+            out = plain_out
+            if c is mcorr:
+                c.correct_range(0, n)
+                out = os.path.join(tmp, f"{name}.fq")
+                c.write_output(out)
             tp, fp, fn, tn = base_counts(rs, out)
             counts[name] = {"tp": tp, "fp": fp, "fn": fn, "f1": datagen.f1(tp, fp, fn)}
-            os.unlink(out)
+            if c is mcorr:
+                os.unlink(out)
         mcorr.close()
         mvalue = world * n / (mms / 1e3)
         learned = {"value": mvalue, "unit": "reads/s", "ms_per_step": mms, "ratio_vs_plain": mvalue / value,
@@ -470,10 +476,8 @@ def main():
         "metric": METRIC, "value": value, "unit": "reads/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded), " + rs.name,
-        "config": {"workload": ("se_uneven_%dMbp_40x_50-250bp" % (args.genome // 1_000_000)) if uneven
-                   else ("pe_large_%dMbp_50x_150bp_indels_N" % (args.genome // 1_000_000)) if large
-                   else "pe_5Mbp_30x_150bp", "reads_per_gpu": n, "args": run_args,
-                   "genome_bp": args.genome, "l2": "flushed between steps (252 MB write); working set > L2",
+        "config": {**workload_config(args), "reads_per_gpu": n,
+                   "l2": "flushed between steps (252 MB write); working set > L2",
                    "parallelism": f"replicas x{world} (independent read sets)",
                    "stage_ms": {"candidates": stage[0], "align": stage[1], "msa": stage[2]},
                    "pairs_per_step": stats["pairs"], "wall_ms_per_step": wall_ms,
@@ -517,18 +521,29 @@ def main():
     }
     if learned is not None:
         line["learned"] = learned
-    if rank == 0 and world == 1 and not args.no_cpu_baseline and args.workload == "pe" and os.path.exists(CARE_CPU):
+    line["parity"] = {"checked": False, "gpu_sha256": plain_sha}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and os.path.exists(CARE_CPU):
+        # care-cpu on all host cores on the same FASTQ with the same options:
+        # the reported baseline, and the byte comparison of the two outputs
         threads = host_cores()
-        progress(f"e2e done; care-cpu sample on {threads} threads")
-        runs = [care_cpu_sample(tmp, threads) for _ in range(3)]
+        progress(f"e2e done; care-cpu on the same {n} reads, {threads} threads")
+        runs, cpu_sha = [], None
+        for r in range(3):
+            v, out = care_cpu_run(fq, tmp, threads, run_args)
+            runs.append(v)
+            if cpu_sha is None:
+                cpu_sha = sha256_file(out)
+            os.unlink(out)
         v = float(np.median(runs))
+        line["parity"] = {"checked": True, "identical": cpu_sha == plain_sha, "gpu_sha256": plain_sha,
+                          "care_cpu_sha256": cpu_sha,
+                          "what": "corrected FASTQ of the plain method (tuned mapping) vs care-cpu's, same input"}
         progress("care-cpu sample on 1 thread")
-        one = care_cpu_sample(tmp, 1, genome=250_000)
+        one = care_cpu_sample(tmp, 1)
         line["cpu_baseline"] = {"value": v, "unit": "reads/s", "cores": threads, "kind": "reference",
-                                "sample": "care-cpu -t all cores on 1.25 Mbp genome, 250,000 reads, same model; "
-                                          "median of 3 runs",
+                                "sample": f"the whole workload ({n} reads), care-cpu -t {threads}; median of 3 runs",
                                 "runs": runs, "per_core_reads_s": one,
-                                "per_core_sample": "care-cpu -t 1 on 250 kbp genome, 50,000 reads, same model",
+                                "per_core_sample": "care-cpu -t 1 on 250 kbp genome, 50,000 reads, PE model",
                                 "cpu_model": cpu_model()}
     corr.close()
     shutil.rmtree(tmp, ignore_errors=True)

@@ -17,9 +17,11 @@ pytestmark = pytest.mark.gpu
 CASES = sorted(__import__("conftest").manifest()["cases"])
 
 
-def run_gpu(files, args, out=None, stats=None, **kw):
+def run_gpu(files, args, out=None, stats=None, tuning=None, **kw):
     o = care_b200.options_from_args(args, **kw)
     with care_b200.Corrector(o) as c:
+        if tuning:
+            c.tuning = tuning
         c.load_files(files)
         c.build_tables()
         res = c.correct_range()
@@ -77,13 +79,19 @@ def test_stage_outputs_match_oracle(golden, case):
     compare_with_oracle(files, m["args"], res, tables)
 
 
+@pytest.mark.parametrize("mapping", ["default", "tuned"])
 @pytest.mark.parametrize("workload,args", [
     ("pe", "-c 30 -k 20 -h 32 -q --qualityScoreBits 2 --pairmode PE --candidateCorrection"),
     ("se", "-c 30 -k 20 -h 16 --pairmode SE"),
     ("un", "-c 40 -k 20 -h 32 -q --qualityScoreBits 2 --pairmode SE --candidateCorrection"),
     ("large", "-c 50 -k 20 -h 48 -q --qualityScoreBits 2 --pairmode PE --excludeAmbiguous --candidateCorrection"),
 ])
-def test_medium_sets_match_oracle(tmp_path, workload, args):
+def test_medium_sets_match_oracle(tmp_path, workload, args, mapping):
+    """Medium sets of each workload model against the oracle, with the default
+    launch mapping and with the committed tuning of that workload."""
+    from care_b200 import autotune
+    tuning = autotune.load({"pe": "pe", "se": "pe", "un": "uneven", "large": "large"}[workload]) \
+        if mapping == "tuned" else None
     if workload == "large":
         # the large set's model: 50x, indels, N bases (ambiguous reads excluded)
         rs = datagen.paired_end_large(seed=24, genome_size=300_000, chunk_pairs=20_000)
@@ -95,7 +103,7 @@ def test_medium_sets_match_oracle(tmp_path, workload, args):
         rs = datagen.single_end_uneven(seed=23, genome_size=200_000, coverage=40)
     inp = str(tmp_path / "in.fq")
     rs.write_fastq(inp)
-    res, tables = run_gpu([inp], args)
+    res, tables = run_gpu([inp], args, tuning=tuning)
     compare_with_oracle([inp], args, res, tables)
 
 
