@@ -76,6 +76,7 @@ EXPORTS = [
     "care_b200_load_reads_from_files", "care_b200_write_output", "care_b200_last_timing",
     "care_b200_last_stats", "care_b200_count_word_compares", "care_b200_load_preprocessed_reads",
     "care_b200_save_preprocessed_reads", "care_b200_load_hashtables", "care_b200_save_hashtables", "care_b200_num_reads", "care_b200_max_length", "care_b200_num_maps",
+    "care_b200_result_threshold",
     "care_b200_correct_range_noalloc",
     "care_b200_set_mlp", "care_b200_collect_features", "care_b200_mlp_default_train_options",
     "care_b200_mlp_create", "care_b200_mlp_destroy", "care_b200_mlp_last_error", "care_b200_mlp_set_params",
@@ -89,7 +90,7 @@ class Tuning(ctypes.Structure):
     """care_b200_tuning: launch mapping of a batch (results do not depend on it)."""
     _fields_ = [("msa_order", ctypes.c_int), ("msa_queue", ctypes.c_int), ("msa_warps", ctypes.c_int),
                 ("align_block", ctypes.c_int), ("pair_order", ctypes.c_int), ("graph", ctypes.c_int),
-                ("pair_mirror", ctypes.c_int), ("cand_set_log2", ctypes.c_int)]
+                ("pair_mirror", ctypes.c_int), ("cand_set_log2", ctypes.c_int), ("align_warp", ctypes.c_int)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -139,7 +140,7 @@ class DeviceReads(ctypes.Structure):
 class DeviceTables(ctypes.Structure):
     """care_b200_device_tables: caller-owned device minhash tables."""
     _fields_ = [("num_maps", ctypes.c_int), ("descs", ctypes.c_void_p), ("slots", ctypes.c_void_p),
-                ("values", ctypes.c_void_p)]
+                ("values", ctypes.c_void_p), ("threshold", ctypes.c_int)]
 
 _lib = None
 
@@ -208,6 +209,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.care_b200_num_reads.restype = ctypes.c_uint32
     lib.care_b200_max_length.argtypes = [c_ctx]
     lib.care_b200_num_maps.argtypes = [c_ctx]
+    lib.care_b200_result_threshold.argtypes = [c_ctx]
     _lib = lib
     return lib
 
@@ -354,6 +356,11 @@ class Corrector:
     def num_maps(self) -> int:
         return int(self.lib.care_b200_num_maps(self._ctx))
 
+    @property
+    def result_threshold(self) -> int:
+        """Per-map result threshold of the tables (buckets with more ids are dropped)."""
+        return int(self.lib.care_b200_result_threshold(self._ctx))
+
     # -- correction ------------------------------------------------------------
     def correct_range_raw(self, first: int, count: int) -> Results:
         res = Results()
@@ -447,11 +454,11 @@ class Corrector:
         }
 
     def last_stats(self):
-        st = (ctypes.c_uint64 * 9)()
-        self._check(self.lib.care_b200_last_stats(self._ctx, st, 9), "last_stats")
+        st = (ctypes.c_uint64 * 11)()
+        self._check(self.lib.care_b200_last_stats(self._ctx, st, 11), "last_stats")
         return {"anchors": st[0], "pairs": st[1], "candidate_corrections": st[2], "word_compares": st[3],
                 "msa_elements": st[4], "batches": st[5], "launches": st[6], "spilled_anchors": st[7],
-                "word_compares_run": st[8]}
+                "word_compares_run": st[8], "msa_rebuild_elements": st[9], "msa_rebuilt_anchors": st[10]}
 
     def count_word_compares(self, on: bool = True):
         """Run the alignment's statistics form in the following calls: it also
@@ -464,6 +471,14 @@ class Corrector:
         st = (ctypes.c_float * 4)()
         self._check(self.lib.care_b200_last_timing(self._ctx, ctypes.byref(t), st, 4), "last_timing")
         return t.value, list(st)
+
+    def signatures_ms(self) -> float:
+        """Device ms of the last minhash-signature pass over the read storage
+        (once per uploaded or loaded storage; the correction calls reuse it)."""
+        t = ctypes.c_float()
+        st = (ctypes.c_float * 5)()
+        self._check(self.lib.care_b200_last_timing(self._ctx, ctypes.byref(t), st, 5), "last_timing")
+        return float(st[4])
 
 
 def train_options(**kw) -> TrainOptions:

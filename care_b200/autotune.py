@@ -11,6 +11,8 @@ The knobs change how a batch is laid onto the GPU, never what it computes:
 - pair_mirror (a, c) and (c, a) of equal-length anchors of a batch share one scan
 - cand_set_log2  capacity of the main candidate pass's de-duplication set
   (occupancy against anchors redone by the full-set pass)
+- align_warp  a warp per alignment work item (lanes take shifts) instead of
+  a thread per work item
 
 Coordinate descent from the default: each knob in turn takes the value with
 the lowest device time (CUDA events of the pipeline, mean of timed passes
@@ -46,9 +48,10 @@ KNOBS = {
     "graph": [0, 1],
     "pair_mirror": [0, 1],
     "cand_set_log2": [9, 10, 11],
+    "align_warp": [0, 1],
 }
 DEFAULT = {"msa_order": 0, "msa_queue": 0, "msa_warps": 4, "align_block": 128, "pair_order": 0, "graph": 0,
-           "pair_mirror": 0, "cand_set_log2": 10}
+           "pair_mirror": 0, "cand_set_log2": 10, "align_warp": 0}
 
 WORKLOADS = {
     "pe": ("-c 30 -k 20 -h 32 -q --qualityScoreBits 2 --pairmode PE", 5_000_000),

@@ -68,7 +68,7 @@ constexpr int kMsaBlock = 128;
 
 // The launch mapping of a new context: one kernel per stage in anchor order,
 // 4 MSA warps, 128-thread alignment CTAs, a 1024-entry candidate set.
-constexpr care_b200_tuning kDefaultTuning{0, 0, 4, 128, 0, 0, 0, 10};
+constexpr care_b200_tuning kDefaultTuning{0, 0, 4, 128, 0, 0, 0, 10, 0};
 
 // Largest candidate arena of one batch: pair indices and offsets are 32-bit.
 constexpr unsigned long long kMaxBatchPairs = 0xffffffffull;
@@ -78,6 +78,8 @@ struct care_b200_ctx {
     std::string err;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    cudaEvent_t sig_ev[2] = {nullptr, nullptr};    // around the last signature pass
+    bool sig_timed = false;
     float last_ms = 0.f, stage_ms[4] = {0.f, 0.f, 0.f, 0.f};
 
     // read storage
@@ -133,6 +135,7 @@ struct care_b200_ctx {
     HBuf r_status, r_nedits, r_seq;
     HBuf r_cid, r_canc, r_cshift, r_cue, r_cseq;
     uint64_t r_ncand = 0, r_pairs = 0, r_words = 0, r_elems = 0, r_batches = 0, r_launches = 0, r_spilled = 0;
+    uint64_t r_rb_elems = 0, r_rb_anchors = 0;
     uint64_t r_run_words = 0;
     bool count_words = false;         // the alignment's statistics form (care_b200_count_word_compares)
     double pairs_per_anchor = 96.0;   // seen in the last correction call (automatic batch size)
@@ -221,6 +224,7 @@ int compute_signatures(care_b200_ctx* ctx, int maps) {
     const DevReads r = make_dev_reads(ctx);
     CK(ctx->d_sigs.ensure((size_t)ctx->n * maps * 8), "alloc signatures");
     const uint32_t chunk = 1u << 20;
+    CK(cudaEventRecord(ctx->sig_ev[0], ctx->stream), "event");
     for (uint32_t b = 0; b < ctx->n; b += chunk) {
         const uint32_t cnt = std::min(chunk, ctx->n - b);
         const int wpb = 8;
@@ -228,6 +232,8 @@ int compute_signatures(care_b200_ctx* ctx, int maps) {
             o, r, b, cnt, ctx->d_sigs.as<unsigned long long>() + (size_t)b * maps);
         CK(cudaGetLastError(), "k_signatures");
     }
+    CK(cudaEventRecord(ctx->sig_ev[1], ctx->stream), "event");
+    ctx->sig_timed = true;
     ctx->sigs_maps = maps;
     return CARE_B200_OK;
 }
@@ -329,6 +335,7 @@ static int care_b200_create_impl(const care_b200_options* opt, care_b200_ctx** o
     CK(cudaSetDevice(opt->device), "cudaSetDevice");
     CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking), "cudaStreamCreate");
     for (auto& e : ctx->ev) CK(cudaEventCreate(&e), "cudaEventCreate");
+    for (auto& e : ctx->sig_ev) CK(cudaEventCreate(&e), "cudaEventCreate");
     CK(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking), "cudaStreamCreate");
     for (auto& row : ctx->stage_ev)
         for (auto& e : row) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
@@ -345,6 +352,7 @@ int care_b200_destroy(care_b200_ctx* ctx) {
     cudaSetDevice(ctx->opt.device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     for (auto& e : ctx->ev) if (e) cudaEventDestroy(e);
+    for (auto& e : ctx->sig_ev) if (e) cudaEventDestroy(e);
     if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);
     for (auto& row : ctx->stage_ev)
         for (auto& e : row) if (e) cudaEventDestroy(e);
@@ -639,10 +647,25 @@ struct AlignArgs {
     unsigned long long* words; const uint32_t* pair_order;
     const uint2* work; const unsigned int* work_n;
     unsigned long long* run_words;             // non-null: the statistics form, counting words run
+    bool warp;                                 // k_align_warp: a warp per work item
+    int sms;
 };
 
 template <int B, int NW, bool CNT>
 cudaError_t align_go(const AlignArgs& a, cudaStream_t st) {
+    if (a.warp) {
+        // persistent: the resident blocks' warps stride over the work items
+        int nb = 0;
+        const cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_align_warp<B, NW, CNT>, B, 0);
+        if (e != cudaSuccess) return e;
+        const unsigned long long need = (a.cap + B / 32 - 1) / (B / 32);
+        const unsigned grid = (unsigned)std::max<unsigned long long>(
+            1, std::min<unsigned long long>(need, (unsigned long long)a.sms * std::max(nb, 1)));
+        k_align_warp<B, NW, CNT><<<grid, B, 0, st>>>(a.o, a.r, a.first, a.cand_ids, a.cand_anchor, a.seg_off,
+                                                     a.seg_cnt, a.total, a.cap, a.status, a.out, a.words,
+                                                     a.pair_order, a.work, a.work_n, a.run_words);
+        return cudaGetLastError();
+    }
     const unsigned long long blocks = (a.cap + B - 1) / B;
     k_align<B, NW, CNT><<<(unsigned)blocks, B, 0, st>>>(a.o, a.r, a.first, a.cand_ids, a.cand_anchor, a.seg_off,
                                                         a.seg_cnt, a.total, a.cap, a.status, a.out, a.words,
@@ -749,7 +772,7 @@ int run_batch(care_b200_ctx* ctx, uint32_t first, uint32_t count, bool timed) {
     CK(ctx->d_st.ensure(count), "alloc");
     CK(ctx->d_ned.ensure((size_t)count * 4), "alloc");
     CK(ctx->d_oseq.ensure((size_t)count * ctx->max_len), "alloc");
-    CK(ctx->h_small.ensure(80), "alloc");
+    CK(ctx->h_small.ensure(96), "alloc");
     if (tu.msa_order) {
         CK(ctx->d_order.ensure((size_t)count * 4), "alloc");
         CK(ctx->d_bins.ensure(kLptBins * 4), "alloc");
@@ -819,6 +842,7 @@ int run_batch(care_b200_ctx* ctx, uint32_t first, uint32_t count, bool timed) {
         mo.feat_count = counters + 2;
         mo.feat_cap = emit ? fcap : 0;
         mo.elem_count = counters + 5;
+        mo.rebuild_count = counters + 9;             // counters 9 and 10
 
         AlignArgs aa{o, r, first, ctx->d_cand_ids.as<uint32_t>(), ctx->d_cand_anchor.as<uint32_t>(),
                      ctx->d_seg_off.as<uint32_t>(), ctx->d_seg_cnt.as<uint32_t>(), counters, cap, status,
@@ -826,7 +850,7 @@ int run_batch(care_b200_ctx* ctx, uint32_t first, uint32_t count, bool timed) {
                      tu.pair_order ? ctx->d_pair_order.as<uint32_t>() : nullptr,
                      tu.pair_mirror ? ctx->d_pair_work.as<uint2>() : nullptr,
                      reinterpret_cast<const unsigned int*>(counters + 6),
-                     ctx->count_words ? counters + 8 : nullptr};
+                     ctx->count_words ? counters + 8 : nullptr, tu.align_warp != 0, ctx->sms};
         MsaArgs ma{o, r, first, count, tu.msa_order ? ctx->d_order.as<uint32_t>() : nullptr,
                    reinterpret_cast<unsigned int*>(counters + 4), ctx->d_cand_ids.as<uint32_t>(),
                    ctx->d_seg_off.as<uint32_t>(), ctx->d_seg_cnt.as<uint32_t>(), ctx->d_ares.as<AlignRes>(),
@@ -922,10 +946,10 @@ int run_batch(care_b200_ctx* ctx, uint32_t first, uint32_t count, bool timed) {
                 launches += 3;                   // inference, verdicts, recount
             }
             EQ(mark(4), "event");
-            EQ(cudaMemcpyAsync(ctx->h_small.p, counters, 72, cudaMemcpyDeviceToHost, st), "counters");
-            EQ(cudaMemcpyAsync(ctx->h_small.as<char>() + 72, status, 4, cudaMemcpyDeviceToHost, st), "status");
+            EQ(cudaMemcpyAsync(ctx->h_small.p, counters, 88, cudaMemcpyDeviceToHost, st), "counters");
+            EQ(cudaMemcpyAsync(ctx->h_small.as<char>() + 88, status, 4, cudaMemcpyDeviceToHost, st), "status");
             if (o.clf_mode == 2)
-                EQ(cudaMemcpyAsync(ctx->h_small.as<char>() + 76, ctx->d_mlp_err.p, 4, cudaMemcpyDeviceToHost, st), "status");
+                EQ(cudaMemcpyAsync(ctx->h_small.as<char>() + 92, ctx->d_mlp_err.p, 4, cudaMemcpyDeviceToHost, st), "status");
 #undef EQ
             return CARE_B200_OK;
         };
@@ -958,7 +982,9 @@ int run_batch(care_b200_ctx* ctx, uint32_t first, uint32_t count, bool timed) {
         const unsigned long long elems = ctx->h_small.as<unsigned long long>()[5];
         const unsigned int spilled = ctx->h_small.as<unsigned int>()[14];     // counters + 7
         const unsigned long long run_words = ctx->h_small.as<unsigned long long>()[8];
-        const int stw = *(int*)(ctx->h_small.as<char>() + 72);
+        const unsigned long long rb_elems = ctx->h_small.as<unsigned long long>()[9];
+        const unsigned long long rb_anchors = ctx->h_small.as<unsigned long long>()[10];
+        const int stw = *(int*)(ctx->h_small.as<char>() + 88);
         if (stw & kStatusColumns) return fail(ctx, CARE_B200_ELIMIT, "MSA wider than the kernel's column capacity");
         bool again = false;
         if ((stw & kStatusCandOverflow) || used > cap) {
@@ -971,7 +997,7 @@ int run_batch(care_b200_ctx* ctx, uint32_t first, uint32_t count, bool timed) {
         if ((stw & kStatusCorrOverflow) || corr > ccap) { ctx->corr_cap = corr + corr / 8 + 1024; again = true; }
         if (emit && ((stw & kStatusFeatOverflow) || nfeat > fcap)) { ctx->feat_cap = nfeat + nfeat / 8 + 4096; again = true; }
         if (again) continue;
-        if (o.clf_mode == 2 && *(int*)(ctx->h_small.as<char>() + 76))
+        if (o.clf_mode == 2 && *(int*)(ctx->h_small.as<char>() + 92))
             return fail(ctx, CARE_B200_ECUDA, "tensor-core completion wait ran out");
         if (timed) {
             float a = 0, b = 0, c = 0, d = 0;
@@ -1000,6 +1026,8 @@ int run_batch(care_b200_ctx* ctx, uint32_t first, uint32_t count, bool timed) {
         ctx->r_pairs += used;
         ctx->r_words += words;
         ctx->r_elems += elems;
+        ctx->r_rb_elems += rb_elems;
+        ctx->r_rb_anchors += rb_anchors;
         ctx->r_spilled += spilled;
         ctx->r_run_words += run_words;
         return (int)std::min<unsigned long long>(corr, 0x7fffffff);
@@ -1054,6 +1082,8 @@ int correct_impl(care_b200_ctx* ctx, uint32_t first, uint32_t count, care_b200_r
     ctx->r_pairs = 0;
     ctx->r_words = 0;
     ctx->r_elems = 0;
+    ctx->r_rb_elems = 0;
+    ctx->r_rb_anchors = 0;
     ctx->r_batches = 0;
     ctx->r_launches = 0;
     ctx->r_spilled = 0;
@@ -1180,7 +1210,8 @@ int care_b200_set_tuning(care_b200_ctx* ctx, const care_b200_tuning* t) {
     if (!ctx || !t) return CARE_B200_EINVAL;
     if ((t->msa_warps != 4 && t->msa_warps != 8) || (t->align_block != 128 && t->align_block != 256) ||
         (unsigned)t->msa_order > 1 || (unsigned)t->msa_queue > 1 || (unsigned)t->pair_order > 1 ||
-        (unsigned)t->graph > 1 || (unsigned)t->pair_mirror > 1 || t->cand_set_log2 < 6 || t->cand_set_log2 > 14)
+        (unsigned)t->graph > 1 || (unsigned)t->pair_mirror > 1 || t->cand_set_log2 < 6 || t->cand_set_log2 > 14 ||
+        (unsigned)t->align_warp > 1)
         return fail(ctx, CARE_B200_EINVAL, "invalid tuning");
     ctx->tune = *t;
     return CARE_B200_OK;
@@ -1528,19 +1559,26 @@ int care_b200_last_timing(const care_b200_ctx* ctx, float* total_ms, float* stag
     if (!ctx) return CARE_B200_EINVAL;
     if (total_ms) *total_ms = ctx->last_ms;
     for (int i = 0; i < nstages && i < 4 && stage_ms; i++) stage_ms[i] = ctx->stage_ms[i];
+    if (stage_ms && nstages > 4) {
+        float ms = 0.f;
+        if (ctx->sig_timed && cudaEventSynchronize(ctx->sig_ev[1]) == cudaSuccess)
+            cudaEventElapsedTime(&ms, ctx->sig_ev[0], ctx->sig_ev[1]);
+        stage_ms[4] = ms;
+    }
     return CARE_B200_OK;
 }
 
 int care_b200_last_stats(const care_b200_ctx* ctx, uint64_t* stats, int nstats) {
     if (!ctx || !stats) return CARE_B200_EINVAL;
-    const uint64_t v[9] = {ctx->r_count, ctx->r_pairs, ctx->r_ncand, ctx->r_words, ctx->r_elems, ctx->r_batches,
-                           ctx->r_launches, ctx->r_spilled, ctx->r_run_words};
-    for (int i = 0; i < nstats && i < 9; i++) stats[i] = v[i];
+    const uint64_t v[11] = {ctx->r_count, ctx->r_pairs, ctx->r_ncand, ctx->r_words, ctx->r_elems, ctx->r_batches,
+                            ctx->r_launches, ctx->r_spilled, ctx->r_run_words, ctx->r_rb_elems, ctx->r_rb_anchors};
+    for (int i = 0; i < nstats && i < 11; i++) stats[i] = v[i];
     return CARE_B200_OK;
 }
 
 uint32_t care_b200_num_reads(const care_b200_ctx* ctx) { return ctx ? ctx->n : 0; }
 int care_b200_max_length(const care_b200_ctx* ctx) { return ctx ? ctx->max_len : 0; }
 int care_b200_num_maps(const care_b200_ctx* ctx) { return ctx ? ctx->num_maps : 0; }
+int care_b200_result_threshold(const care_b200_ctx* ctx) { return ctx ? ctx->threshold : 0; }
 
 }  // extern "C"

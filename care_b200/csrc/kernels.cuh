@@ -448,6 +448,224 @@ k_align(DevOptions o, DevReads r, uint32_t first, const uint32_t* __restrict__ c
 }
 
 // ---------------------------------------------------------------------------
+// Warp-cooperative alignment: one warp per work item, lane r of the warp
+// takes shift 32*w + r of each group w of 32 shifts (the funnel shift amount
+// is the lane; the planes slide by one word per group, as in shd_scan).
+// Every lane counts its shift's mismatches up to its own limit
+// min(int(ov * maxErrorRate), best - total + 2*ov), with `best` the score
+// found by the earlier groups, and the warp keeps the smallest key
+// (score << 10 | rank of the shift in the scan order). The result is the
+// first shift in scan order with the smallest score among the shifts whose
+// mismatches are below int(ov * maxErrorRate): the same shift the sequential
+// scan with early exits returns (src/cpu_alignment.cpp:247-316). A direction
+// ends at the first group whose leading shift can no longer reach the best
+// (its limit is <= 0 and the limit does not grow along a direction).
+// TIES: the equal-length pair form (both directions of a mirrored pair, as
+// shd_scan_ties): ties with the best are kept (limit + 1) and a second key
+// ranks the shifts in the order of the (C, A) scan.
+constexpr unsigned kKeyRankBits = 10;          // ranks and scores stay below 1024 (reads <= 256 bases)
+constexpr unsigned kKeyRankMask = (1u << kKeyRankBits) - 1u;
+
+// D0: shifts of the first direction (its ranks are t, the second's D0 + t - 1);
+// negs: the (C, A) order's count of shifts <= 0 after 0 (TIES).
+template <int NW, bool TIES, class Cnt>
+__device__ __forceinline__ void shd_scan_lanes(uint32_t (&Sh)[NW + 2], uint32_t (&Sl)[NW + 2],
+                                               const uint32_t (&Oh)[NW + 2], const uint32_t (&Ol)[NW + 2],
+                                               int t0, int t1, int dir, int La, int Lc, int total, int D0,
+                                               int negs, const int* __restrict__ mextab, unsigned& keyA,
+                                               unsigned& keyB, Cnt* cnt) {
+    if (t1 < t0) return;
+    const int lane = threadIdx.x & 31;
+    const int tie = TIES ? 1 : 0;
+    auto overlap = [&](int t) { return dir == 0 ? min(La - t, Lc) : min(La, Lc - t); };
+#pragma unroll 1
+    for (int w = 0; w <= (t1 >> 5); ++w) {
+        const int t = 32 * w + lane;
+        const int best = (int)(keyA >> kKeyRankBits);
+        unsigned ka = 0xFFFFFFFFu, kb = 0xFFFFFFFFu;
+        if (t >= t0 && t <= t1) {
+            const int ov = overlap(t);
+            const int mex = min(mextab[ov], best - total + 2 * ov + tie);
+            if (mex > 0) {
+                const int r = lane;
+                uint32_t d0 = (funnel_l(Sh[1], Sh[0], r) ^ Oh[0]) | (funnel_l(Sl[1], Sl[0], r) ^ Ol[0]);
+                uint32_t d1 = (funnel_l(Sh[2], Sh[1], r) ^ Oh[1]) | (funnel_l(Sl[2], Sl[1], r) ^ Ol[1]);
+                if (ov < 64) { d0 &= lead_mask(ov); d1 &= lead_mask(ov - 32); }
+                int mm = popc32(d0) + popc32(d1);
+                if (cnt) cnt->add(2);
+                if (mm < mex && ov > 64) {
+#pragma unroll
+                    for (int j = 2; j < NW; ++j) {
+                        if (32 * j < ov && mm < mex) {
+                            uint32_t dj = (funnel_l(Sh[j + 1], Sh[j], r) ^ Oh[j]) |
+                                          (funnel_l(Sl[j + 1], Sl[j], r) ^ Ol[j]);
+                            dj &= lead_mask(ov - 32 * j);
+                            mm += popc32(dj);
+                            if (cnt) cnt->add(1);
+                        }
+                    }
+                }
+                if (mm < mex) {
+                    const unsigned sc = (unsigned)(mm + total - 2 * ov) << kKeyRankBits;
+                    ka = sc | (unsigned)(dir == 0 ? t : D0 + t - 1);
+                    if constexpr (TIES) kb = sc | (unsigned)(dir == 0 ? (t == 0 ? 0 : negs + t) : t);
+                }
+            }
+        }
+        keyA = min(keyA, __reduce_min_sync(0xffffffffu, ka));
+        if constexpr (TIES) keyB = min(keyB, __reduce_min_sync(0xffffffffu, kb));
+        const int tn = 32 * (w + 1);
+        if (tn > t1) break;
+        {   // end of the direction: the next group's first shift cannot reach the best
+            const int ovn = overlap(tn);
+            if (min(mextab[ovn], (int)(keyA >> kKeyRankBits) - total + 2 * ovn + tie) <= 0) break;
+        }
+#pragma unroll
+        for (int j = 0; j < NW + 1; ++j) { Sh[j] = Sh[j + 1]; Sl[j] = Sl[j + 1]; }
+        Sh[NW + 1] = 0u; Sl[NW + 1] = 0u;
+    }
+}
+
+// ShdResult of a scan from its best key: shift of rank `rank`, the overlap,
+// score and mismatches (nOps) of that shift.
+__device__ __forceinline__ ShdResult shd_from_shift(int shift, int score, int La, int Lc) {
+    ShdResult res;
+    res.valid = shift != -Lc;
+    const int cb = max(-shift, 0);
+    const int ce = min(Lc, La - shift);
+    res.overlap = ce - cb;
+    res.score = score;
+    res.shift = shift;
+    res.nops = score - (La + Lc) + 2 * res.overlap;
+    return res;
+}
+
+// shifted_hamming with the warp: every lane returns the same result.
+template <int NW, class Cnt>
+__device__ __forceinline__ ShdResult shifted_hamming_lanes(const uint32_t (&Ah)[NW + 2], const uint32_t (&Al)[NW + 2],
+                                                           int La, const uint32_t (&Ch)[NW + 2],
+                                                           const uint32_t (&Cl)[NW + 2], int Lc, int minov,
+                                                           const int* __restrict__ mextab, Cnt* cnt) {
+    const int total = La + Lc;
+    const int T0 = La - minov;
+    const int D0 = T0 + 1 > 0 ? T0 + 1 : 0;      // shifts of the first direction: ranks 0..D0-1
+    unsigned keyA = ((unsigned)total << kKeyRankBits) | kKeyRankMask, keyB = 0xFFFFFFFFu;
+    uint32_t Sh[NW + 2], Sl[NW + 2];
+#pragma unroll 1
+    for (int dir = 0; dir < 2; ++dir) {
+#pragma unroll
+        for (int j = 0; j < NW + 2; ++j) { Sh[j] = dir ? Ch[j] : Ah[j]; Sl[j] = dir ? Cl[j] : Al[j]; }
+        if (dir == 0) shd_scan_lanes<NW, false>(Sh, Sl, Ch, Cl, 0, T0, 0, La, Lc, total, D0, 0, mextab, keyA, keyB, cnt);
+        else shd_scan_lanes<NW, false>(Sh, Sl, Ah, Al, 1, Lc - minov, 1, La, Lc, total, D0, 0, mextab, keyA, keyB, cnt);
+    }
+    const int score = (int)(keyA >> kKeyRankBits), rank = (int)(keyA & kKeyRankMask);
+    const int shift = score >= total ? -Lc : (rank < D0 ? rank : -(rank - D0 + 1));
+    return shd_from_shift(shift, score, La, Lc);
+}
+
+// shifted_hamming_pair with the warp: forward (A, C) and (C, A) of a pair of
+// equal length L.
+template <int NW, class Cnt>
+__device__ __forceinline__ void shifted_hamming_pair_lanes(const uint32_t (&Ah)[NW + 2], const uint32_t (&Al)[NW + 2],
+                                                           const uint32_t (&Ch)[NW + 2], const uint32_t (&Cl)[NW + 2],
+                                                           int L, int minov, const int* __restrict__ mextab,
+                                                           ShdResult& ac, ShdResult& ca, Cnt* cnt) {
+    const int total = 2 * L;
+    const int T = L - minov;
+    unsigned keyA = ((unsigned)total << kKeyRankBits) | kKeyRankMask, keyB = keyA;
+    uint32_t Sh[NW + 2], Sl[NW + 2];
+#pragma unroll 1
+    for (int dir = 0; dir < 2; ++dir) {
+#pragma unroll
+        for (int j = 0; j < NW + 2; ++j) { Sh[j] = dir ? Ch[j] : Ah[j]; Sl[j] = dir ? Cl[j] : Al[j]; }
+        if (dir == 0) shd_scan_lanes<NW, true>(Sh, Sl, Ch, Cl, 0, T, 0, L, L, total, T + 1, T, mextab, keyA, keyB, cnt);
+        else shd_scan_lanes<NW, true>(Sh, Sl, Ah, Al, 1, T, 1, L, L, total, T + 1, T, mextab, keyA, keyB, cnt);
+    }
+    const int score = (int)(keyA >> kKeyRankBits);
+    const int ra = (int)(keyA & kKeyRankMask), rb = (int)(keyB & kKeyRankMask);
+    const int sA = score >= total ? -L : (ra <= T ? ra : -(ra - T));
+    // rank in the (C, A) order: 0 for shift 0, -s for s < 0, T + s for s > 0
+    const int sB = score >= total ? -L : (rb <= T ? -rb : rb - T);
+    ac = shd_from_shift(sA, score, L, L);
+    ca = shd_from_shift(sB == -L ? -L : -sB, score, L, L);
+}
+
+// The alignment stage with a warp per work item (a mirrored pair or a single
+// pair; the same items and outputs as k_align). Persistent: the grid's warps
+// stride over the items.
+template <int BLOCK, int NW, bool CNT = false>
+__global__ void __launch_bounds__(BLOCK)
+k_align_warp(DevOptions o, DevReads r, uint32_t first, const uint32_t* __restrict__ cand_ids,
+             const uint32_t* __restrict__ cand_anchor, const uint32_t* __restrict__ seg_off,
+             const uint32_t* __restrict__ seg_cnt, const unsigned long long* __restrict__ total_ptr,
+             unsigned long long arena_cap, const int* __restrict__ status, AlignRes* __restrict__ out,
+             unsigned long long* __restrict__ work_count, const uint32_t* __restrict__ pair_order,
+             const uint2* __restrict__ work, const unsigned int* __restrict__ work_n,
+             unsigned long long* __restrict__ run_count) {
+    using Cnt = typename std::conditional<CNT, WordCount, NoCount>::type;
+    __shared__ int s_mex[kMaxLen + 1];
+    for (int i = threadIdx.x; i <= kMaxLen; i += BLOCK) s_mex[i] = __float2int_rz(__fmul_rn((float)i, o.max_error_rate));
+    __syncthreads();
+    if (*status & kStatusCandOverflow) return;
+    const unsigned long long total = *total_ptr;
+    if (total > arena_cap) return;
+    const unsigned long long items = work ? (unsigned long long)work_n[0] + work_n[1] : total;
+    const int lane = threadIdx.x & 31;
+    const unsigned long long nwarps = (unsigned long long)gridDim.x * (BLOCK / 32);
+    const float ler = __fmul_rn(o.estimated_errorrate, 4.0f);
+#pragma unroll 1
+    for (unsigned long long slot = (unsigned long long)blockIdx.x * (BLOCK / 32) + (threadIdx.x >> 5); slot < items;
+         slot += nwarps) {
+        Cnt wc;
+        unsigned long long i;
+        uint32_t j = kNoMirror;
+        if (work) {
+            const unsigned nl = work_n[0];
+            const uint2 wv = slot < nl ? work[slot] : work[total - 1 - (slot - nl)];
+            i = wv.x;
+            j = wv.y;
+        } else {
+            i = pair_order ? pair_order[slot] : slot;
+        }
+        const uint32_t ai = cand_anchor[i];
+        const uint32_t a = first + ai;
+        const uint32_t c = cand_ids[i];
+        const int La = r.len[a], Lc = r.len[c];
+        uint32_t Ah[NW + 2], Al[NW + 2], Ch[NW + 2], Cl[NW + 2];
+        load_planes<NW>(r.seq + (size_t)a * r.seq_pitch, La, Ah, Al);
+        load_planes<NW>(r.seq + (size_t)c * r.seq_pitch, Lc, Ch, Cl);
+        const int lo = __float2int_rz(__fmul_rn((float)La, o.min_overlap_ratio));
+        const int minov = o.min_overlap > lo ? o.min_overlap : lo;
+        if (work_count && lane == 0) atomicAdd(work_count, (unsigned long long)(2 * unpruned_words(La, Lc, minov)));
+        ShdResult f, g;
+        if (j != kNoMirror) shifted_hamming_pair_lanes<NW, Cnt>(Ah, Al, Ch, Cl, La, minov, s_mex, f, g, &wc);
+        else f = shifted_hamming_lanes<NW, Cnt>(Ah, Al, La, Ch, Cl, Lc, minov, s_mex, &wc);
+        uint32_t Rh[NW + 2], Rl[NW + 2];
+        revcomp_planes<NW>(Ch, Cl, Lc, Rh, Rl);
+        const ShdResult rc = shifted_hamming_lanes<NW, Cnt>(Ah, Al, La, Rh, Rl, Lc, minov, s_mex, &wc);
+        if constexpr (CNT) {
+            const unsigned ws = __reduce_add_sync(0xffffffffu, (unsigned)wc.n);
+            if (lane == 0) atomicAdd(run_count, (unsigned long long)ws);
+        }
+        if (lane == 0) {
+            auto result = [&](const ShdResult& fw, uint32_t anchor_index, uint32_t cand) {
+                const int orient = choose_orientation(fw, rc, La, o.min_overlap_ratio, o.min_overlap, ler);
+                AlignRes res;
+                const ShdResult& b = orient == 2 ? rc : fw;
+                res.shift = (int16_t)b.shift;
+                res.overlap = (int16_t)b.overlap;
+                res.nops = (int16_t)b.nops;
+                res.orient = (uint8_t)orient;
+                res.paired = o.paired_end ? mate_flag(cand_ids, seg_off, seg_cnt, anchor_index, cand) : 0;
+                return res;
+            };
+            out[i] = result(f, ai, c);
+            if (j != kNoMirror) out[j] = result(g, c - first, a);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Stage 3: filters, MSA, refinement, correction.
 //   filterCandidatesByAlignmentFlag / ...MismatchRatio(WithPairFlags)
 //                                     include/corrector.hpp:982-1211
@@ -492,6 +710,9 @@ struct MsaOut {
     // elements added to column sums (anchor and candidate bases, every
     // build): the MSA stage's roofline work; may be null
     unsigned long long* elem_count;
+    // refinement statistics, may be null: [0] elements added by rebuilds
+    // (builds after the first), [1] anchors rebuilt at least once
+    unsigned long long* rebuild_count;
 };
 
 constexpr int kNumFeatures = 24;
@@ -567,6 +788,7 @@ msa_anchor(const DevOptions& o, const DevReads& r, uint32_t first, uint32_t ai,
     __shared__ uint8_t s_alive[kStageMax];
     __shared__ int s_red[NWARP][4];
     __shared__ int s_vals[12];
+    __shared__ __align__(16) float s_asup[kMaxLen];   // support of the anchor's columns, position order
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint32_t a = first + ai;
@@ -622,6 +844,16 @@ msa_anchor(const DevOptions& o, const DevReads& r, uint32_t first, uint32_t ai,
         return pre + x - v;
     };
 
+    // ---- quality weights (qualityscoreweights.hpp:12-44) ----
+    for (int i = tid; i < 256; i += BLOCK) s_qw[i] = c_qweight[i];
+    const int qbits = o.quality_bits;
+    if (tid < 4) {
+        // the characters a 2- or 1-bit code stands for (qualityscorecompression.hpp:121-145)
+        const uint32_t ch = qbits == 2 ? (tid == 0 ? '$' : tid == 1 ? '(' : tid == 2 ? '1' : '9')
+                                       : (tid == 1 ? '5' : '(');
+        s_qwc[tid] = c_qweight[ch];
+    }
+
     // ---- alignment filters (corrector.hpp:982-1211), ordered compaction ----
     const float base = fmul_rn(o.estimated_errorrate, 1.0f);
     int c0 = 0, c1 = 0, c2 = 0, n1 = 0;
@@ -650,6 +882,9 @@ msa_anchor(const DevOptions& o, const DevReads& r, uint32_t first, uint32_t ai,
             else if ((float)red[2] >= good) thr = fmul_rn(4.0f, base);
         }
     }
+    // every candidate fits the staged rows: the survivors' records go straight
+    // to shared memory (else to the global records, staged chunk by chunk)
+    const bool direct = cnt <= (uint32_t)nstage;
     int V = 0;
     for (uint32_t c = 0; c < cnt; c += BLOCK) {
         const uint32_t i = c + tid;
@@ -672,7 +907,19 @@ msa_anchor(const DevOptions& o, const DevReads& r, uint32_t first, uint32_t ai,
             // calculateOverlapWeight: 1 - sqrtf(nOps / (overlap * maxMismatchRatio))
             rec.weight = fsub_rn(1.0f, __fsqrt_rn(fdiv_rn((float)ar.nops, fmul_rn((float)ar.overlap, o.max_error_rate))));
             rec.orient = ar.orient;
-            recs[off + V + pre] = rec;
+            const int k = V + pre;
+            if (direct) {
+                s_beg[k] = rec.shift;
+                s_len[k] = rec.len;
+                s_w[k] = rec.weight;
+                s_fwd[k] = rec.orient == 1;
+                s_id[k] = rec.id;
+                s_bl[k] = make_int2(rec.shift, rec.len);
+#pragma unroll
+                for (int q = 0; q < 4; ++q) s_wq[k][q] = fmul_rn(rec.weight, s_qwc[q]);
+            } else {
+                recs[off + k] = rec;
+            }
         }
         V += tot;
     }
@@ -682,16 +929,8 @@ msa_anchor(const DevOptions& o, const DevReads& r, uint32_t first, uint32_t ai,
     }
     __syncthreads();
 
-    // ---- quality weights, anchor row ----
-    for (int i = tid; i < 256; i += BLOCK) s_qw[i] = c_qweight[i];
-    const int qbits = o.quality_bits;
+    // ---- anchor row ----
     const int sp = r.seq_pitch, qp = r.qual_pitch;
-    if (tid < 4) {
-        // the characters a 2- or 1-bit code stands for (qualityscorecompression.hpp:121-145)
-        const uint32_t ch = qbits == 2 ? (tid == 0 ? '$' : tid == 1 ? '(' : tid == 2 ? '1' : '9')
-                                       : (tid == 1 ? '5' : '(');
-        s_qwc[tid] = c_qweight[ch];
-    }
     // quality character at position q of an encoded row (qualityscorecompression.hpp:121-145)
     auto qual_char = [&](const uint32_t* row, int q) -> uint32_t {
         if (qbits == 8) return (row[q >> 2] >> (8 * (q & 3))) & 0xFFu;
@@ -717,41 +956,46 @@ msa_anchor(const DevOptions& o, const DevReads& r, uint32_t first, uint32_t ai,
     // place (bases reversed and complemented, qualities reversed over the
     // whole quality pitch: reverseQualitiesOfRCAlignments, corrector.hpp:
     // 1227-1239), so the column sums read every row forward
-    auto stage = [&](int c, int n) {
+    auto stage = [&](int c, int n, bool fill) {
         __syncthreads();
-        for (int k = tid; k < n; k += BLOCK) {
-            const CandRec rc = recs[off + c + k];
-            s_beg[k] = rc.shift;                // relative to the anchor; abegin added per build
-            s_len[k] = rc.len;
-            s_w[k] = rc.weight;
-            s_fwd[k] = rc.orient == 1;
-            s_id[k] = rc.id;
-            s_bl[k] = make_int2(rc.shift, rc.len);
+        if (fill) {
+            for (int k = tid; k < n; k += BLOCK) {
+                const CandRec rc = recs[off + c + k];
+                s_beg[k] = rc.shift;                // relative to the anchor; abegin added per build
+                s_len[k] = rc.len;
+                s_w[k] = rc.weight;
+                s_fwd[k] = rc.orient == 1;
+                s_id[k] = rc.id;
+                s_bl[k] = make_int2(rc.shift, rc.len);
 #pragma unroll
-            for (int q = 0; q < 4; ++q) s_wq[k][q] = fmul_rn(rc.weight, s_qwc[q]);
+                for (int q = 0; q < 4; ++q) s_wq[k][q] = fmul_rn(rc.weight, s_qwc[q]);
+            }
+            __syncthreads();
         }
-        __syncthreads();
-        for (int k0 = warp; k0 < n; k0 += 8 * NWARP) {
-            for (int w0 = 0; w0 < rw; w0 += 32) {
-                const int w = w0 + lane;
-                uint32_t v[8];
+        // word idx = k * rw + w of the staged rows, eight words in flight per
+        // thread; k = floor(idx / rw) by a multiply-high (exact: idx * rw < 2^32)
+        const int nw = n * rw;
+        const unsigned long long mrw = ((1ull << 32) + (unsigned)rw - 1) / (unsigned)rw;
+        for (int b0 = 0; b0 < nw; b0 += 8 * BLOCK) {
+            uint32_t v[8];
 #pragma unroll
-                for (int u = 0; u < 8; ++u) {
-                    const int k = k0 + u * NWARP;
-                    v[u] = 0u;
-                    if (k < n && w < rw) {
-                        const size_t id = s_id[k];
-                        v[u] = w < sp ? __ldg(r.seq + id * sp + w) : __ldg(r.qual + id * qp + (w - sp));
-                    }
-                }
-#pragma unroll
-                for (int u = 0; u < 8; ++u) {
-                    const int k = k0 + u * NWARP;
-                    if (k < n && w < rw) s_raw[k * rw + w] = v[u];
+            for (int u = 0; u < 8; ++u) {
+                const int idx = b0 + u * BLOCK + tid;
+                v[u] = 0u;
+                if (idx < nw) {
+                    const int k = (int)(((unsigned long long)idx * mrw) >> 32);
+                    const int w = idx - k * rw;
+                    const size_t id = s_id[k];
+                    v[u] = w < sp ? __ldg(r.seq + id * sp + w) : __ldg(r.qual + id * qp + (w - sp));
                 }
             }
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const int idx = b0 + u * BLOCK + tid;
+                if (idx < nw) s_raw[idx] = v[u];
+            }
         }
-        __syncwarp();
+        __syncthreads();
         // reverse-complement rows: a warp per row, each lane one output word
         // built from a window of the source words (fetched by shuffle)
         for (int k = warp; k < n; k += NWARP) {
@@ -828,7 +1072,7 @@ msa_anchor(const DevOptions& o, const DevReads& r, uint32_t first, uint32_t ai,
     const bool persistent = V <= nstage;      // all rows stay staged across rebuilds
     int nalive = V;
     if (persistent) {
-        stage(0, V);
+        stage(0, V, !direct);
         for (int k = tid; k < V; k += BLOCK) s_alive[k] = (uint8_t)k;
     }
     __syncthreads();
@@ -869,6 +1113,10 @@ msa_anchor(const DevOptions& o, const DevReads& r, uint32_t first, uint32_t ai,
             int tot = La;
             for (int w = 0; w < NWARP; ++w) tot += s_red[w][2];
             atomicAdd(out.elem_count, (unsigned long long)tot);
+            if (iter > 0 && out.rebuild_count) {
+                atomicAdd(out.rebuild_count, (unsigned long long)tot);
+                if (iter == 1) atomicAdd(out.rebuild_count + 1, 1ull);
+            }
         }
         ncols = mx - mn;
         abegin = -mn;
@@ -953,7 +1201,7 @@ msa_anchor(const DevOptions& o, const DevReads& r, uint32_t first, uint32_t ai,
                 // more rows than fit: each chunk is staged (by all warps) per block
                 for (int c = 0; c < nalive; c += nstage) {
                     const int n = min(nstage, nalive - c);
-                    stage(c, n);
+                    stage(c, n, true);
                     if (active) run_rows(nullptr, n);
                     flush();
                 }
@@ -966,7 +1214,12 @@ msa_anchor(const DevOptions& o, const DevReads& r, uint32_t first, uint32_t ai,
                 if (wT > cw) { cs = 3; cw = wT; }
                 const float colw = __fadd_rn(__fadd_rn(__fadd_rn(wA, wC), wG), wT);
                 s_cons[col] = cs;
-                s_support[col] = fdiv_rn(cw, colw);
+                const float sup = fdiv_rn(cw, colw);
+                s_support[col] = sup;
+                {
+                    const int p = col - abegin;
+                    if (p >= 0 && p < La) s_asup[p] = sup;
+                }
                 const uint32_t nA = cAC & 0xFFFFu, nC = cAC >> 16;
                 const uint32_t nG = cGT & 0xFFFFu, nT = cGT >> 16;
                 s_cov[col] = (uint16_t)(nA + nC + nG + nT);
@@ -1091,12 +1344,23 @@ msa_anchor(const DevOptions& o, const DevReads& r, uint32_t first, uint32_t ai,
         __syncthreads();
         if (lane == 0) { s_red[warp][0] = __float_as_int(mnS); s_red[warp][1] = mnC; }
         __syncthreads();
-        if (tid == 0) {
+        if (warp == 0) {
             float minSup = 3.402823466e+38f;
             int minCov = 0x7fffffff;
             for (int w = 0; w < NWARP; ++w) { minSup = fminf(minSup, __int_as_float(s_red[w][0])); minCov = min(minCov, s_red[w][1]); }
-            float sum = 0.0f;                 // std::accumulate order
-            for (int p = 0; p < La; ++p) sum = __fadd_rn(sum, s_support[abegin + p]);
+            // std::accumulate order: one serial chain of IEEE adds (lane 0),
+            // the supports read four at a time
+            float sum = 0.0f;
+            if (lane == 0) {
+                const float4* v4 = reinterpret_cast<const float4*>(s_asup);
+                int p = 0;
+                for (; p + 4 <= La; p += 4) {
+                    const float4 v = v4[p >> 2];
+                    sum = __fadd_rn(__fadd_rn(__fadd_rn(__fadd_rn(sum, v.x), v.y), v.z), v.w);
+                }
+                for (; p < La; ++p) sum = __fadd_rn(sum, s_asup[p]);
+            }
+            sum = __shfl_sync(0xffffffffu, sum, 0);
             const float avgSup = fdiv_rn(sum, (float)La);
             const float e = o.estimated_errorrate;
             const float avgThr = fsub_rn(1.0f, fmul_rn(1.0f, e));
@@ -1104,22 +1368,32 @@ msa_anchor(const DevOptions& o, const DevReads& r, uint32_t first, uint32_t ai,
             const float covThr = fmul_rn(fdiv_rn(o.m_coverage, 6.0f), o.estimated_coverage);
             const bool good = fgeq(avgSup, avgThr) && fgeq(minSup, minThr) && fgeq((float)minCov, covThr);
             bool isHQ = false;
-            if (good) {
+            if (good) {                       // warp-uniform
+                // the smallest percentage pc in [0, pct] whose thresholds hold
+                // (the reference's loop from pct down to 0 keeps the last one)
                 int smallest = 100;
                 const int pct = (int)ceilf(fmul_rn(e, 100.0f));
-                for (int pc = pct; pc >= 0; --pc) {
+                auto holds = [&](int pc) {
                     const float fac = fdiv_rn((float)pc, 100.0f);
                     const float at = fsub_rn(1.0f, fmul_rn(1.0f, fac));
                     const float mt = fsub_rn(1.0f, fmul_rn(3.0f, fac));
-                    if (fgeq(avgSup, at) && fgeq(minSup, mt)) smallest = pc;
+                    return fgeq(avgSup, at) && fgeq(minSup, mt);
+                };
+                if (pct < 32) {
+                    const unsigned bm = __ballot_sync(0xffffffffu, lane <= pct && holds(lane));
+                    if (bm) smallest = __ffs(bm) - 1;
+                } else {
+                    for (int pc = pct; pc >= 0; --pc) if (holds(pc)) smallest = pc;
                 }
                 isHQ = fgeq((float)minCov, covThr) && fleq((float)smallest, fmul_rn((float)pct, 0.5f));
             }
-            s_vals[4] = good;
-            s_vals[5] = isHQ;
-            s_vals[6] = __float_as_int(avgSup);
-            s_vals[7] = __float_as_int(minSup);
-            s_vals[8] = minCov;
+            if (lane == 0) {
+                s_vals[4] = good;
+                s_vals[5] = isHQ;
+                s_vals[6] = __float_as_int(avgSup);
+                s_vals[7] = __float_as_int(minSup);
+                s_vals[8] = minCov;
+            }
         }
         __syncthreads();
         allGood = s_vals[4];
@@ -1272,7 +1546,7 @@ msa_anchor(const DevOptions& o, const DevReads& r, uint32_t first, uint32_t ai,
 // One CTA per anchor, in `order` (e.g. most candidates first) when given;
 // the hardware block scheduler hands out the anchors.
 template <int BLOCK, int JB, bool EMIT = false>
-__global__ void __launch_bounds__(BLOCK, 768 / BLOCK)
+__global__ void __launch_bounds__(BLOCK, (EMIT ? 768 : 1024) / BLOCK)
 k_msa(DevOptions o, DevReads r, uint32_t first, uint32_t count, const uint32_t* __restrict__ order,
       const uint32_t* __restrict__ cand_ids, const uint32_t* __restrict__ seg_off,
       const uint32_t* __restrict__ seg_cnt, const AlignRes* __restrict__ ares,
@@ -1286,7 +1560,7 @@ k_msa(DevOptions o, DevReads r, uint32_t first, uint32_t count, const uint32_t* 
 // Persistent form: a grid of resident CTAs pulls anchors from a device work
 // queue (an atomic cursor over `order`) until the batch is done.
 template <int BLOCK, int JB, bool EMIT = false>
-__global__ void __launch_bounds__(BLOCK, 768 / BLOCK)
+__global__ void __launch_bounds__(BLOCK, (EMIT ? 768 : 1024) / BLOCK)
 k_msa_queue(DevOptions o, DevReads r, uint32_t first, uint32_t count, const uint32_t* __restrict__ order,
             unsigned int* __restrict__ cursor, const uint32_t* __restrict__ cand_ids,
             const uint32_t* __restrict__ seg_off, const uint32_t* __restrict__ seg_cnt,

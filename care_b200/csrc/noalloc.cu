@@ -11,6 +11,7 @@
 #include "hostio.hpp"
 #include "kernels.cuh"
 
+#include <algorithm>
 #include <mutex>
 
 using namespace careb200;
@@ -60,6 +61,19 @@ int setup_device(int dev, unsigned char** out) {
     return CARE_B200_OK;
 }
 
+constexpr int kStatusBadLength = 1 << 16;    // a read length outside [0, max_length]
+
+// Every read length within [0, max_len]: the kernels size their shared memory
+// and registers from max_len and index by the lengths.
+__global__ void k_check_lengths(const int* __restrict__ len, uint32_t n, int max_len, int* __restrict__ status) {
+    bool bad = false;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int L = len[i];
+        bad |= L < 0 || L > max_len;
+    }
+    if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(status, kStatusBadLength);
+}
+
 }  // namespace
 
 extern "C" int care_b200_correct_range_noalloc(const care_b200_options* opt, const care_b200_device_reads* reads,
@@ -81,6 +95,10 @@ extern "C" int care_b200_correct_range_noalloc(const care_b200_options* opt, con
     if (num_anchors > kNoAllocMaxAnchors) return CARE_B200_ELIMIT;
     if (reads->max_length < 1 || reads->max_length > kMaxLen) return CARE_B200_ELIMIT;
     if ((size_t)(reads->max_length + 15) / 16 > reads->pitch_ints) return CARE_B200_EINVAL;
+    if (opt->use_quality &&
+        (size_t)((int64_t)reads->max_length * opt->quality_bits + 31) / 32 > reads->qual_pitch_ints)
+        return CARE_B200_EINVAL;
+    if (tables->threshold < 0 || tables->threshold > 65535) return CARE_B200_EINVAL;
 
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return CARE_B200_ECUDA;
@@ -99,7 +117,9 @@ extern "C" int care_b200_correct_range_noalloc(const care_b200_options* opt, con
     o.exclude_ambiguous = opt->exclude_ambiguous;
     o.correct_candidates = 0;
     o.paired_end = opt->paired_end;
-    {
+    if (tables->threshold > 0) {
+        o.threshold = tables->threshold;                                 // the tables' own (e.g. from a file)
+    } else {
         const int cov = (int)opt->estimated_coverage;
         int t = (int)(cov * 2.5f);
         t = t > 65535 ? 65535 : t;
@@ -137,6 +157,16 @@ extern "C" int care_b200_correct_range_noalloc(const care_b200_options* opt, con
     // the counters and status word keep the previous call's values: clear them
     if (cudaMemsetAsync(scratch, 0, 256, st) != cudaSuccess) return CARE_B200_ECUDA;
     if (cudaMemsetAsync(sequences, 0, (size_t)num_anchors * reads->max_length, st) != cudaSuccess) return CARE_B200_ECUDA;
+    // lengths beyond max_length would take the kernels past their buffers:
+    // rejected before any of them runs
+    {
+        const unsigned cb = (unsigned)std::min<uint64_t>((r.n + 255) / 256, 1024);
+        k_check_lengths<<<cb, 256, 0, st>>>(r.len, r.n, r.max_len, dstatus);
+        int hs = 0;
+        if (cudaMemcpyAsync(&hs, dstatus, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess) return CARE_B200_ECUDA;
+        if (cudaStreamSynchronize(st) != cudaSuccess) return CARE_B200_ECUDA;
+        if (hs & kStatusBadLength) return CARE_B200_EINVAL;
+    }
 
     const int h = o.num_maps;
     const size_t tmax = (size_t)h * o.threshold;
@@ -150,7 +180,14 @@ extern "C" int care_b200_correct_range_noalloc(const care_b200_options* opt, con
         o, r, static_cast<const TableDesc*>(tables->descs), static_cast<const Slot*>(tables->slots), tables->values,
         nullptr, first_anchor, num_anchors, set_log2, nullptr, nullptr, cand_ids, cand_anchor, seg_off, seg_cnt, counters, kNoAllocMaxPairs,
         dstatus);
-    const unsigned ablocks = (unsigned)((kNoAllocMaxPairs + 127) / 128);
+    // the pairs the candidate pass found size the alignment grid; a count
+    // above the array's pair capacity ends the call here
+    unsigned long long npairs = 0;
+    if (cudaMemcpyAsync(&npairs, counters, sizeof(npairs), cudaMemcpyDeviceToHost, st) != cudaSuccess)
+        return CARE_B200_ECUDA;
+    if (cudaStreamSynchronize(st) != cudaSuccess) return CARE_B200_ECUDA;
+    if (npairs > kNoAllocMaxPairs) return CARE_B200_ELIMIT;
+    const unsigned ablocks = (unsigned)std::max<unsigned long long>((npairs + 127) / 128, 1);
     const int nw = (r.max_len + 31) / 32;
 #define LAUNCH_ALIGN(NW)                                                                                    \
     k_align<128, NW><<<ablocks, 128, 0, st>>>(o, r, first_anchor, cand_ids, cand_anchor, seg_off, seg_cnt,  \

@@ -184,7 +184,11 @@ int care_b200_save_hashtables(care_b200_ctx* ctx, const char* path);
 int care_b200_write_output(care_b200_ctx* ctx, const char* outfile);
 
 /* Statistics of the last correction call: device milliseconds of the
- * pipeline and per-stage kernel times (signature+query, alignment, MSA). */
+ * pipeline and per-stage kernel times: stage_ms[0] candidate lookup (table
+ * queries of the anchors' resident signatures), [1] alignment, [2] MSA and
+ * correction, [3] the learned decision. stage_ms[4], when asked for, is the
+ * last minhash-signature pass over the read storage (run once per uploaded
+ * or loaded storage, not by the correction calls). */
 int care_b200_last_timing(const care_b200_ctx* ctx, float* total_ms, float* stage_ms, int nstages);
 
 /* Counters of the last correction call: stats[0] anchors, stats[1]
@@ -198,7 +202,10 @@ int care_b200_last_timing(const care_b200_ctx* ctx, float* total_ms, float* stag
  * this library launched (every batch and every arena-growth attempt),
  * stats[7] anchors whose candidate lists took the second, full-set pass,
  * stats[8] 32-bit word compares the alignment scans actually ran after their
- * early exits (counted only while care_b200_count_word_compares is on, else 0). */
+ * early exits (counted only while care_b200_count_word_compares is on, else 0),
+ * stats[9] bases added to MSA column sums by refinement rebuilds (the builds
+ * after an anchor's first; included in stats[4]), stats[10] anchors whose
+ * MSA was rebuilt at least once (refineMSA, include/corrector.hpp:1307-1421). */
 int care_b200_last_stats(const care_b200_ctx* ctx, uint64_t* stats, int nstats);
 
 /* on = 1: the following correction calls run the alignment's statistics form,
@@ -229,12 +236,16 @@ typedef struct care_b200_device_reads {
  * {uint64 key; uint32 offset; uint32 count} (16 bytes; count 0 = empty;
  * capacity mask+1 a power of two; a key starts probing at
  * MurmurHash3-fmix64(key) & mask and moves to the next slot), and one value
- * array of read ids (the key's ids at value_base + offset, ascending). */
+ * array of read ids (the key's ids at value_base + offset, ascending; every
+ * id below the storage's num_reads). */
 typedef struct care_b200_device_tables {
     int             num_maps;
     const void*     descs;
     const void*     slots;
     const uint32_t* values;
+    int             threshold;        /* per-map result threshold of these tables
+                                         (care_b200_result_threshold); 0: derived
+                                         from opt->estimated_coverage */
 } care_b200_device_tables;
 
 #define CARE_B200_NOALLOC_MAX_ANCHORS 16384
@@ -251,14 +262,20 @@ typedef struct care_b200_device_tables {
  * available here (opt->correct_candidates must be 0). Work runs on `stream`
  * (a cudaStream_t, NULL for the default stream) and the call returns when it
  * has finished.
- * Working memory is one device array compiled into the library (about 32 MB;
- * every GPU that loads the library holds it until the process exits): at
- * most CARE_B200_NOALLOC_MAX_ANCHORS anchors and
+ * Working memory is one device array compiled into the library (about 32 MB):
+ * at most CARE_B200_NOALLOC_MAX_ANCHORS anchors and
  * CARE_B200_NOALLOC_MAX_PAIRS (anchor, candidate) pairs per call; larger
- * requests return CARE_B200_ELIMIT. The first call on a device looks up the
- * array's device address and loads constants, so make it before any stream
- * capture. All calls share the array: calls that overlap on the GPU (from
- * several threads or streams) race and must be serialised by the caller.
+ * requests return CARE_B200_ELIMIT. CUDA places a module's device arrays
+ * when the module is first used, so the array is reserved by the first call
+ * on each device (which also looks up its address and loads constants) and
+ * then held until the process exits: make that first call before the
+ * caller's own pool takes the device's memory, and before any stream
+ * capture; later calls leave the device's free memory unchanged. Every read
+ * length must lie in [0, max_length] (checked on the device first:
+ * CARE_B200_EINVAL otherwise), and with qualities qual_pitch_ints must hold
+ * max_length * quality_bits bits. All calls share the array: calls that
+ * overlap on the GPU (from several threads or streams) race and must be
+ * serialised by the caller.
  * Returns 0 or a CARE_B200_E* code. */
 int care_b200_correct_range_noalloc(const care_b200_options* opt, const care_b200_device_reads* reads,
                                     const care_b200_device_tables* tables, uint32_t first_anchor,
@@ -363,6 +380,9 @@ typedef struct care_b200_tuning {
     int cand_set_log2; /* 6..14: de-duplication set of the main candidate pass, 2^x entries;
                           anchors with more than 2^(x-1) unique candidates take a second pass
                           with a set for every retrieved id (default 10) */
+    int align_warp;    /* 1: a warp per alignment work item, its lanes taking the shifts of
+                          each group of 32 (the scan's first minimal shift found by warp
+                          reductions); 0: a thread per work item */
 } care_b200_tuning;
 
 int care_b200_default_tuning(care_b200_tuning* t);
@@ -373,6 +393,12 @@ int care_b200_get_tuning(const care_b200_ctx* ctx, care_b200_tuning* t);
 uint32_t care_b200_num_reads(const care_b200_ctx* ctx);
 int      care_b200_max_length(const care_b200_ctx* ctx);
 int      care_b200_num_maps(const care_b200_ctx* ctx);
+/* Per-map result threshold of the context's tables: buckets with more read
+ * ids are dropped at query time (OrdinaryCpuMinhasher::queryMap,
+ * include/ordinaryminhasher.hpp:437-449). Derived from the coverage
+ * (calculateResultsPerMapThreshold, include/minhasherlimit.hpp:9-15) unless
+ * tables were loaded from a file, whose own threshold is then used. */
+int      care_b200_result_threshold(const care_b200_ctx* ctx);
 
 #ifdef __cplusplus
 }

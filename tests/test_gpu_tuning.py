@@ -27,6 +27,9 @@ VARIANTS = [
     {"pair_mirror": 1, "pair_order": 1},
     {"cand_set_log2": 8},
     {"cand_set_log2": 12},
+    {"align_warp": 1},
+    {"align_warp": 1, "pair_mirror": 1, "align_block": 256},
+    {"align_warp": 1, "pair_mirror": 1, "pair_order": 1},
     {"msa_order": 1, "msa_queue": 1, "msa_warps": 8, "align_block": 256, "pair_order": 1, "graph": 1,
      "pair_mirror": 1},
 ]
