@@ -61,17 +61,21 @@ def run(cmd: list[str]) -> None:
 def build(force: bool = False, verbose: bool = False) -> str:
     os.makedirs(BUILD, exist_ok=True)
     deps = _deps()
-    objs = []
+    objs, jobs = [], []
     for src in CU_SOURCES:
         obj = os.path.join(BUILD, src + ".o")
         if force or _newer(obj, deps):
-            run([nvcc()] + NVFLAGS + ["-c", os.path.join(CSRC, src), "-o", obj])
+            jobs.append([nvcc()] + NVFLAGS + ["-c", os.path.join(CSRC, src), "-o", obj])
         objs.append(obj)
     for src in CXX_SOURCES:
         obj = os.path.join(BUILD, src + ".o")
         if force or _newer(obj, deps):
-            run(["g++"] + CXXFLAGS + ["-c", os.path.join(CSRC, src), "-o", obj])
+            jobs.append(["g++"] + CXXFLAGS + ["-c", os.path.join(CSRC, src), "-o", obj])
         objs.append(obj)
+    # translation units compile in parallel
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
+        list(ex.map(run, jobs))
     if force or _newer(LIB, objs):
         run([nvcc()] + ARCH + ["-shared", "-o", LIB] + objs + ["-lpthread"])
     if force or _newer(EXE, [LIB, os.path.join(CSRC, "main.cpp")]):
