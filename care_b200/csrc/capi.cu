@@ -694,38 +694,38 @@ struct MsaArgs {
     const uint32_t* cand_ids; const uint32_t* seg_off; const uint32_t* seg_cnt; const AlignRes* ares;
     CandRec* recs; MsaOut out; int* status; size_t smem;
     bool queue; int sms; int grid;             // grid: resident CTAs of the queue form (prepare)
+    int jb;                                    // 32-column blocks per warp
 };
 
 // prepare (host only: attributes, occupancy) or launch one MSA variant
-template <int B, int JB, bool E>
+template <int B, int QB, bool E>
 cudaError_t msa_go(MsaArgs& a, bool prepare, cudaStream_t st) {
     if (prepare) {
-        cudaError_t e = cudaFuncSetAttribute(k_msa<B, JB, E>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)a.smem);
+        cudaError_t e = cudaFuncSetAttribute(k_msa<B, QB, E>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)a.smem);
         if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(k_msa_queue<B, JB, E>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)a.smem);
+            e = cudaFuncSetAttribute(k_msa_queue<B, QB, E>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)a.smem);
         int nb = 0;
-        if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_msa_queue<B, JB, E>, B, a.smem);
+        if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_msa_queue<B, QB, E>, B, a.smem);
         a.grid = (int)std::min<uint64_t>(a.count, (uint64_t)a.sms * (uint64_t)std::max(nb, 1));
         return e;
     }
     if (a.queue)
-        k_msa_queue<B, JB, E><<<a.grid, B, a.smem, st>>>(a.o, a.r, a.first, a.count, a.order, a.cursor, a.cand_ids,
-                                                        a.seg_off, a.seg_cnt, a.ares, a.recs, a.out, a.status);
+        k_msa_queue<B, QB, E><<<a.grid, B, a.smem, st>>>(a.o, a.r, a.first, a.count, a.jb, a.order, a.cursor,
+                                                        a.cand_ids, a.seg_off, a.seg_cnt, a.ares, a.recs, a.out,
+                                                        a.status);
     else
-        k_msa<B, JB, E><<<a.count, B, a.smem, st>>>(a.o, a.r, a.first, a.count, a.order, a.cand_ids, a.seg_off,
-                                                    a.seg_cnt, a.ares, a.recs, a.out, a.status);
+        k_msa<B, QB, E><<<a.count, B, a.smem, st>>>(a.o, a.r, a.first, a.count, a.jb, a.order, a.cand_ids,
+                                                    a.seg_off, a.seg_cnt, a.ares, a.recs, a.out, a.status);
     return cudaGetLastError();
 }
 
-cudaError_t msa_dispatch(int warps, int jb, bool emit, MsaArgs& a, bool prepare, cudaStream_t st) {
-#define MS(B, J) return emit ? msa_go<B, J, true>(a, prepare, st) : msa_go<B, J, false>(a, prepare, st);
+// qb: the quality encoding the column sums read (0 when qualities are unused)
+cudaError_t msa_dispatch(int warps, int qb, bool emit, MsaArgs& a, bool prepare, cudaStream_t st) {
+#define MS(B, Q) return emit ? msa_go<B, Q, true>(a, prepare, st) : msa_go<B, Q, false>(a, prepare, st);
     if (warps == 8) {
-        switch (jb) { case 1: MS(256, 1) case 2: MS(256, 2) default: MS(256, 3) }
+        switch (qb) { case 0: MS(256, 0) case 1: MS(256, 1) case 2: MS(256, 2) default: MS(256, 8) }
     }
-    switch (jb) {
-        case 1: MS(128, 1) case 2: MS(128, 2) case 3: MS(128, 3)
-        case 4: MS(128, 4) case 5: MS(128, 5) default: MS(128, 6)
-    }
+    switch (qb) { case 0: MS(128, 0) case 1: MS(128, 1) case 2: MS(128, 2) default: MS(128, 8) }
 #undef MS
 }
 
@@ -799,7 +799,9 @@ int run_batch(care_b200_ctx* ctx, uint32_t first, uint32_t count, bool timed) {
     const int warps = tu.msa_warps == 8 ? 8 : 4;
     const int jb = (maxcols + 32 * warps - 1) / (32 * warps);
     const int nw = (ctx->max_len + 31) / 32;           // bit-plane width: 32-base words of the longest read
-    const size_t msmem = msa_smem_bytes(ctx->max_len, ctx->seq_pitch, ctx->has_qual ? ctx->qual_pitch : 0, emit);
+    const size_t msmem = msa_smem_bytes(ctx->max_len, ctx->seq_pitch, ctx->has_qual ? ctx->qual_pitch : 0, emit,
+                                        32 * jb * warps);
+    const int qb = ctx->has_qual ? ctx->opt.quality_bits : 0;
 
     for (int attempt = 0; attempt < 8; ++attempt) {
         const unsigned long long cap = ctx->cand_cap;
@@ -854,8 +856,8 @@ int run_batch(care_b200_ctx* ctx, uint32_t first, uint32_t count, bool timed) {
         MsaArgs ma{o, r, first, count, tu.msa_order ? ctx->d_order.as<uint32_t>() : nullptr,
                    reinterpret_cast<unsigned int*>(counters + 4), ctx->d_cand_ids.as<uint32_t>(),
                    ctx->d_seg_off.as<uint32_t>(), ctx->d_seg_cnt.as<uint32_t>(), ctx->d_ares.as<AlignRes>(),
-                   ctx->d_recs.as<CandRec>(), mo, status, msmem, tu.msa_queue != 0, ctx->sms, 0};
-        CK(msa_dispatch(warps, jb, emit, ma, true, ctx->stream), "MSA launch setup");
+                   ctx->d_recs.as<CandRec>(), mo, status, msmem, tu.msa_queue != 0, ctx->sms, 0, jb};
+        CK(msa_dispatch(warps, qb, emit, ma, true, ctx->stream), "MSA launch setup");
 
         cudaStream_t st = ctx->stream;
         const bool graph = tu.graph != 0;
@@ -926,7 +928,7 @@ int run_batch(care_b200_ctx* ctx, uint32_t first, uint32_t count, bool timed) {
                 EQ(cudaGetLastError(), "LPT order");
                 launches += 3;
             }
-            EQ(msa_dispatch(warps, jb, emit, ma, false, st), "k_msa");
+            EQ(msa_dispatch(warps, qb, emit, ma, false, st), "k_msa");
             ++launches;
             EQ(mark(3), "event");
             if (o.clf_mode == 2) {

@@ -728,11 +728,15 @@ __host__ __device__ inline int msa_stage_rows(int seq_pitch, int qual_pitch) {
 
 // dynamic shared memory of k_msa: the anchor's decoded row, the staged
 // packed candidate rows; with decision rows also three per-anchor-column
-// weights
-__host__ __device__ inline size_t msa_smem_bytes(int max_len, int seq_pitch, int qual_pitch, bool emit = false) {
-    const size_t elem = ((size_t)max_len * 2 + 15) & ~(size_t)15;
-    const size_t raw = (size_t)msa_stage_rows(seq_pitch, qual_pitch) * (seq_pitch + qual_pitch) * 4;
-    return elem + raw + (emit ? (size_t)3 * max_len * 4 : 0);
+// weights; then the per-column arrays of `maxcols` columns (four 16-bit
+// counts, support, coverage, consensus). Every part starts on a 16-byte
+// boundary (maxcols is a multiple of 128).
+__host__ __device__ inline size_t msa_round16(size_t x) { return (x + 15) & ~(size_t)15; }
+__host__ __device__ inline size_t msa_smem_bytes(int max_len, int seq_pitch, int qual_pitch, bool emit, int maxcols) {
+    const size_t elem = msa_round16((size_t)max_len * 2);
+    const size_t raw = msa_round16((size_t)msa_stage_rows(seq_pitch, qual_pitch) * (seq_pitch + qual_pitch) * 4);
+    const size_t fw = emit ? msa_round16((size_t)3 * max_len * 4) : 0;
+    return elem + raw + fw + (size_t)maxcols * (8 + 4 + 2 + 1);
 }
 
 // One element of a column: weight w added to the sum of its base b (0..3)
@@ -764,20 +768,20 @@ __device__ __forceinline__ void msa_add(float& wA, float& wC, float& wG, float& 
 
 // The whole MSA stage of one anchor (local index ai) for one CTA. Every
 // early return is taken by all threads of the CTA together.
-template <int BLOCK, int JB, bool EMIT>
+// QB: the quality encoding the sums read (0: qualities unused, else 1, 2 or
+// 8 bits per quality); jb: 32-column blocks per warp (the MSA holds at most
+// 32 * jb * warps columns).
+template <int BLOCK, int QB, bool EMIT>
 __device__ __forceinline__ void
-msa_anchor(const DevOptions& o, const DevReads& r, uint32_t first, uint32_t ai,
+msa_anchor(const DevOptions& o, const DevReads& r, uint32_t first, uint32_t ai, int jb,
            const uint32_t* __restrict__ cand_ids, const uint32_t* __restrict__ seg_off,
            const uint32_t* __restrict__ seg_cnt, const AlignRes* __restrict__ ares,
            CandRec* __restrict__ recs, const MsaOut& out, int* __restrict__ status) {
     constexpr int NWARP = BLOCK / 32;
-    constexpr int MAXCOLS = 32 * JB * NWARP;
+    const int MAXCOLS = 32 * jb * NWARP;
     extern __shared__ __align__(16) unsigned char dsm[];
-    __shared__ uint8_t s_cons[MAXCOLS];
-    __shared__ float s_support[MAXCOLS];
-    __shared__ uint16_t s_cov[MAXCOLS];
-    __shared__ uint16_t s_cnt[MAXCOLS][4];
     __shared__ float s_qw[256];
+    __shared__ uint2 s_hits[NWARP][32];      // per warp: the staged rows meeting its column block
     __shared__ float s_qwc[4];               // weight of a 1- or 2-bit quality code
     __shared__ int s_beg[kStageMax], s_len[kStageMax];
     __shared__ float s_w[kStageMax];
@@ -795,15 +799,25 @@ msa_anchor(const DevOptions& o, const DevReads& r, uint32_t first, uint32_t ai,
     const uint32_t off = seg_off[ai], cnt = seg_cnt[ai];
     const int La = r.len[a];
     const int mlen = r.max_len;
-    const bool useQ = o.use_quality && r.qual != nullptr;
+    constexpr bool useQ = QB != 0;
     char* aout = out.seq + (size_t)ai * mlen;
     const int nstage = msa_stage_rows(r.seq_pitch, r.qual_pitch);
     const int rw = r.seq_pitch + r.qual_pitch;               // words per staged row
+    // dynamic shared memory, each part 16-byte aligned (msa_smem_bytes)
     uint16_t* s_aelem = (uint16_t*)dsm;                      // anchor row: base | quality char << 2
-    uint32_t* s_raw = (uint32_t*)(dsm + (((size_t)mlen * 2 + 15) & ~(size_t)15));   // [nstage][rw]
+    uint32_t* s_raw = (uint32_t*)(dsm + msa_round16((size_t)mlen * 2));   // [nstage][rw]
     // per anchor column: column weight sum, consensus weight, weight of the
     // anchor's base (EMIT only)
-    float* s_fw = (float*)(s_raw + (size_t)nstage * rw);
+    float* s_fw = (float*)((unsigned char*)s_raw + msa_round16((size_t)nstage * rw * 4));
+    // per MSA column: counts of A C G T, support, coverage, consensus
+    ushort4* s_cnt4 = (ushort4*)((unsigned char*)s_fw + (EMIT ? msa_round16((size_t)3 * mlen * 4) : 0));
+    float* s_support = (float*)(s_cnt4 + MAXCOLS);
+    uint16_t* s_cov = (uint16_t*)(s_support + MAXCOLS);
+    uint8_t* s_cons = (uint8_t*)(s_cov + MAXCOLS);
+    auto cnt_of = [&](int col, int b) -> int {
+        const ushort4 c = s_cnt4[col];
+        return b == 0 ? c.x : b == 1 ? c.y : b == 2 ? c.z : c.w;
+    };
 
     if (cnt == 0) {
         if (tid == 0) { out.status[ai] = 0; out.nedits[ai] = 0; }
@@ -846,7 +860,7 @@ msa_anchor(const DevOptions& o, const DevReads& r, uint32_t first, uint32_t ai,
 
     // ---- quality weights (qualityscoreweights.hpp:12-44) ----
     for (int i = tid; i < 256; i += BLOCK) s_qw[i] = c_qweight[i];
-    const int qbits = o.quality_bits;
+    constexpr int qbits = QB;
     if (tid < 4) {
         // the characters a 2- or 1-bit code stands for (qualityscorecompression.hpp:121-145)
         const uint32_t ch = qbits == 2 ? (tid == 0 ? '$' : tid == 1 ? '(' : tid == 2 ? '1' : '9')
@@ -1059,16 +1073,6 @@ msa_anchor(const DevOptions& o, const DevReads& r, uint32_t first, uint32_t ai,
     // base (2-bit, in the candidate's aligned orientation) of staged row k at
     // position p < s_len[k]
     auto cand_base = [&](int k, int p) -> uint32_t { return base_at(s_raw + k * rw, p); };
-    // weight of staged row k's element at position p: row weight times its
-    // quality weight (the product computed once per row and code for 1- and
-    // 2-bit qualities)
-    auto cand_weight = [&](int k, int p) -> float {
-        const uint32_t* qrow = s_raw + k * rw + sp;
-        if (qbits == 2) return s_wq[k][(qrow[p >> 4] >> (30 - 2 * (p & 15))) & 3u];
-        if (qbits == 8) return fmul_rn(s_w[k], s_qw[(qrow[p >> 2] >> (8 * (p & 3))) & 0xFFu]);
-        return s_wq[k][(qrow[p >> 5] >> (31 - (p & 31))) & 1u];
-    };
-
     const bool persistent = V <= nstage;      // all rows stay staged across rebuilds
     int nalive = V;
     if (persistent) {
@@ -1130,7 +1134,7 @@ msa_anchor(const DevOptions& o, const DevReads& r, uint32_t first, uint32_t ai,
         //      consensus (findConsensus, msa.cpp:135-157): each warp takes one
         //      32-column block at a time, lane = column ----
 #pragma unroll 1
-        for (int j = 0; j < JB; ++j) {
+        for (int j = 0; j < jb; ++j) {
             const int c0 = 32 * (warp + NWARP * j);
             const int col = c0 + lane;
             const bool active = c0 < ncols;                  // warp-uniform
@@ -1153,46 +1157,56 @@ msa_anchor(const DevOptions& o, const DevReads& r, uint32_t first, uint32_t ai,
                 }
             }
             // staged rows (slot list[i], or slot i) meeting this block, in
-            // list order; up to four rows load together, then add in order
+            // list order: per chunk of 32 rows the warp lists the rows that
+            // meet the block (ballot, order kept) as {row word offset | slot
+            // << 16 | length << 23, first position - lane}; up to four listed
+            // rows load together, then add in order
             auto run_rows = [&](const uint8_t* list, int nrows) {
                 for (int i0 = 0; i0 < nrows; i0 += 32) {
                     bool hit = false;
+                    uint2 ent = make_uint2(0u, 0u);
                     if (i0 + lane < nrows) {
                         const int k = list ? list[i0 + lane] : i0 + lane;
                         const int2 bl = s_bl[k];
                         const int cb = abegin + bl.x;
                         hit = cb < c0 + 32 && cb + bl.y > c0;
+                        ent = make_uint2((uint32_t)(k * rw) | ((uint32_t)k << 16) | ((uint32_t)bl.y << 23),
+                                         (uint32_t)(c0 - cb));
                     }
-                    unsigned m = __ballot_sync(0xffffffffu, hit);
-                    while (m) {
+                    const unsigned m = __ballot_sync(0xffffffffu, hit);
+                    if (hit) s_hits[warp][__popc(m & ((1u << lane) - 1u))] = ent;
+                    __syncwarp();
+                    const int nh = __popc(m);
+                    for (int h0 = 0; h0 < nh; h0 += 4) {
                         bool v[4];
                         uint32_t bb[4];
                         float ww[4];
-                        int nu = 0;
 #pragma unroll
                         for (int u = 0; u < 4; ++u) {
                             v[u] = false;
                             bb[u] = 0u;
                             ww[u] = 0.0f;
-                            if (m) {                             // warp-uniform
-                                const int i = i0 + __ffs(m) - 1;
-                                m &= m - 1;
-                                ++nu;
-                                const int k = list ? list[i] : i;
-                                const int2 bl = s_bl[k];
-                                const int p = col - (abegin + bl.x);
-                                const bool in = (unsigned)p < (unsigned)bl.y;
+                            if (h0 + u < nh) {                   // warp-uniform
+                                const uint2 e = s_hits[warp][h0 + u];
+                                const int p = lane + (int)e.y;
+                                const bool in = (unsigned)p < (e.x >> 23);
                                 const int pc = in ? p : 0;          // loads stay inside the row
-                                const float w = useQ ? cand_weight(k, pc) : s_w[k];
+                                const uint32_t* row = s_raw + (e.x & 0xFFFFu);
+                                const int k = (e.x >> 16) & 0x7F;
+                                const int wi = pc >> 4, sh = 30 - 2 * (pc & 15);
+                                bb[u] = (row[wi] >> sh) & 3u;
+                                if constexpr (QB == 0) ww[u] = s_w[k];
+                                else if constexpr (QB == 2) ww[u] = s_wq[k][(row[sp + wi] >> sh) & 3u];
+                                else if constexpr (QB == 1) ww[u] = s_wq[k][(row[sp + (pc >> 5)] >> (31 - (pc & 31))) & 1u];
+                                else ww[u] = fmul_rn(s_w[k], s_qw[(row[sp + (pc >> 2)] >> (8 * (pc & 3))) & 0xFFu]);
                                 v[u] = in;
-                                bb[u] = cand_base(k, pc);
-                                ww[u] = w;
                             }
                         }
 #pragma unroll
                         for (int u = 0; u < 4; ++u)
-                            if (u < nu) add(bb[u], ww[u], v[u]);
+                            if (h0 + u < nh) add(bb[u], ww[u], v[u]);
                     }
+                    __syncwarp();
                 }
             };
             if (persistent) {
@@ -1223,8 +1237,7 @@ msa_anchor(const DevOptions& o, const DevReads& r, uint32_t first, uint32_t ai,
                 const uint32_t nA = cAC & 0xFFFFu, nC = cAC >> 16;
                 const uint32_t nG = cGT & 0xFFFFu, nT = cGT >> 16;
                 s_cov[col] = (uint16_t)(nA + nC + nG + nT);
-                s_cnt[col][0] = (uint16_t)nA; s_cnt[col][1] = (uint16_t)nC;
-                s_cnt[col][2] = (uint16_t)nG; s_cnt[col][3] = (uint16_t)nT;
+                s_cnt4[col] = make_ushort4((uint16_t)nA, (uint16_t)nC, (uint16_t)nG, (uint16_t)nT);
                 if constexpr (EMIT) {
                     const int p = col - abegin;
                     if (p >= 0 && p < La) {
@@ -1250,7 +1263,7 @@ msa_anchor(const DevOptions& o, const DevReads& r, uint32_t first, uint32_t ai,
             const int cs = s_cons[col];
             bool sig = false;
 #pragma unroll
-            for (int b = 0; b < 4; ++b) sig |= (b != cs && sigThr <= (int)s_cnt[col][b]);
+            for (int b = 0; b < 4; ++b) sig |= (b != cs && sigThr <= cnt_of(col, b));
             if (sig) atomicMin(&s_vals[1], col);
         }
         __syncthreads();
@@ -1259,7 +1272,7 @@ msa_anchor(const DevOptions& o, const DevReads& r, uint32_t first, uint32_t ai,
         int foundBase = -1;                   // the last qualifying base index wins (:591-601)
         {
             const int cs = s_cons[col];
-            for (int b = 0; b < 4; ++b) if (b != cs && sigThr <= (int)s_cnt[col][b]) foundBase = b;
+            for (int b = 0; b < 4; ++b) if (b != cs && sigThr <= cnt_of(col, b)) foundBase = b;
         }
         const int orig = s_aelem[col - abegin] & 3u;
         const bool keepMatching = orig == foundBase;
@@ -1412,7 +1425,7 @@ msa_anchor(const DevOptions& o, const DevReads& r, uint32_t first, uint32_t ai,
         uint32_t cb;
         if (allGood) cb = s_cons[col];
         else {
-            const int oc = s_cnt[col][ob];    // origCoverages: count of the anchor's base
+            const int oc = cnt_of(col, ob);   // origCoverages: count of the anchor's base
             cb = (s_support[col] > 0.90f && oc <= 2) ? s_cons[col] : ob;
         }
         aout[p] = "ACGT"[cb];
@@ -1458,7 +1471,7 @@ msa_anchor(const DevOptions& o, const DevReads& r, uint32_t first, uint32_t ai,
                 const uint32_t ob = s_aelem[p] & 3u, cb = s_cons[col];
                 if (ob == cb || (int)s_cov[col] < o.clf_min_coverage) continue;
                 const float cov = (float)s_cov[col];
-                const int oc = s_cnt[col][ob], cc = s_cnt[col][cb];
+                const int oc = cnt_of(col, ob), cc = cnt_of(col, cb);
                 const float wsum = s_fw[p], wc = s_fw[mlen + p], wo = s_fw[2 * mlen + p];
                 float x[kNumFeatures];
                 x[0] = fdiv_rn((float)oc, cov);
@@ -1545,23 +1558,23 @@ msa_anchor(const DevOptions& o, const DevReads& r, uint32_t first, uint32_t ai,
 
 // One CTA per anchor, in `order` (e.g. most candidates first) when given;
 // the hardware block scheduler hands out the anchors.
-template <int BLOCK, int JB, bool EMIT = false>
+template <int BLOCK, int QB, bool EMIT = false>
 __global__ void __launch_bounds__(BLOCK, (EMIT ? 768 : 1024) / BLOCK)
-k_msa(DevOptions o, DevReads r, uint32_t first, uint32_t count, const uint32_t* __restrict__ order,
+k_msa(DevOptions o, DevReads r, uint32_t first, uint32_t count, int jb, const uint32_t* __restrict__ order,
       const uint32_t* __restrict__ cand_ids, const uint32_t* __restrict__ seg_off,
       const uint32_t* __restrict__ seg_cnt, const AlignRes* __restrict__ ares,
       CandRec* __restrict__ recs, MsaOut out, int* __restrict__ status) {
     if (blockIdx.x >= count) return;
     if (*status & kStatusCandOverflow) return;   // batch is repeated with a larger arena
-    msa_anchor<BLOCK, JB, EMIT>(o, r, first, order ? order[blockIdx.x] : blockIdx.x, cand_ids, seg_off,
+    msa_anchor<BLOCK, QB, EMIT>(o, r, first, order ? order[blockIdx.x] : blockIdx.x, jb, cand_ids, seg_off,
                                 seg_cnt, ares, recs, out, status);
 }
 
 // Persistent form: a grid of resident CTAs pulls anchors from a device work
 // queue (an atomic cursor over `order`) until the batch is done.
-template <int BLOCK, int JB, bool EMIT = false>
+template <int BLOCK, int QB, bool EMIT = false>
 __global__ void __launch_bounds__(BLOCK, (EMIT ? 768 : 1024) / BLOCK)
-k_msa_queue(DevOptions o, DevReads r, uint32_t first, uint32_t count, const uint32_t* __restrict__ order,
+k_msa_queue(DevOptions o, DevReads r, uint32_t first, uint32_t count, int jb, const uint32_t* __restrict__ order,
             unsigned int* __restrict__ cursor, const uint32_t* __restrict__ cand_ids,
             const uint32_t* __restrict__ seg_off, const uint32_t* __restrict__ seg_cnt,
             const AlignRes* __restrict__ ares, CandRec* __restrict__ recs, MsaOut out,
@@ -1574,7 +1587,7 @@ k_msa_queue(DevOptions o, DevReads r, uint32_t first, uint32_t count, const uint
         __syncthreads();
         const uint32_t it = s_item;
         if (it >= count) return;
-        msa_anchor<BLOCK, JB, EMIT>(o, r, first, order ? order[it] : it, cand_ids, seg_off, seg_cnt, ares,
+        msa_anchor<BLOCK, QB, EMIT>(o, r, first, order ? order[it] : it, jb, cand_ids, seg_off, seg_cnt, ares,
                                     recs, out, status);
     }
 }

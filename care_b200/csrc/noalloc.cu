@@ -212,22 +212,20 @@ extern "C" int care_b200_correct_range_noalloc(const care_b200_options* opt, con
         maxcols = c > maxcols ? c : maxcols;
     }
     const int jb = (maxcols + 127) / 128;
-    const size_t msmem = msa_smem_bytes(r.max_len, r.seq_pitch, r.qual_pitch);
-#define LAUNCH_MSA(JB)                                                                                   \
+    const size_t msmem = msa_smem_bytes(r.max_len, r.seq_pitch, r.qual_pitch, false, 128 * jb);
+#define LAUNCH_MSA(QB)                                                                                   \
     do {                                                                                                  \
-        if (cudaFuncSetAttribute(k_msa<128, JB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)msmem) \
+        if (cudaFuncSetAttribute(k_msa<128, QB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)msmem) \
             != cudaSuccess)                                                                               \
             return CARE_B200_ECUDA;                                                                       \
-        k_msa<128, JB><<<num_anchors, 128, msmem, st>>>(o, r, first_anchor, num_anchors, nullptr,         \
+        k_msa<128, QB><<<num_anchors, 128, msmem, st>>>(o, r, first_anchor, num_anchors, jb, nullptr,     \
                                                         cand_ids, seg_off, seg_cnt, ares, recs, mo,       \
                                                         dstatus);                                         \
     } while (0)
-    if (jb <= 1) LAUNCH_MSA(1);
-    else if (jb <= 2) LAUNCH_MSA(2);
-    else if (jb <= 3) LAUNCH_MSA(3);
-    else if (jb <= 4) LAUNCH_MSA(4);
-    else if (jb <= 5) LAUNCH_MSA(5);
-    else LAUNCH_MSA(6);
+    if (!o.use_quality) LAUNCH_MSA(0);
+    else if (o.quality_bits == 1) LAUNCH_MSA(1);
+    else if (o.quality_bits == 2) LAUNCH_MSA(2);
+    else LAUNCH_MSA(8);
 #undef LAUNCH_MSA
     if (cudaGetLastError() != cudaSuccess) return CARE_B200_ECUDA;
     int hstatus = 0;
