@@ -35,6 +35,11 @@ src/dispatch_care_correct_cpu.cpp:157-168; reads/s = reads / STEP2 time).
           reads of 50-250 bp at 40x (~2.7M reads), same error and quality
           model; -c 40 -k 20 -h 32 -q --qualityScoreBits 2 --pairmode SE.
 
+Blocks of the default run (pe, one GPU; --no-extra skips them): `uneven` and
+`large`, the two other workloads below with their committed tunings, a few
+steps each (min(steps, 5) after min(warmup, 3)), timed like `value`; the large
+block also carries plain and learned base-level counts.
+
 Multi-GPU: one process per GPU; each rank corrects its own read set
 (independent genome partitions, no data-path collective) -> weak scaling.
 """
@@ -291,6 +296,62 @@ def timed_steps(corr, n, steps, flush):
     return float(np.mean(dev_ms)), stage / steps, t_wall / steps * 1e3
 
 
+def workload_block(kind: str, steps: int, warmup: int, flush, local: int, tmp: str, learned: bool) -> dict:
+    """Another workload of the same metric as a block of the line: its own
+    seeded read set and options, the committed tuning, the same timing as
+    `value` (device time of whole passes, L2 flushed between steps); for the
+    large set also base-level counts of the plain and learned forms."""
+    import care_b200
+    from care_b200 import autotune, datagen
+    genome = {"uneven": 10_000_000, "large": 50_000_000}[kind]
+    run_args = {"uneven": ARGS_UNEVEN, "large": ARGS_LARGE}[kind]
+    progress(f"{kind} block: generating reads")
+    rs = workload(0, genome, kind)
+    n = rs.num_reads
+    fq = os.path.join(tmp, f"{kind}.fq")
+    datagen.write_fastq_fast(rs, fq)
+    tuned = autotune.load(kind)
+    forms = [("plain", 0)] + ([("learned", 1)] if learned and kind == "large" and os.path.exists(MLP_FILE_LARGE) else [])
+    out = {"workload": workload_config(argparse.Namespace(workload=kind, genome=genome))["workload"],
+           "reads": n, "args": run_args, "steps": steps, "warmup": warmup, "tuning": tuned,
+           "timing": "as value: device time of whole passes, inputs resident, L2 flushed between steps"}
+    for name, ctype in forms:
+        c = care_b200.Corrector(care_b200.options_from_args(run_args, device=local, correction_type=ctype))
+        if ctype:
+            from care_b200 import learned as lrn
+            c.set_mlp(lrn.load_params(MLP_FILE_LARGE))
+        if tuned:
+            c.tuning = tuned
+        t0 = time.perf_counter()
+        c.load_files([fq])
+        c.build_tables()
+        step1 = time.perf_counter() - t0
+        for _ in range(warmup):
+            c.correct_range_device(0, n)
+        import torch
+        torch.cuda.synchronize()
+        ms, stage, _ = timed_steps(c, n, steps, flush)
+        st = c.last_stats()
+        blk = {"value": n / (ms / 1e3), "unit": "reads/s", "ms_per_step": ms,
+               "stage_ms": {"candidates": stage[0], "align": stage[1], "msa": stage[2], "classifier": stage[3]},
+               "pairs_per_step": st["pairs"], "step1_s": step1, "gpu_launches": st["launches"] * steps}
+        if kind == "large":
+            progress(f"{kind} block: {name} base-level counts")
+            c.correct_range(0, n)
+            o = os.path.join(tmp, f"{kind}_{name}.fq")
+            c.write_output(o)
+            tp, fp, fn, tn = base_counts(rs, o)
+            blk["base_level"] = {"tp": tp, "fp": fp, "fn": fn, "f1": datagen.f1(tp, fp, fn)}
+            os.unlink(o)
+        c.close()
+        out[name] = blk
+        progress(f"{kind} block: {name} {blk['value'] / 1e6:.2f}M reads/s")
+    if "learned" in out:
+        out["learned"]["ratio_vs_plain"] = out["learned"]["value"] / out["plain"]["value"]
+    os.unlink(fq)
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -301,6 +362,8 @@ def main():
     ap.add_argument("--genome", type=int, default=None, help="bp (default 5 Mbp, uneven 10 Mbp, large 50 Mbp)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned", action="store_true")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="skip the uneven and large workload blocks of the default (pe, 1 GPU) run")
     ap.add_argument("--tuning", default="auto", choices=["auto", "default"],
                     help="auto: the committed launch mapping of the workload (care_b200/tuning/)")
     args = ap.parse_args()
@@ -555,6 +618,16 @@ def main():
                                 "per_core_sample": "care-cpu -t 1 on 250 kbp genome, 50,000 reads, PE model",
                                 "cpu_model": cpu_model()}
     corr.close()
+    if rank == 0 and world == 1 and args.workload == "pe" and not args.no_extra:
+        # the batched uneven set and the large set, a few steps each
+        del rs
+        ks, kw = min(args.steps, 5), min(args.warmup, 3)
+        for kind in ("uneven", "large"):
+            try:
+                line[kind] = workload_block(kind, ks, kw, flush, local, tmp, learned=not args.no_learned)
+            except Exception as e:           # the main line is still printed
+                line[kind] = {"error": f"{type(e).__name__}: {e}"}
+                progress(f"{kind} block failed: {e}")
     shutil.rmtree(tmp, ignore_errors=True)
     if world > 1:
         dist.barrier()

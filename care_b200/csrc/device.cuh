@@ -293,6 +293,9 @@ CB_HD void shd_scan(uint32_t (&Sh)[NW + 2], uint32_t (&Sl)[NW + 2],
                                          Cnt* cnt = nullptr) {
     if (t1 < t0) return;
     bool stop = false;
+    // overlap at shift t: min(A - t, B) in both directions
+    const int A = sign > 0 ? La : Lc, B = sign > 0 ? Lc : La;
+    int bt = best - total;
 #pragma unroll 1
     for (int w = 0; w <= (t1 >> 5) && !stop; ++w) {
         const int rb = (w == (t0 >> 5)) ? (t0 & 31) : 0;
@@ -300,8 +303,8 @@ CB_HD void shd_scan(uint32_t (&Sh)[NW + 2], uint32_t (&Sl)[NW + 2],
 #pragma unroll 1
         for (int r = rb; r <= re; ++r) {
             const int t = 32 * w + r;
-            const int ov = sign > 0 ? min(La - t, Lc) : min(La, Lc - t);
-            const int mex = min(mextab[ov], best - total + 2 * ov);
+            const int ov = min(A - t, B);
+            const int mex = min(mextab[ov], bt + 2 * ov);
             if (mex <= 0) { stop = true; break; }
             uint32_t d0 = (funnel_l(Sh[1], Sh[0], r) ^ Oh[0]) | (funnel_l(Sl[1], Sl[0], r) ^ Ol[0]);
             uint32_t d1 = (funnel_l(Sh[2], Sh[1], r) ^ Oh[1]) | (funnel_l(Sl[2], Sl[1], r) ^ Ol[1]);
@@ -320,9 +323,11 @@ CB_HD void shd_scan(uint32_t (&Sh)[NW + 2], uint32_t (&Sl)[NW + 2],
                     }
                 }
             }
+            // mm < mex <= best - total + 2*ov: the score improves on the best
             if (mm < mex) {
-                const int sc = mm + total - 2 * ov;
-                if (sc < best) { best = sc; bestShift = sign * t; }
+                bt = mm - 2 * ov;
+                best = bt + total;
+                bestShift = sign * t;
             }
         }
         // slide the shifted planes by one 32-base word
