@@ -73,7 +73,7 @@ EXPORTS = [
     "care_b200_last_error", "care_b200_upload_reads", "care_b200_upload_tables",
     "care_b200_build_tables", "care_b200_get_table", "care_b200_correct_range",
     "care_b200_correct_range_device", "care_b200_serialize_results",
-    "care_b200_load_reads_from_files", "care_b200_write_output", "care_b200_last_timing",
+    "care_b200_load_reads_from_files", "care_b200_load_reads_from_files_device", "care_b200_write_output", "care_b200_last_timing",
     "care_b200_last_stats", "care_b200_count_word_compares", "care_b200_load_preprocessed_reads",
     "care_b200_save_preprocessed_reads", "care_b200_load_hashtables", "care_b200_save_hashtables", "care_b200_num_reads", "care_b200_max_length", "care_b200_num_maps",
     "care_b200_result_threshold",
@@ -173,6 +173,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.care_b200_serialize_results.argtypes = [c_ctx, P(Results), P(ctypes.c_uint8), ctypes.c_size_t,
                                                 P(ctypes.c_size_t)]
     lib.care_b200_load_reads_from_files.argtypes = [c_ctx, P(ctypes.c_char_p), ctypes.c_int]
+    lib.care_b200_load_reads_from_files_device.argtypes = [c_ctx, P(ctypes.c_char_p), ctypes.c_int]
     lib.care_b200_write_output.argtypes = [c_ctx, ctypes.c_char_p]
     lib.care_b200_last_timing.argtypes = [c_ctx, P(ctypes.c_float), P(ctypes.c_float), ctypes.c_int]
     lib.care_b200_last_stats.argtypes = [c_ctx, P(ctypes.c_uint64), ctypes.c_int]
@@ -292,9 +293,15 @@ class Corrector:
             self._ctx, _ptr(packed, ctypes.c_uint32), packed.shape[1], _ptr(lengths, ctypes.c_int32),
             qp, qpitch, _ptr(amb, ctypes.c_uint32), amb.shape[0], packed.shape[0]), "upload_reads")
 
-    def load_files(self, files: Sequence[str]):
+    def load_files(self, files: Sequence[str], device: bool = False):
+        """STEP1 from FASTQ/FASTA files; device=True parses and encodes on the
+        GPU (strict 4-line FASTQ / 2-line FASTA; CareError otherwise)."""
         arr = (ctypes.c_char_p * len(files))(*[f.encode() for f in files])
-        self._check(self.lib.care_b200_load_reads_from_files(self._ctx, arr, len(files)), "load_reads_from_files")
+        if device:
+            self._check(self.lib.care_b200_load_reads_from_files_device(self._ctx, arr, len(files)),
+                        "load_reads_from_files_device")
+        else:
+            self._check(self.lib.care_b200_load_reads_from_files(self._ctx, arr, len(files)), "load_reads_from_files")
 
     def load_preprocessed_reads(self, path: str):
         """Read storage from a file written by care-cpu --save-preprocessedreads-to

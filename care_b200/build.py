@@ -27,7 +27,7 @@ NVFLAGS = ARCH + ["-O3", "-lineinfo", "--fmad=false", "-std=c++17", "-Xcompiler"
                   "-Xptxas", "-warn-spills"]
 CXXFLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-Wall", "-Wextra"]
 
-CU_SOURCES = ["capi.cu", "noalloc.cu", "mlp.cu", "tables.cu"]
+CU_SOURCES = ["capi.cu", "noalloc.cu", "mlp.cu", "tables.cu", "parse.cu"]
 CXX_SOURCES = ["hostio.cpp", "readfile.cpp"]
 
 

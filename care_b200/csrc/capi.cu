@@ -5,6 +5,7 @@
 #include "readfile.hpp"
 #include "kernels.cuh"
 #include "mlp.hpp"
+#include "parse.hpp"
 #include "tables.hpp"
 
 #include <algorithm>
@@ -111,6 +112,7 @@ struct care_b200_ctx {
     DBuf d_cid, d_canc, d_cshift, d_cue, d_cseq;
     unsigned long long corr_cap = 0;
     HBuf h_small;
+    HBuf h_text;                      // input files' bytes (records parsed on the device point into it)
     // host -> device staging of uploads: two pinned chunks per copy stream
     HBuf h_stage[2][2];
     cudaEvent_t stage_ev[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
@@ -1373,6 +1375,103 @@ static int care_b200_load_reads_from_files_impl(care_b200_ctx* ctx, const char* 
     return care_b200_upload_reads(ctx, h.seq.data(), h.seq_pitch, h.len.data(),
                                   h.has_quality ? h.qual.data() : nullptr, h.qual_pitch,
                                   h.ambiguous_ids.data(), h.ambiguous_ids.size(), h.n);
+}
+
+static int care_b200_load_reads_from_files_device_impl(care_b200_ctx* ctx, const char* const* files, int num_files);
+
+// host allocations that fail are returned as CARE_B200_ENOMEM: nothing is
+// thrown across the C ABI
+int care_b200_load_reads_from_files_device(care_b200_ctx* ctx, const char* const* files, int num_files) {
+    try {
+        return care_b200_load_reads_from_files_device_impl(ctx, files, num_files);
+    } catch (const std::exception& e) {
+        return ctx ? fail(ctx, CARE_B200_ENOMEM, std::string("care_b200_load_reads_from_files_device: ") + e.what())
+                   : CARE_B200_ENOMEM;
+    }
+}
+
+static int care_b200_load_reads_from_files_device_impl(care_b200_ctx* ctx, const char* const* files, int num_files) {
+    if (!ctx || !files || num_files < 1 || num_files > 2) return CARE_B200_EINVAL;
+    CK(cudaSetDevice(ctx->opt.device), "cudaSetDevice");
+    // the files one after the other in pinned memory, each ending with a line end
+    size_t sizes[2] = {0, 0}, begin[2] = {0, 0}, total = 0;
+    std::FILE* fp[2] = {nullptr, nullptr};
+    auto close_all = [&]() { for (auto& f : fp) if (f) { std::fclose(f); f = nullptr; } };
+    for (int f = 0; f < num_files; f++) {
+        fp[f] = std::fopen(files[f], "rb");
+        if (!fp[f]) { close_all(); return fail(ctx, CARE_B200_EIO, std::string("cannot read input file ") + files[f]); }
+        std::fseek(fp[f], 0, SEEK_END);
+        const long sz = std::ftell(fp[f]);
+        std::fseek(fp[f], 0, SEEK_SET);
+        sizes[f] = sz > 0 ? (size_t)sz : 0;
+        begin[f] = total;
+        total += sizes[f] + 1;
+    }
+    if (ctx->h_text.ensure(total) != cudaSuccess) { close_all(); return fail(ctx, CARE_B200_ENOMEM, "pinned input buffer"); }
+    char* text = ctx->h_text.as<char>();
+    size_t used = 0;
+    for (int f = 0; f < num_files; f++) {
+        begin[f] = used;
+        if (sizes[f] && std::fread(text + used, 1, sizes[f], fp[f]) != sizes[f]) {
+            close_all();
+            return fail(ctx, CARE_B200_EIO, std::string("cannot read input file ") + files[f]);
+        }
+        used += sizes[f];
+        if (sizes[f] == 0 || text[used - 1] != '\n') text[used++] = '\n';
+    }
+    close_all();
+    DeviceParsed dp;
+    const std::string e = parse_on_device(text, used, begin, num_files, ctx->opt.paired_end != 0, ctx->opt.use_quality != 0,
+                                          ctx->opt.quality_bits, kMaxLen, ctx->stream, dp);
+    if (!e.empty()) {
+        dp.release();
+        if (e == "irregular")
+            return fail(ctx, CARE_B200_EINVAL, "records not in strict 4-line FASTQ / 2-line FASTA layout "
+                                               "(care_b200_load_reads_from_files reads them)");
+        return fail(ctx, e.rfind("reads longer", 0) == 0 ? CARE_B200_ELIMIT : CARE_B200_EIO, e);
+    }
+    if (ctx->opt.paired_end && (dp.n % 2)) {
+        dp.release();
+        return fail(ctx, CARE_B200_EINVAL, "paired-end storage needs an even number of reads");
+    }
+    // the device arrays become the read storage
+    ctx->d_seq.adopt(dp.seq, (size_t)dp.n * dp.seq_pitch * 4);
+    ctx->d_len.adopt(dp.len, (size_t)dp.n * 4);
+    ctx->d_ambig.adopt(dp.ambig, dp.n);
+    if (dp.has_quality) ctx->d_qual.adopt(dp.qual, (size_t)dp.n * dp.qual_pitch * 4);
+    ctx->n = dp.n;
+    ctx->max_len = dp.max_len;
+    ctx->seq_pitch = dp.seq_pitch;
+    ctx->has_qual = dp.has_quality;
+    ctx->qual_pitch = dp.has_quality ? dp.qual_pitch : 0;
+    ctx->h_len = dp.h_len;
+    ctx->h_ambig = dp.h_ambig;
+    HostReads& h = ctx->reads;
+    h = HostReads{};
+    h.n = dp.n;
+    h.min_len = dp.min_len;
+    h.max_len = dp.max_len;
+    h.seq_pitch = dp.seq_pitch;
+    h.qual_pitch = dp.qual_pitch;
+    h.quality_bits = ctx->opt.quality_bits;
+    h.has_quality = dp.has_quality;
+    h.fasta = dp.fasta;
+    h.seq = std::move(dp.h_seq);
+    h.len = std::move(dp.h_len);
+    h.ambig = std::move(dp.h_ambig);
+    for (uint32_t i = 0; i < h.n; i++) if (h.ambig[i]) h.ambiguous_ids.push_back(i);
+    h.raw = text;
+    h.rec_h = std::move(dp.rec_h);
+    h.rec_hl = std::move(dp.rec_hl);
+    h.rec_s = std::move(dp.rec_s);
+    h.rec_q = std::move(dp.rec_q);
+    ctx->have_records = true;
+    ctx->sigs_maps = 0;
+    if (int rc = compute_signatures(ctx, ctx->num_maps ? ctx->num_maps : ctx->opt.num_maps)) return rc;
+    CK(cudaStreamSynchronize(ctx->stream), "signatures");
+    if (ctx->tables_ready && ctx->t_keys.size() && h.n != ctx->tables_reads) ctx->tables_ready = false;
+    ctx->r_valid = false;
+    return CARE_B200_OK;
 }
 
 static int care_b200_load_preprocessed_reads_impl(care_b200_ctx* ctx, const char* path);

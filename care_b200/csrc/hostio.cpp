@@ -352,10 +352,22 @@ std::string write_corrected(const HostReads& reads, const HostCorrections& c, bo
             } else std::memcpy(o, seq, (size_t)L);
         };
         for (uint32_t i = b; i < e; i++) {
-            const char* h = reads.text.data() + reads.rec_off[i];
-            const char* s = h + std::strlen(h) + 1;
-            const char* q = s + std::strlen(s) + 1;
             const int L = reads.len[i];
+            const char *h, *s, *q;
+            size_t hl, ql;
+            if (reads.raw) {
+                h = reads.raw + reads.rec_h[i];
+                hl = reads.rec_hl[i];
+                s = reads.raw + reads.rec_s[i];
+                q = reads.raw + reads.rec_q[i];
+                ql = reads.fasta ? 0 : (size_t)L;
+            } else {
+                h = reads.text.data() + reads.rec_off[i];
+                hl = std::strlen(h);
+                s = h + hl + 1;
+                q = s + std::strlen(s) + 1;
+                ql = std::strlen(q);
+            }
             std::memcpy(outseq.data(), s, (size_t)L);
             const uint64_t cb = cstart[i], ce = cstart[i + 1];
             const uint64_t ncand = ce - cb;
@@ -390,12 +402,12 @@ std::string write_corrected(const HostReads& reads, const HostCorrections& c, bo
                 }
             }
             buf.push_back(reads.fasta ? '>' : '@');
-            buf.append(h);
+            buf.append(h, hl);
             if (quality_labels && (int64_t)i <= last) { buf.append(" care:q="); buf.push_back((char)('0' + (corrected ? label : 0))); }
             buf.push_back('\n');
             buf.append(outseq.data(), (size_t)L);
             buf.push_back('\n');
-            if (!reads.fasta) { buf.append("+\n"); buf.append(q); buf.push_back('\n'); }
+            if (!reads.fasta) { buf.append("+\n"); buf.append(q, ql); buf.push_back('\n'); }
         }
     };
     // blocks of reads formatted by threads, written in read order

@@ -24,6 +24,12 @@ struct HostReads {
     // original records for output: header, sequence, quality, NUL separated
     std::vector<char> text;
     std::vector<size_t> rec_off;
+    // or (records parsed on the device) offsets into the input files' bytes:
+    // header (after '@' / '>', without the line end), sequence, quality
+    // (both of the read's length)
+    const char* raw = nullptr;
+    std::vector<uint64_t> rec_h, rec_s, rec_q;
+    std::vector<uint32_t> rec_hl;
 };
 
 // Returns an empty string on success, else an error message.

@@ -781,7 +781,8 @@ msa_anchor(const DevOptions& o, const DevReads& r, uint32_t first, uint32_t ai, 
     const int MAXCOLS = 32 * jb * NWARP;
     extern __shared__ __align__(16) unsigned char dsm[];
     __shared__ float s_qw[256];
-    __shared__ uint2 s_hits[NWARP][32];      // per warp: the staged rows meeting its column block
+    __shared__ uint2 s_hits[NWARP][36];      // per warp: the staged rows meeting its column block
+    __shared__ int s_blk;                    // next column block (persistent rows: warps take blocks in turn)
     __shared__ float s_qwc[4];               // weight of a 1- or 2-bit quality code
     __shared__ int s_beg[kStageMax], s_len[kStageMax];
     __shared__ float s_w[kStageMax];
@@ -823,6 +824,10 @@ msa_anchor(const DevOptions& o, const DevReads& r, uint32_t first, uint32_t ai, 
         if (tid == 0) { out.status[ai] = 0; out.nedits[ai] = 0; }
         return;
     }
+
+    // the padding entries of the hit lists stay zero: a group of four rows
+    // reads them, with its element adds switched off, past a list's end
+    for (int i = tid; i < NWARP * 36; i += BLOCK) (&s_hits[0][0])[i] = make_uint2(0u, 0u);
 
     auto block_sum4 = [&](int v0, int v1, int v2, int v3, int* res) {
 #pragma unroll
@@ -1108,6 +1113,7 @@ msa_anchor(const DevOptions& o, const DevReads& r, uint32_t first, uint32_t ai, 
             mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, d));
             sl += __shfl_xor_sync(0xffffffffu, sl, d);
         }
+        if (tid == 0) s_blk = 0;             // the previous build's sums are done (CTA barrier after them)
         __syncthreads();
         if (lane == 0) { s_red[warp][0] = mn; s_red[warp][1] = mx; s_red[warp][2] = sl; }
         __syncthreads();
@@ -1133,9 +1139,22 @@ msa_anchor(const DevOptions& o, const DevReads& r, uint32_t first, uint32_t ai, 
         // ---- column sums (anchor first, then candidates in list order) and
         //      consensus (findConsensus, msa.cpp:135-157): each warp takes one
         //      32-column block at a time, lane = column ----
+        // persistent rows: the warps take the column blocks in turn from a
+        // shared counter (blocks differ in their row counts); rows staged in
+        // chunks: every warp runs its jb blocks (staging synchronises the CTA)
+        const int nblk = (ncols + 31) >> 5;
 #pragma unroll 1
-        for (int j = 0; j < jb; ++j) {
-            const int c0 = 32 * (warp + NWARP * j);
+        for (int j = 0;; ++j) {
+            int blk;
+            if (persistent) {
+                if (lane == 0) blk = atomicAdd(&s_blk, 1);
+                blk = __shfl_sync(0xffffffffu, blk, 0);
+                if (blk >= nblk) break;
+            } else {
+                if (j >= jb) break;
+                blk = warp + NWARP * j;
+            }
+            const int c0 = 32 * blk;
             const int col = c0 + lane;
             const bool active = c0 < ncols;                  // warp-uniform
             uint32_t cAC = 0u, cGT = 0u;                     // 16-bit counts: A | C << 16, G | T << 16
@@ -1181,30 +1200,26 @@ msa_anchor(const DevOptions& o, const DevReads& r, uint32_t first, uint32_t ai, 
                         bool v[4];
                         uint32_t bb[4];
                         float ww[4];
+                        // branch free: entries past the list (zero, or an
+                        // earlier chunk's) load in bounds and add nothing
 #pragma unroll
                         for (int u = 0; u < 4; ++u) {
-                            v[u] = false;
-                            bb[u] = 0u;
-                            ww[u] = 0.0f;
-                            if (h0 + u < nh) {                   // warp-uniform
-                                const uint2 e = s_hits[warp][h0 + u];
-                                const int p = lane + (int)e.y;
-                                const bool in = (unsigned)p < (e.x >> 23);
-                                const int pc = in ? p : 0;          // loads stay inside the row
-                                const uint32_t* row = s_raw + (e.x & 0xFFFFu);
-                                const int k = (e.x >> 16) & 0x7F;
-                                const int wi = pc >> 4, sh = 30 - 2 * (pc & 15);
-                                bb[u] = (row[wi] >> sh) & 3u;
-                                if constexpr (QB == 0) ww[u] = s_w[k];
-                                else if constexpr (QB == 2) ww[u] = s_wq[k][(row[sp + wi] >> sh) & 3u];
-                                else if constexpr (QB == 1) ww[u] = s_wq[k][(row[sp + (pc >> 5)] >> (31 - (pc & 31))) & 1u];
-                                else ww[u] = fmul_rn(s_w[k], s_qw[(row[sp + (pc >> 2)] >> (8 * (pc & 3))) & 0xFFu]);
-                                v[u] = in;
-                            }
+                            const uint2 e = s_hits[warp][h0 + u];
+                            const int p = lane + (int)e.y;
+                            const bool in = h0 + u < nh && (unsigned)p < (e.x >> 23);
+                            const int pc = in ? p : 0;          // loads stay inside the row
+                            const uint32_t* row = s_raw + (e.x & 0xFFFFu);
+                            const int k = (e.x >> 16) & 0x7F;
+                            const int wi = pc >> 4, sh = 30 - 2 * (pc & 15);
+                            bb[u] = (row[wi] >> sh) & 3u;
+                            if constexpr (QB == 0) ww[u] = s_w[k];
+                            else if constexpr (QB == 2) ww[u] = s_wq[k][(row[sp + wi] >> sh) & 3u];
+                            else if constexpr (QB == 1) ww[u] = s_wq[k][(row[sp + (pc >> 5)] >> (31 - (pc & 31))) & 1u];
+                            else ww[u] = fmul_rn(s_w[k], s_qw[(row[sp + (pc >> 2)] >> (8 * (pc & 3))) & 0xFFu]);
+                            v[u] = in;
                         }
 #pragma unroll
-                        for (int u = 0; u < 4; ++u)
-                            if (h0 + u < nh) add(bb[u], ww[u], v[u]);
+                        for (int u = 0; u < 4; ++u) add(bb[u], ww[u], v[u]);
                     }
                     __syncwarp();
                 }

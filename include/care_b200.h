@@ -150,6 +150,19 @@ int care_b200_serialize_results(care_b200_ctx* ctx, const care_b200_results* res
  * and uploads the read storage. */
 int care_b200_load_reads_from_files(care_b200_ctx* ctx, const char* const* files, int num_files);
 
+/* The same storage, parsed and encoded on the device (STEP1's parse and
+ * encode, include/chunkedreadstorageconstruction.hpp:29-400 and
+ * include/qualityscorecompression.hpp:90-119): the files' bytes are copied
+ * to the device once, line ends and records are found by device scans, the
+ * N-rotation counter (restarting every 65,536-read parser batch) by a scan of
+ * each read's ambiguous characters, and every read is encoded by one warp.
+ * For records in strict 4-line FASTQ or 2-line FASTA layout (a missing last
+ * line end and CRLF line ends included); any other layout returns
+ * CARE_B200_EINVAL with the storage unchanged, and
+ * care_b200_load_reads_from_files reads it. The output records are written
+ * from the same bytes (care_b200_write_output). */
+int care_b200_load_reads_from_files_device(care_b200_ctx* ctx, const char* const* files, int num_files);
+
 /* Read-storage handle, binary file: uploads the read storage that care-cpu
  * saved with --save-preprocessedreads-to (ChunkedReadStorage::loadFromFile,
  * include/chunkedreadstorage.hpp:160-243), in place of parsing FASTQ. As in the
