@@ -90,7 +90,8 @@ class Tuning(ctypes.Structure):
     """care_b200_tuning: launch mapping of a batch (results do not depend on it)."""
     _fields_ = [("msa_order", ctypes.c_int), ("msa_queue", ctypes.c_int), ("msa_warps", ctypes.c_int),
                 ("align_block", ctypes.c_int), ("pair_order", ctypes.c_int), ("graph", ctypes.c_int),
-                ("pair_mirror", ctypes.c_int), ("cand_set_log2", ctypes.c_int), ("align_warp", ctypes.c_int)]
+                ("pair_mirror", ctypes.c_int), ("cand_set_log2", ctypes.c_int), ("align_warp", ctypes.c_int),
+                ("align_classes", ctypes.c_int)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -13,6 +13,8 @@ The knobs change how a batch is laid onto the GPU, never what it computes:
   (occupancy against anchors redone by the full-set pass)
 - align_warp  a warp per alignment work item (lanes take shifts) instead of
   a thread per work item
+- align_classes  pairs partitioned by the plane width of their longer read,
+  one alignment launch per width
 
 Coordinate descent from the default: each knob in turn takes the value with
 the lowest device time (CUDA events of the pipeline, mean of timed passes
@@ -49,9 +51,10 @@ KNOBS = {
     "pair_mirror": [0, 1],
     "cand_set_log2": [9, 10, 11],
     "align_warp": [0, 1],
+    "align_classes": [0, 1],
 }
 DEFAULT = {"msa_order": 0, "msa_queue": 0, "msa_warps": 4, "align_block": 128, "pair_order": 0, "graph": 0,
-           "pair_mirror": 0, "cand_set_log2": 10, "align_warp": 0}
+           "pair_mirror": 0, "cand_set_log2": 10, "align_warp": 0, "align_classes": 0}
 
 WORKLOADS = {
     "pe": ("-c 30 -k 20 -h 32 -q --qualityScoreBits 2 --pairmode PE", 5_000_000),

@@ -69,7 +69,7 @@ constexpr int kMsaBlock = 128;
 
 // The launch mapping of a new context: one kernel per stage in anchor order,
 // 4 MSA warps, 128-thread alignment CTAs, a 1024-entry candidate set.
-constexpr care_b200_tuning kDefaultTuning{0, 0, 4, 128, 0, 0, 0, 10, 0};
+constexpr care_b200_tuning kDefaultTuning{0, 0, 4, 128, 0, 0, 0, 10, 0, 0};
 
 // Largest candidate arena of one batch: pair indices and offsets are 32-bit.
 constexpr unsigned long long kMaxBatchPairs = 0xffffffffull;
@@ -129,7 +129,7 @@ struct care_b200_ctx {
 
     // launch mapping (care_b200_set_tuning) and its scratch
     care_b200_tuning tune = kDefaultTuning;
-    DBuf d_order, d_bins, d_pair_order, d_pair_work, d_spill;
+    DBuf d_order, d_bins, d_pair_order, d_pair_work, d_spill, d_pair_class, d_cls;
     cudaGraphExec_t gexec = nullptr;
     int sms = 0;
 
@@ -651,6 +651,7 @@ struct AlignArgs {
     unsigned long long* run_words;             // non-null: the statistics form, counting words run
     bool warp;                                 // k_align_warp: a warp per work item
     int sms;
+    const uint2* cls;                          // one length class of the pairs (pair_order = the class list)
 };
 
 template <int B, int NW, bool CNT>
@@ -669,6 +670,17 @@ cudaError_t align_go(const AlignArgs& a, cudaStream_t st) {
         return cudaGetLastError();
     }
     const unsigned long long blocks = (a.cap + B - 1) / B;
+    if (a.cls) {        // a length class: resident blocks striding over its pairs
+        int nb = 0;
+        const cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_align_class<B, NW, CNT>, B, 0);
+        if (e != cudaSuccess) return e;
+        const unsigned grid = (unsigned)std::max<unsigned long long>(
+            1, std::min<unsigned long long>(blocks, (unsigned long long)a.sms * std::max(nb, 1)));
+        k_align_class<B, NW, CNT><<<grid, B, 0, st>>>(a.o, a.r, a.first, a.cand_ids, a.cand_anchor, a.seg_off,
+                                                      a.seg_cnt, a.total, a.cap, a.status, a.out, a.words,
+                                                      a.pair_order, a.cls, a.run_words);
+        return cudaGetLastError();
+    }
     k_align<B, NW, CNT><<<(unsigned)blocks, B, 0, st>>>(a.o, a.r, a.first, a.cand_ids, a.cand_anchor, a.seg_off,
                                                         a.seg_cnt, a.total, a.cap, a.status, a.out, a.words,
                                                         a.pair_order, a.work, a.work_n, a.run_words);
@@ -801,6 +813,9 @@ int run_batch(care_b200_ctx* ctx, uint32_t first, uint32_t count, bool timed) {
     const int warps = tu.msa_warps == 8 ? 8 : 4;
     const int jb = (maxcols + 32 * warps - 1) / (32 * warps);
     const int nw = (ctx->max_len + 31) / 32;           // bit-plane width: 32-base words of the longest read
+    // length classes of the alignment (not with mirror pairs, whose work list pairs equal lengths)
+    const bool classes = tu.align_classes != 0 && tu.pair_mirror == 0;
+    if (classes) CK(ctx->d_cls.ensure(64), "alloc");
     const size_t msmem = msa_smem_bytes(ctx->max_len, ctx->seq_pitch, ctx->has_qual ? ctx->qual_pitch : 0, emit,
                                         32 * jb * warps);
     const int qb = ctx->has_qual ? ctx->opt.quality_bits : 0;
@@ -813,6 +828,7 @@ int run_batch(care_b200_ctx* ctx, uint32_t first, uint32_t count, bool timed) {
         CK(ctx->d_recs.ensure(cap * sizeof(CandRec)), "alloc records");
         if (tu.pair_order) CK(ctx->d_pair_order.ensure(cap * 4), "alloc pair order");
         if (tu.pair_mirror) CK(ctx->d_pair_work.ensure(cap * 8), "alloc mirror work list");
+        if (classes) CK(ctx->d_pair_class.ensure(cap * 4), "alloc pair classes");
         const unsigned long long ccap = ctx->corr_cap;
         CK(ctx->d_cid.ensure(ccap * 4), "alloc");
         CK(ctx->d_canc.ensure(ccap * 4), "alloc");
@@ -854,7 +870,7 @@ int run_batch(care_b200_ctx* ctx, uint32_t first, uint32_t count, bool timed) {
                      tu.pair_order ? ctx->d_pair_order.as<uint32_t>() : nullptr,
                      tu.pair_mirror ? ctx->d_pair_work.as<uint2>() : nullptr,
                      reinterpret_cast<const unsigned int*>(counters + 6),
-                     ctx->count_words ? counters + 8 : nullptr, tu.align_warp != 0, ctx->sms};
+                     ctx->count_words ? counters + 8 : nullptr, tu.align_warp != 0, ctx->sms, nullptr};
         MsaArgs ma{o, r, first, count, tu.msa_order ? ctx->d_order.as<uint32_t>() : nullptr,
                    reinterpret_cast<unsigned int*>(counters + 4), ctx->d_cand_ids.as<uint32_t>(),
                    ctx->d_seg_off.as<uint32_t>(), ctx->d_seg_cnt.as<uint32_t>(), ctx->d_ares.as<AlignRes>(),
@@ -917,8 +933,34 @@ int run_batch(care_b200_ctx* ctx, uint32_t first, uint32_t count, bool timed) {
                 EQ(cudaGetLastError(), "k_pair_mirror");
                 ++launches;
             }
-            EQ(align_dispatch(tu.align_block, nw, aa, st), "k_align");
-            ++launches;
+            if (classes) {
+                // pairs by length class, then one alignment launch per class
+                const unsigned g = (unsigned)ctx->sms * 8;
+                uint2* cls = ctx->d_cls.as<uint2>();
+                unsigned int* cursor = reinterpret_cast<unsigned int*>(cls + kAlignClasses);
+                const uint32_t* order_in = tu.pair_order ? ctx->d_pair_order.as<uint32_t>() : nullptr;
+                EQ(cudaMemsetAsync(ctx->d_cls.p, 0, 64, st), "memset");
+                k_pair_class_count<<<g, 256, 0, st>>>(r, first, ctx->d_cand_ids.as<uint32_t>(),
+                                                      ctx->d_cand_anchor.as<uint32_t>(), counters, cap, status,
+                                                      order_in, cls);
+                k_pair_class_offsets<<<1, 32, 0, st>>>(cls, cursor);
+                k_pair_class_scatter<<<g, 256, 0, st>>>(r, first, ctx->d_cand_ids.as<uint32_t>(),
+                                                        ctx->d_cand_anchor.as<uint32_t>(), counters, cap, status,
+                                                        order_in, cursor, ctx->d_pair_class.as<uint32_t>());
+                EQ(cudaGetLastError(), "pair classes");
+                launches += 3;
+                for (int c = 0; c < kAlignClasses; ++c) {
+                    if (align_class_width(c) > std::max(nw, 4) && c > 0 && align_class_width(c - 1) >= nw) break;
+                    AlignArgs ac = aa;
+                    ac.pair_order = ctx->d_pair_class.as<uint32_t>();
+                    ac.cls = cls + c;
+                    EQ(align_dispatch(tu.align_block, align_class_width(c), ac, st), "k_align");
+                    ++launches;
+                }
+            } else {
+                EQ(align_dispatch(tu.align_block, nw, aa, st), "k_align");
+                ++launches;
+            }
             EQ(mark(2), "event");
             if (tu.msa_order) {
                 const unsigned g = (unsigned)std::min<uint64_t>(((uint64_t)count + 255) / 256, (uint64_t)ctx->sms * 8);
@@ -1215,7 +1257,7 @@ int care_b200_set_tuning(care_b200_ctx* ctx, const care_b200_tuning* t) {
     if ((t->msa_warps != 4 && t->msa_warps != 8) || (t->align_block != 128 && t->align_block != 256) ||
         (unsigned)t->msa_order > 1 || (unsigned)t->msa_queue > 1 || (unsigned)t->pair_order > 1 ||
         (unsigned)t->graph > 1 || (unsigned)t->pair_mirror > 1 || t->cand_set_log2 < 6 || t->cand_set_log2 > 14 ||
-        (unsigned)t->align_warp > 1)
+        (unsigned)t->align_warp > 1 || (unsigned)t->align_classes > 1)
         return fail(ctx, CARE_B200_EINVAL, "invalid tuning");
     ctx->tune = *t;
     return CARE_B200_OK;

@@ -374,37 +374,29 @@ __device__ __forceinline__ uint8_t mate_flag(const uint32_t* __restrict__ cand_i
 
 // CNT: the statistics form, which also adds the 32-bit word compares its
 // scans actually run (after the early exits) to run_count.
-template <int BLOCK, int NW, bool CNT = false>
-__global__ void __launch_bounds__(BLOCK)
-k_align(DevOptions o, DevReads r, uint32_t first, const uint32_t* __restrict__ cand_ids,
-        const uint32_t* __restrict__ cand_anchor, const uint32_t* __restrict__ seg_off,
-        const uint32_t* __restrict__ seg_cnt, const unsigned long long* __restrict__ total_ptr,
-        unsigned long long arena_cap, const int* __restrict__ status, AlignRes* __restrict__ out,
-        unsigned long long* __restrict__ work_count, const uint32_t* __restrict__ pair_order,
-        const uint2* __restrict__ work, const unsigned int* __restrict__ work_n,
-        unsigned long long* __restrict__ run_count) {
+// One alignment work item (slot of the mirror work list, of pair_order from
+// `base`, or the pair itself): both orientations, the orientation choice and
+// the AlignRes (a mirrored pair writes both). false past the work list.
+template <int NW, bool CNT>
+__device__ __forceinline__ bool
+align_item(const DevOptions& o, const DevReads& r, uint32_t first, const uint32_t* __restrict__ cand_ids,
+           const uint32_t* __restrict__ cand_anchor, const uint32_t* __restrict__ seg_off,
+           const uint32_t* __restrict__ seg_cnt, unsigned long long total, AlignRes* __restrict__ out,
+           unsigned long long* __restrict__ work_count, const uint32_t* __restrict__ pair_order,
+           unsigned long long base, const uint2* __restrict__ work, const unsigned int* __restrict__ work_n,
+           unsigned long long* __restrict__ run_count, const int* s_mex, unsigned long long slot) {
     using Cnt = typename std::conditional<CNT, WordCount, NoCount>::type;
     Cnt wc;
-    __shared__ int s_mex[kMaxLen + 1];
-    // int(float(ov) * maxErrorRate), the first term of max_errors_excl
-    for (int i = threadIdx.x; i <= kMaxLen; i += BLOCK) s_mex[i] = __float2int_rz(__fmul_rn((float)i, o.max_error_rate));
-    __syncthreads();
-    // an overflowed candidate arena holds unwritten entries: the batch is
-    // repeated with a larger arena, nothing here may read them
-    if (*status & kStatusCandOverflow) return;
-    const unsigned long long slot = (unsigned long long)blockIdx.x * BLOCK + threadIdx.x;
-    const unsigned long long total = *total_ptr;
-    if (total > arena_cap || slot >= total) return;
     unsigned long long i;
     uint32_t j = kNoMirror;
     if (work) {                        // mirror work list (k_pair_mirror)
         const unsigned nl = work_n[0], ns = work_n[1];
-        if (slot >= (unsigned long long)nl + ns) return;
+        if (slot >= (unsigned long long)nl + ns) return false;
         const uint2 w = slot < nl ? work[slot] : work[total - 1 - (slot - nl)];
         i = w.x;
         j = w.y;
     } else {
-        i = pair_order ? pair_order[slot] : slot;
+        i = pair_order ? pair_order[base + slot] : slot;
     }
     const uint32_t ai = cand_anchor[i];
     const uint32_t a = first + ai;
@@ -445,6 +437,59 @@ k_align(DevOptions o, DevReads r, uint32_t first, const uint32_t* __restrict__ c
     };
     out[i] = result(f, ai, c);
     if (j != kNoMirror) out[j] = result(g, c - first, a);
+    return true;
+}
+
+template <int BLOCK>
+__device__ __forceinline__ void align_mex_table(const DevOptions& o, int* s_mex) {
+    // int(float(ov) * maxErrorRate), the first term of max_errors_excl
+    for (int i = threadIdx.x; i <= kMaxLen; i += BLOCK) s_mex[i] = __float2int_rz(__fmul_rn((float)i, o.max_error_rate));
+    __syncthreads();
+}
+
+template <int BLOCK, int NW, bool CNT = false>
+__global__ void __launch_bounds__(BLOCK)
+k_align(DevOptions o, DevReads r, uint32_t first, const uint32_t* __restrict__ cand_ids,
+        const uint32_t* __restrict__ cand_anchor, const uint32_t* __restrict__ seg_off,
+        const uint32_t* __restrict__ seg_cnt, const unsigned long long* __restrict__ total_ptr,
+        unsigned long long arena_cap, const int* __restrict__ status, AlignRes* __restrict__ out,
+        unsigned long long* __restrict__ work_count, const uint32_t* __restrict__ pair_order,
+        const uint2* __restrict__ work, const unsigned int* __restrict__ work_n,
+        unsigned long long* __restrict__ run_count) {
+    __shared__ int s_mex[kMaxLen + 1];
+    align_mex_table<BLOCK>(o, s_mex);
+    // an overflowed candidate arena holds unwritten entries: the batch is
+    // repeated with a larger arena, nothing here may read them
+    if (*status & kStatusCandOverflow) return;
+    const unsigned long long slot = (unsigned long long)blockIdx.x * BLOCK + threadIdx.x;
+    const unsigned long long total = *total_ptr;
+    if (total > arena_cap || slot >= total) return;
+    align_item<NW, CNT>(o, r, first, cand_ids, cand_anchor, seg_off, seg_cnt, total, out, work_count, pair_order, 0,
+                        work, work_n, run_count, s_mex, slot);
+}
+
+// One length class of the batch's pairs (cls = {offset in the class list,
+// pairs}, k_pair_class_*): resident blocks stride over its pairs, with the
+// register budget of the class's plane width.
+template <int BLOCK, int NW, bool CNT = false>
+__global__ void __launch_bounds__(BLOCK, (NW <= 5 ? 1024 : 768) / BLOCK)
+k_align_class(DevOptions o, DevReads r, uint32_t first, const uint32_t* __restrict__ cand_ids,
+              const uint32_t* __restrict__ cand_anchor, const uint32_t* __restrict__ seg_off,
+              const uint32_t* __restrict__ seg_cnt, const unsigned long long* __restrict__ total_ptr,
+              unsigned long long arena_cap, const int* __restrict__ status, AlignRes* __restrict__ out,
+              unsigned long long* __restrict__ work_count, const uint32_t* __restrict__ class_list,
+              const uint2* __restrict__ cls, unsigned long long* __restrict__ run_count) {
+    __shared__ int s_mex[kMaxLen + 1];
+    align_mex_table<BLOCK>(o, s_mex);
+    if (*status & kStatusCandOverflow) return;
+    const unsigned long long total = *total_ptr;
+    if (total > arena_cap) return;
+    const unsigned long long n = cls->y, base = cls->x;
+#pragma unroll 1
+    for (unsigned long long slot = (unsigned long long)blockIdx.x * BLOCK + threadIdx.x; slot < n;
+         slot += (unsigned long long)gridDim.x * BLOCK)
+        align_item<NW, CNT>(o, r, first, cand_ids, cand_anchor, seg_off, seg_cnt, total, out, work_count, class_list,
+                            base, nullptr, nullptr, run_count, s_mex, slot);
 }
 
 // ---------------------------------------------------------------------------
@@ -875,15 +920,30 @@ msa_anchor(const DevOptions& o, const DevReads& r, uint32_t first, uint32_t ai, 
 
     // ---- alignment filters (corrector.hpp:982-1211), ordered compaction ----
     const float base = fmul_rn(o.estimated_errorrate, 1.0f);
+    const float base2 = fmul_rn(2.0f, base), base3 = fmul_rn(3.0f, base), base4 = fmul_rn(4.0f, base);
     int c0 = 0, c1 = 0, c2 = 0, n1 = 0;
+    // the first candidate of each thread: its alignment, mismatch ratio, id
+    // and length stay in registers for the compaction below (the id and
+    // length loads overlap the counting)
+    AlignRes ar0{};
+    float mr0 = 0.0f;
+    uint32_t id0 = 0;
+    int len0 = 0;
     for (uint32_t i = tid; i < cnt; i += BLOCK) {
         const AlignRes ar = ares[off + i];
+        float mr = 0.0f;
         if (ar.orient != 3) {
             n1++;
-            const float mr = fdiv_rn((float)ar.nops, (float)ar.overlap);
-            c0 += mr < fmul_rn(2.0f, base);
-            c1 += mr < fmul_rn(3.0f, base);
-            c2 += mr < fmul_rn(4.0f, base);
+            mr = fdiv_rn((float)ar.nops, (float)ar.overlap);
+            c0 += mr < base2;
+            c1 += mr < base3;
+            c2 += mr < base4;
+        }
+        if (i == (uint32_t)tid) {
+            ar0 = ar;
+            mr0 = mr;
+            id0 = cand_ids[off + i];
+            len0 = r.len[id0];
         }
     }
     int red[4];
@@ -896,9 +956,9 @@ msa_anchor(const DevOptions& o, const DevReads& r, uint32_t first, uint32_t ai, 
     {
         const float good = fmul_rn(o.estimated_coverage, o.m_coverage);
         if (red[0] > 0 || red[1] > 0 || red[2] > 0) {
-            if ((float)red[0] >= good) thr = fmul_rn(2.0f, base);
-            else if ((float)red[1] >= good) thr = fmul_rn(3.0f, base);
-            else if ((float)red[2] >= good) thr = fmul_rn(4.0f, base);
+            if ((float)red[0] >= good) thr = base2;
+            else if ((float)red[1] >= good) thr = base3;
+            else if ((float)red[2] >= good) thr = base4;
         }
     }
     // every candidate fits the staged rows: the survivors' records go straight
@@ -908,21 +968,23 @@ msa_anchor(const DevOptions& o, const DevReads& r, uint32_t first, uint32_t ai, 
     for (uint32_t c = 0; c < cnt; c += BLOCK) {
         const uint32_t i = c + tid;
         int keep = 0;
-        AlignRes ar;
+        AlignRes ar = ar0;
+        float mr = mr0;
         if (i < cnt) {
-            ar = ares[off + i];
-            if (ar.orient != 3) {
-                const float mr = fdiv_rn((float)ar.nops, (float)ar.overlap);
-                keep = o.paired_end ? (ar.paired || mr < o.paired_filter_threshold) : (mr < thr);
+            if (c) {
+                ar = ares[off + i];
+                if (ar.orient != 3) mr = fdiv_rn((float)ar.nops, (float)ar.overlap);
             }
+            if (ar.orient != 3)
+                keep = o.paired_end ? (ar.paired || mr < o.paired_filter_threshold) : (mr < thr);
         }
         int tot;
         const int pre = block_scan(keep, &tot);
         if (keep) {
             CandRec rec;
-            rec.id = cand_ids[off + i];
+            rec.id = c ? cand_ids[off + i] : id0;
             rec.shift = ar.shift;
-            rec.len = (uint16_t)r.len[rec.id];
+            rec.len = (uint16_t)(c ? r.len[rec.id] : len0);
             // calculateOverlapWeight: 1 - sqrtf(nOps / (overlap * maxMismatchRatio))
             rec.weight = fsub_rn(1.0f, __fsqrt_rn(fdiv_rn((float)ar.nops, fmul_rn((float)ar.overlap, o.max_error_rate))));
             rec.orient = ar.orient;
@@ -1224,18 +1286,18 @@ msa_anchor(const DevOptions& o, const DevReads& r, uint32_t first, uint32_t ai, 
                     __syncwarp();
                 }
             };
-            if (persistent) {
-                if (active) run_rows(s_alive, nalive);
-            } else {
-                // more rows than fit: each chunk is staged (by all warps) per block
-                for (int c = 0; c < nalive; c += nstage) {
-                    const int n = min(nstage, nalive - c);
-                    stage(c, n, true);
-                    if (active) run_rows(nullptr, n);
-                    flush();
+            // persistent rows are one chunk; with more rows than fit, each
+            // chunk is staged (by all warps) per block
+            const int nchunk = persistent ? 1 : (nalive + nstage - 1) / nstage;
+            for (int ch = 0; ch < nchunk; ++ch) {
+                int n = nalive;
+                if (!persistent) {
+                    n = min(nstage, nalive - ch * nstage);
+                    stage(ch * nstage, n, true);
                 }
+                if (active) run_rows(persistent ? s_alive : nullptr, n);
+                flush();
             }
-            flush();
             if (active && col < ncols) {
                 uint8_t cs = 0; float cw = wA;
                 if (wC > cw) { cs = 1; cw = wC; }
@@ -1666,6 +1728,74 @@ static __global__ void k_pair_order(const DevReads r, const uint32_t* __restrict
     __syncthreads();
     for (uint32_t k = threadIdx.x; k < cnt; k += blockDim.x)
         pair_order[off + atomicAdd(&s_bin[r.len[cand_ids[off + k]] >> 4], 1u)] = off + k;
+}
+
+// Length classes of the alignment pairs: the plane width (32-base words) the
+// longer read of a pair needs, 4 / 5 / 6 / 8, so that each class runs the
+// k_align instance of its width (fewer registers for short pairs, lanes of
+// similar lengths). cls[c] = {offset in the class list, pairs}; within a
+// class, warps keep the pair order they read (warp-aggregated cursors).
+constexpr int kAlignClasses = 4;
+__host__ __device__ inline int align_class_width(int c) { return c == 0 ? 4 : c == 1 ? 5 : c == 2 ? 6 : 8; }
+__device__ __forceinline__ int align_class_of(int L) {
+    const int nw = (L + 31) >> 5;
+    return nw <= 4 ? 0 : nw == 5 ? 1 : nw == 6 ? 2 : 3;
+}
+__device__ __forceinline__ int pair_class(const DevReads& r, uint32_t first, const uint32_t* cand_ids,
+                                          const uint32_t* cand_anchor, unsigned long long i) {
+    return align_class_of(max(r.len[first + cand_anchor[i]], r.len[cand_ids[i]]));
+}
+static __global__ void k_pair_class_count(DevReads r, uint32_t first, const uint32_t* __restrict__ cand_ids,
+                                          const uint32_t* __restrict__ cand_anchor,
+                                          const unsigned long long* __restrict__ total_ptr, unsigned long long cap,
+                                          const int* __restrict__ status, const uint32_t* __restrict__ pair_order,
+                                          uint2* __restrict__ cls) {
+    if (*status & kStatusCandOverflow) return;
+    const unsigned long long total = *total_ptr;
+    if (total > cap) return;
+    const int lane = threadIdx.x & 31;
+    const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+    for (unsigned long long s0 = (unsigned long long)blockIdx.x * blockDim.x; s0 < total; s0 += stride) {
+        const unsigned long long slot = s0 + threadIdx.x;
+        const bool act = slot < total;
+        const int c = act ? pair_class(r, first, cand_ids, cand_anchor, pair_order ? pair_order[slot] : slot) : -1;
+#pragma unroll
+        for (int k = 0; k < kAlignClasses; ++k) {
+            const unsigned m = __ballot_sync(0xffffffffu, c == k);
+            if (m && lane == 0) atomicAdd(&cls[k].y, (unsigned)__popc(m));
+        }
+    }
+}
+static __global__ void k_pair_class_offsets(uint2* __restrict__ cls, unsigned int* __restrict__ cursor) {
+    if (threadIdx.x != 0) return;
+    unsigned run = 0;
+    for (int k = 0; k < kAlignClasses; ++k) { cls[k].x = run; cursor[k] = run; run += cls[k].y; }
+}
+static __global__ void k_pair_class_scatter(DevReads r, uint32_t first, const uint32_t* __restrict__ cand_ids,
+                                            const uint32_t* __restrict__ cand_anchor,
+                                            const unsigned long long* __restrict__ total_ptr, unsigned long long cap,
+                                            const int* __restrict__ status, const uint32_t* __restrict__ pair_order,
+                                            unsigned int* __restrict__ cursor, uint32_t* __restrict__ list) {
+    if (*status & kStatusCandOverflow) return;
+    const unsigned long long total = *total_ptr;
+    if (total > cap) return;
+    const int lane = threadIdx.x & 31;
+    const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+    for (unsigned long long s0 = (unsigned long long)blockIdx.x * blockDim.x; s0 < total; s0 += stride) {
+        const unsigned long long slot = s0 + threadIdx.x;
+        const bool act = slot < total;
+        const uint32_t i = act ? (pair_order ? pair_order[slot] : (uint32_t)slot) : 0u;
+        const int c = act ? pair_class(r, first, cand_ids, cand_anchor, i) : -1;
+#pragma unroll
+        for (int k = 0; k < kAlignClasses; ++k) {
+            const unsigned m = __ballot_sync(0xffffffffu, c == k);
+            if (!m) continue;
+            unsigned b = 0;
+            if (lane == 0) b = atomicAdd(&cursor[k], (unsigned)__popc(m));
+            b = __shfl_sync(0xffffffffu, b, 0);
+            if (c == k) list[b + __popc(m & ((1u << lane) - 1u))] = i;
+        }
+    }
 }
 
 // The network's verdict on each decision column of the batch: the consensus

@@ -396,6 +396,9 @@ typedef struct care_b200_tuning {
     int align_warp;    /* 1: a warp per alignment work item, its lanes taking the shifts of
                           each group of 32 (the scan's first minimal shift found by warp
                           reductions); 0: a thread per work item */
+    int align_classes; /* 1: the batch's pairs partitioned by the plane width their longer read
+                          needs (4/5/6/8 words of 32 bases), one alignment launch per class
+                          (no effect with pair_mirror) */
 } care_b200_tuning;
 
 int care_b200_default_tuning(care_b200_tuning* t);

@@ -30,6 +30,8 @@ VARIANTS = [
     {"align_warp": 1},
     {"align_warp": 1, "pair_mirror": 1, "align_block": 256},
     {"align_warp": 1, "pair_mirror": 1, "pair_order": 1},
+    {"align_classes": 1},
+    {"align_classes": 1, "pair_order": 1, "align_block": 256},
     {"msa_order": 1, "msa_queue": 1, "msa_warps": 8, "align_block": 256, "pair_order": 1, "graph": 1,
      "pair_mirror": 1},
 ]
