@@ -53,12 +53,24 @@ def record_multiset(blob: bytes):
 
 
 def gather_records(blob: bytes, group=None) -> bytes:
-    """All ranks' record streams, merged in rank order (on every rank)."""
+    """All ranks' record streams, merged in rank order (on every rank): the
+    sizes first, then one all-gather of byte tensors padded to the largest
+    stream (CUDA tensors over NCCL, host tensors over gloo; no pickling)."""
+    import torch
     import torch.distributed as dist
     world = dist.get_world_size(group)
-    parts = [None] * world
-    dist.all_gather_object(parts, blob, group=group)
-    return merge_records(parts)
+    dev = torch.device("cuda", torch.cuda.current_device()) if dist.get_backend(group) == "nccl" else torch.device("cpu")
+    size = torch.tensor([len(blob)], dtype=torch.int64, device=dev)
+    sizes = [torch.zeros(1, dtype=torch.int64, device=dev) for _ in range(world)]
+    dist.all_gather(sizes, size, group=group)
+    sizes = [int(x.item()) for x in sizes]
+    cap = max(max(sizes), 1)
+    mine = torch.zeros(cap, dtype=torch.uint8, device=dev)
+    if blob:
+        mine[:len(blob)] = torch.frombuffer(bytearray(blob), dtype=torch.uint8).to(dev)
+    parts = [torch.empty(cap, dtype=torch.uint8, device=dev) for _ in range(world)]
+    dist.all_gather(parts, mine, group=group)
+    return merge_records(p[:n].cpu().numpy().tobytes() for p, n in zip(parts, sizes))
 
 
 def correct_sharded(corrector, rank: int, world: int, group=None) -> bytes:

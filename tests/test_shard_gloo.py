@@ -82,3 +82,27 @@ def test_two_ranks_equal_one_run(golden, tmp_path, case):
     assert len(merged) == len(ref)
     assert shard.record_multiset(merged) == shard.record_multiset(ref)
     assert any(t == 1 for _, _, _, t, _ in shard.iter_records(ref))      # candidate corrections included
+
+
+def _gather_worker(rank, world, port, out):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120))
+    try:
+        blob = bytes(range(256)) * (rank * 3) + bytes([rank]) * (rank % 2)   # rank 0 contributes nothing
+        merged = shard.gather_records(blob)
+        with open(out % rank, "wb") as f:
+            f.write(merged)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_gather_streams_of_unequal_and_empty_sizes(tmp_path):
+    """The byte-tensor gather returns the streams in rank order on every
+    rank, whatever their sizes (an empty one included)."""
+    world = 3
+    out = str(tmp_path / "g%d.bin")
+    mp.start_processes(_gather_worker, args=(world, _free_port(), out), nprocs=world, start_method="spawn")
+    exp = b"".join(bytes(range(256)) * (r * 3) + bytes([r]) * (r % 2) for r in range(world))
+    for r in range(world):
+        assert open(out % r, "rb").read() == exp
