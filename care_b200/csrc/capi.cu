@@ -11,6 +11,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <functional>
 #include <memory>
 #include <mutex>
 #include <numeric>
@@ -79,8 +80,10 @@ struct care_b200_ctx {
     std::string err;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
-    cudaEvent_t sig_ev[2] = {nullptr, nullptr};    // around the last signature pass
-    bool sig_timed = false;
+    // around each launch of the last signature pass (pairs; the pass may be
+    // split into chunks interleaved with the upload of the reads)
+    std::vector<cudaEvent_t> sig_ev;
+    int sig_used = 0;
     float last_ms = 0.f, stage_ms[4] = {0.f, 0.f, 0.f, 0.f};
 
     // read storage
@@ -117,6 +120,7 @@ struct care_b200_ctx {
     HBuf h_stage[2][2];
     cudaEvent_t stage_ev[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
     cudaStream_t copy_stream = nullptr;
+    cudaStream_t copy_stream2 = nullptr;          // quality words while the sequences upload
 
     // learned decision: parameters, decision-column rows of a batch
     DBuf d_mlp, d_mlp_err;
@@ -219,23 +223,37 @@ uint64_t host_murmur64(uint64_t x) {
     return x;
 }
 
-// minhash signatures of every read for `maps` hash functions into d_sigs
-int compute_signatures(care_b200_ctx* ctx, int maps) {
+// minhash signatures of reads [b, e) for `maps` hash functions into d_sigs
+// (allocated for every read by the caller), each launch timed by an event pair
+int signatures_range(care_b200_ctx* ctx, int maps, uint32_t b, uint32_t e) {
     DevOptions o = make_dev_options(ctx);
     o.num_maps = maps;
     const DevReads r = make_dev_reads(ctx);
-    CK(ctx->d_sigs.ensure((size_t)ctx->n * maps * 8), "alloc signatures");
     const uint32_t chunk = 1u << 20;
-    CK(cudaEventRecord(ctx->sig_ev[0], ctx->stream), "event");
-    for (uint32_t b = 0; b < ctx->n; b += chunk) {
-        const uint32_t cnt = std::min(chunk, ctx->n - b);
+    for (; b < e; b += chunk) {
+        const uint32_t cnt = std::min(chunk, e - b);
+        if ((size_t)ctx->sig_used + 2 > ctx->sig_ev.size()) {
+            cudaEvent_t a2[2];
+            for (auto& x : a2) CK(cudaEventCreate(&x), "cudaEventCreate");
+            ctx->sig_ev.push_back(a2[0]);
+            ctx->sig_ev.push_back(a2[1]);
+        }
         const int wpb = 8;
+        CK(cudaEventRecord(ctx->sig_ev[ctx->sig_used], ctx->stream), "event");
         k_signatures<<<(cnt + wpb - 1) / wpb, 32 * wpb, 0, ctx->stream>>>(
             o, r, b, cnt, ctx->d_sigs.as<unsigned long long>() + (size_t)b * maps);
         CK(cudaGetLastError(), "k_signatures");
+        CK(cudaEventRecord(ctx->sig_ev[ctx->sig_used + 1], ctx->stream), "event");
+        ctx->sig_used += 2;
     }
-    CK(cudaEventRecord(ctx->sig_ev[1], ctx->stream), "event");
-    ctx->sig_timed = true;
+    return CARE_B200_OK;
+}
+
+// minhash signatures of every read for `maps` hash functions into d_sigs
+int compute_signatures(care_b200_ctx* ctx, int maps) {
+    CK(ctx->d_sigs.ensure((size_t)ctx->n * maps * 8), "alloc signatures");
+    ctx->sig_used = 0;
+    if (int rc = signatures_range(ctx, maps, 0, ctx->n)) return rc;
     ctx->sigs_maps = maps;
     return CARE_B200_OK;
 }
@@ -243,11 +261,15 @@ int compute_signatures(care_b200_ctx* ctx, int maps) {
 // Host -> device copy of pageable caller memory through two pinned chunks of
 // staging slot `slot`: host threads fill one chunk while the copy engine
 // drains the other. Asynchronous on `st` (the caller synchronises).
-int staged_upload(care_b200_ctx* ctx, int slot, void* dst, const void* src, size_t bytes, cudaStream_t st) {
+// on_chunk(end, done): called after the copy of bytes [.., end) is enqueued
+// on st; the event `done` completes with that copy.
+int staged_upload(care_b200_ctx* ctx, int slot, void* dst, const void* src, size_t bytes, cudaStream_t st,
+                  const std::function<int(size_t, cudaEvent_t)>& on_chunk = nullptr) {
     constexpr size_t kChunk = 16u << 20;
     if (bytes <= kChunk / 4) {               // small: one pinned copy is not worth it
         CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st), "upload");
         CK(cudaStreamSynchronize(st), "upload");
+        if (on_chunk) if (int rc = on_chunk(bytes, nullptr)) return rc;
         return CARE_B200_OK;
     }
     for (auto& b : ctx->h_stage[slot]) CK(b.ensure(kChunk), "alloc staging");
@@ -269,6 +291,7 @@ int staged_upload(care_b200_ctx* ctx, int slot, void* dst, const void* src, size
         for (auto& x : th) x.join();
         CK(cudaMemcpyAsync(static_cast<char*>(dst) + off, pin, len, cudaMemcpyHostToDevice, st), "upload");
         CK(cudaEventRecord(ctx->stage_ev[slot][b], st), "staging");
+        if (on_chunk) if (int rc = on_chunk(off + len, ctx->stage_ev[slot][b])) return rc;
     }
     return CARE_B200_OK;
 }
@@ -337,8 +360,8 @@ static int care_b200_create_impl(const care_b200_options* opt, care_b200_ctx** o
     CK(cudaSetDevice(opt->device), "cudaSetDevice");
     CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking), "cudaStreamCreate");
     for (auto& e : ctx->ev) CK(cudaEventCreate(&e), "cudaEventCreate");
-    for (auto& e : ctx->sig_ev) CK(cudaEventCreate(&e), "cudaEventCreate");
     CK(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    CK(cudaStreamCreateWithFlags(&ctx->copy_stream2, cudaStreamNonBlocking), "cudaStreamCreate");
     for (auto& row : ctx->stage_ev)
         for (auto& e : row) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
     float qw[256];
@@ -355,10 +378,13 @@ int care_b200_destroy(care_b200_ctx* ctx) {
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     for (auto& e : ctx->ev) if (e) cudaEventDestroy(e);
     for (auto& e : ctx->sig_ev) if (e) cudaEventDestroy(e);
+    ctx->sig_ev.clear();
     if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);
+    if (ctx->copy_stream2) cudaStreamSynchronize(ctx->copy_stream2);
     for (auto& row : ctx->stage_ev)
         for (auto& e : row) if (e) cudaEventDestroy(e);
     if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
+    if (ctx->copy_stream2) cudaStreamDestroy(ctx->copy_stream2);
     if (ctx->gexec) cudaGraphExecDestroy(ctx->gexec);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
@@ -403,19 +429,36 @@ static int care_b200_upload_reads_impl(care_b200_ctx* ctx, const uint32_t* packe
     ctx->qual_pitch = ctx->has_qual ? (int)qual_pitch_ints : 0;
     if (ctx->has_qual && (size_t)quality_ints(mx, ctx->opt.quality_bits) > qual_pitch_ints)
         return fail(ctx, CARE_B200_EINVAL, "qual_pitch_ints too small for the longest read");
-    // packed rows and lengths first; the minhash signatures of the new
-    // storage are computed on the main stream while the quality words upload
-    // on the copy stream
-    CK(ctx->d_seq.ensure((size_t)num_reads * pitch_ints * 4), "alloc reads");
-    if (int rc = staged_upload(ctx, 0, ctx->d_seq.p, packed, (size_t)num_reads * pitch_ints * 4, ctx->stream)) return rc;
+    // lengths, then the packed rows on the main stream, each chunk's whole
+    // reads hashed (minhash signatures) as soon as its copy is enqueued; the
+    // quality words upload on the copy stream meanwhile
+    CK(cudaStreamSynchronize(ctx->stream), "upload");      // no earlier work still reads the storage
     CK(ctx->d_len.ensure((size_t)num_reads * 4), "alloc lengths");
     if (int rc = staged_upload(ctx, 0, ctx->d_len.p, lengths, (size_t)num_reads * 4, ctx->stream)) return rc;
+    CK(ctx->d_seq.ensure((size_t)num_reads * pitch_ints * 4), "alloc reads");
+    const int maps = ctx->num_maps ? ctx->num_maps : ctx->opt.num_maps;
     ctx->sigs_maps = 0;
-    if (int rc = compute_signatures(ctx, ctx->num_maps ? ctx->num_maps : ctx->opt.num_maps)) return rc;
+    CK(ctx->d_sigs.ensure((size_t)num_reads * maps * 8), "alloc signatures");
+    ctx->sig_used = 0;
+    uint32_t hashed = 0;
+    const size_t row_bytes = pitch_ints * 4;
+    // copies on the copy stream; the main stream waits for each chunk's copy
+    // and hashes its whole reads while the next chunks copy
+    auto hash_chunk = [&](size_t end, cudaEvent_t done) -> int {
+        if (done) CK(cudaStreamWaitEvent(ctx->stream, done, 0), "wait");
+        const uint32_t whole = (uint32_t)std::min<size_t>(end / row_bytes, num_reads);
+        const int rc = signatures_range(ctx, maps, hashed, whole);
+        hashed = whole;
+        return rc;
+    };
+    if (int rc = staged_upload(ctx, 0, ctx->d_seq.p, packed, (size_t)num_reads * row_bytes, ctx->copy_stream,
+                               hash_chunk))
+        return rc;
+    ctx->sigs_maps = maps;
     if (ctx->has_qual) {
         CK(ctx->d_qual.ensure((size_t)num_reads * qual_pitch_ints * 4), "alloc qualities");
         if (int rc = staged_upload(ctx, 1, ctx->d_qual.p, enc_quals, (size_t)num_reads * qual_pitch_ints * 4,
-                                   ctx->copy_stream)) return rc;
+                                   ctx->copy_stream2)) return rc;
     }
     ctx->h_len.assign(lengths, lengths + num_reads);
     ctx->h_ambig.assign(num_reads, 0);
@@ -426,6 +469,7 @@ static int care_b200_upload_reads_impl(care_b200_ctx* ctx, const uint32_t* packe
     CK(ctx->d_ambig.ensure(num_reads), "alloc ambiguous flags");
     CK(cudaMemcpyAsync(ctx->d_ambig.p, ctx->h_ambig.data(), num_reads, cudaMemcpyHostToDevice, ctx->stream), "upload ambiguous flags");
     CK(cudaStreamSynchronize(ctx->copy_stream), "upload");
+    CK(cudaStreamSynchronize(ctx->copy_stream2), "upload");
     CK(cudaStreamSynchronize(ctx->stream), "upload");
     if (ctx->tables_ready && ctx->t_keys.size() && num_reads != ctx->tables_reads) ctx->tables_ready = false;
     ctx->r_valid = false;
@@ -1704,8 +1748,12 @@ int care_b200_last_timing(const care_b200_ctx* ctx, float* total_ms, float* stag
     for (int i = 0; i < nstages && i < 4 && stage_ms; i++) stage_ms[i] = ctx->stage_ms[i];
     if (stage_ms && nstages > 4) {
         float ms = 0.f;
-        if (ctx->sig_timed && cudaEventSynchronize(ctx->sig_ev[1]) == cudaSuccess)
-            cudaEventElapsedTime(&ms, ctx->sig_ev[0], ctx->sig_ev[1]);
+        for (int k = 0; k + 1 < ctx->sig_used; k += 2) {
+            float part = 0.f;
+            if (cudaEventSynchronize(ctx->sig_ev[k + 1]) == cudaSuccess &&
+                cudaEventElapsedTime(&part, ctx->sig_ev[k], ctx->sig_ev[k + 1]) == cudaSuccess)
+                ms += part;
+        }
         stage_ms[4] = ms;
     }
     return CARE_B200_OK;
