@@ -421,6 +421,9 @@ static int care_b200_upload_reads_impl(care_b200_ctx* ctx, const uint32_t* packe
     for (uint32_t i = 0; i < num_reads; i++) mx = std::max(mx, (int)lengths[i]);
     if (mx > kMaxLen) return fail(ctx, CARE_B200_ELIMIT, "reads longer than 256 bases are not supported");
     if ((size_t)(mx + 15) / 16 > pitch_ints) return fail(ctx, CARE_B200_EINVAL, "pitch_ints too small for the longest read");
+    if (pitch_ints > (size_t)kMaxLen / 16) return fail(ctx, CARE_B200_EINVAL, "pitch_ints above 16 (256 bases)");
+    if (enc_quals && ctx->opt.use_quality && qual_pitch_ints > (size_t)quality_ints(kMaxLen, ctx->opt.quality_bits))
+        return fail(ctx, CARE_B200_EINVAL, "qual_pitch_ints above the words of 256 qualities");
     CK(cudaSetDevice(ctx->opt.device), "cudaSetDevice");
     ctx->n = num_reads;
     ctx->max_len = mx;
@@ -860,9 +863,9 @@ int run_batch(care_b200_ctx* ctx, uint32_t first, uint32_t count, bool timed) {
     // length classes of the alignment (not with mirror pairs, whose work list pairs equal lengths)
     const bool classes = tu.align_classes != 0 && tu.pair_mirror == 0;
     if (classes) CK(ctx->d_cls.ensure(64), "alloc");
-    const size_t msmem = msa_smem_bytes(ctx->max_len, ctx->seq_pitch, ctx->has_qual ? ctx->qual_pitch : 0, emit,
-                                        32 * jb * warps);
     const int qb = ctx->has_qual ? ctx->opt.quality_bits : 0;
+    const size_t msmem = msa_smem_bytes(ctx->max_len, ctx->seq_pitch, ctx->has_qual ? ctx->qual_pitch : 0, qb, emit,
+                                        32 * jb * warps);
 
     for (int attempt = 0; attempt < 8; ++attempt) {
         const unsigned long long cap = ctx->cand_cap;

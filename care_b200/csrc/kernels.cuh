@@ -763,52 +763,110 @@ struct MsaOut {
 constexpr int kNumFeatures = 24;
 
 constexpr int kStageMax = 128;        // candidate rows held in shared memory, at most
-constexpr int kStageBudget = 16384;   // bytes of staged packed rows
+constexpr int kStageBudget = 16384;   // bytes of staged rows
+constexpr int kStageGuard = 32;       // bytes before and after the staged rows
 
-// candidate rows staged at once: packed sequence + encoded quality words
-__host__ __device__ inline int msa_stage_rows(int seq_pitch, int qual_pitch) {
-    const int rows = kStageBudget / ((seq_pitch + qual_pitch) * 4);
+// words of a staged row (qb: the quality encoding the sums read). The bases
+// are realigned to the anchor's 16-base grid, so they take one word more than
+// the read's pitch; 1- and 8-bit quality codes follow on their own grids (32
+// and 4 codes per word), 2-bit codes are interleaved with the bases as word
+// pairs {bases, qualities} of the same 16 positions.
+__host__ __device__ inline int msa_slot_words(int seq_pitch, int qual_pitch, int qb) {
+    if (qb == 0) return seq_pitch + 1;
+    if (qb == 2) return 2 * ((seq_pitch > qual_pitch ? seq_pitch : qual_pitch) + 1);
+    return seq_pitch + 1 + qual_pitch + 1;
+}
+
+// candidate rows staged at once
+__host__ __device__ inline int msa_stage_rows(int seq_pitch, int qual_pitch, int qb) {
+    const int rows = kStageBudget / (msa_slot_words(seq_pitch, qual_pitch, qb) * 4);
     return rows > kStageMax ? kStageMax : (rows < 16 ? 16 : rows);
 }
 
 // dynamic shared memory of k_msa: the anchor's decoded row, the staged
-// packed candidate rows; with decision rows also three per-anchor-column
-// weights; then the per-column arrays of `maxcols` columns (four 16-bit
-// counts, support, coverage, consensus). Every part starts on a 16-byte
-// boundary (maxcols is a multiple of 128).
+// candidate rows (between two guard bands: a lane whose column lies outside
+// a row may read a few words past either end of it, and adds nothing); with
+// decision rows also three per-anchor-column weights; then the per-column
+// arrays of `maxcols` columns (four 16-bit counts, support, coverage,
+// consensus). Every part starts on a 16-byte boundary (maxcols is a multiple
+// of 128).
 __host__ __device__ inline size_t msa_round16(size_t x) { return (x + 15) & ~(size_t)15; }
-__host__ __device__ inline size_t msa_smem_bytes(int max_len, int seq_pitch, int qual_pitch, bool emit, int maxcols) {
+__host__ __device__ inline size_t msa_raw_bytes(int seq_pitch, int qual_pitch, int qb) {
+    return msa_round16(2 * kStageGuard + (size_t)msa_stage_rows(seq_pitch, qual_pitch, qb) *
+                                             msa_slot_words(seq_pitch, qual_pitch, qb) * 4);
+}
+__host__ __device__ inline size_t msa_smem_bytes(int max_len, int seq_pitch, int qual_pitch, int qb, bool emit,
+                                                 int maxcols) {
     const size_t elem = msa_round16((size_t)max_len * 2);
-    const size_t raw = msa_round16((size_t)msa_stage_rows(seq_pitch, qual_pitch) * (seq_pitch + qual_pitch) * 4);
     const size_t fw = emit ? msa_round16((size_t)3 * max_len * 4) : 0;
-    return elem + raw + fw + (size_t)maxcols * (8 + 4 + 2 + 1);
+    return elem + msa_raw_bytes(seq_pitch, qual_pitch, qb) + fw + (size_t)maxcols * (8 + 4 + 2 + 1);
 }
 
-// One element of a column: weight w added to the sum of its base b (0..3)
-// and one to the base's 8-bit count in c8 (A | C << 8 | G << 16 | T << 24),
-// nothing when the column lies outside the row (in false). IEEE adds
-// (add.rn.f32, no contraction), predicated on (base, in): the sums see the
-// same additions in the same order as an add per element of the base.
-__device__ __forceinline__ void msa_add(float& wA, float& wC, float& wG, float& wT, uint32_t& c8,
-                                        uint32_t b, float w, bool in) {
+// Realigned and reversed rows: a window of one word of codes whose first
+// code is code s0 of a source row (codes before the row and past its end
+// read as zero), the source row's words held one per lane in m (zero from
+// the row's pitch on; lane 31 zero for the 2- and 1-bit forms, whose pitches
+// are at most 16 and 8 words). Branch free: the row is read as if preceded
+// by one zero word, and a funnel shift with a zero count returns its high
+// word.
+// 2-bit codes, 16 per word, MSB first
+__device__ __forceinline__ uint32_t window2(uint32_t m, int s0) {
+    const int sc = max(s0 + 16, 0);
+    const int wi = sc >> 4;
+    const uint32_t a = __shfl_sync(0xffffffffu, m, (wi + 31) & 31);    // source word wi - 1
+    const uint32_t b = __shfl_sync(0xffffffffu, m, wi & 31);
+    return __funnelshift_l(b, a, 2 * (sc & 15));
+}
+// 1-bit codes, 32 per word, MSB first
+__device__ __forceinline__ uint32_t window1(uint32_t m, int s0) {
+    const int sc = max(s0 + 32, 0);
+    const int wi = sc >> 5;
+    const uint32_t a = __shfl_sync(0xffffffffu, m, (wi + 31) & 31);
+    const uint32_t b = __shfl_sync(0xffffffffu, m, wi & 31);
+    return __funnelshift_l(b, a, sc & 31);
+}
+// 8-bit codes, 4 per word, little-endian; source words 0..31 in m0, 32..63 in m1
+__device__ __forceinline__ uint32_t window8(uint32_t m0, uint32_t m1, int s0) {
+    const int sc = max(s0 + 4, 0);
+    const int wi = sc >> 2;
+    const int ia = wi - 1, ib = wi;
+    const uint32_t a0 = __shfl_sync(0xffffffffu, m0, ia & 31), a1 = __shfl_sync(0xffffffffu, m1, ia & 31);
+    const uint32_t b0 = __shfl_sync(0xffffffffu, m0, ib & 31), b1 = __shfl_sync(0xffffffffu, m1, ib & 31);
+    const uint32_t a = ia < 0 ? 0u : ia < 32 ? a0 : a1;
+    const uint32_t b = ib < 32 ? b0 : b1;
+    return __funnelshift_r(a, b, 8 * (sc & 3));
+}
+// reverse the 16 2-bit codes of a word, keeping each code's bits
+__device__ __forceinline__ uint32_t rev2(uint32_t w) {
+    w = __brev(w);
+    return ((w >> 1) & 0x55555555u) | ((w & 0x55555555u) << 1);
+}
+
+// One element of a column: weight w added to the sum of its base (b8 = base
+// * 8) and one to the base's 8-bit count in c8 (A | C << 8 | G << 16 |
+// T << 24), nothing when the column lies outside the row (p, the column's
+// position in the row, not below len). IEEE adds (add.rn.f32, no
+// contraction), predicated on (base, in row): the sums see the same
+// additions in the same order as an add per element of the base.
+__device__ __forceinline__ void msa_add8(float& wA, float& wC, float& wG, float& wT, uint32_t& c8,
+                                         uint32_t b8, float w, int p, int len) {
     asm("{\n\t"
         ".reg .pred pin, pa, pc, pg, pt;\n\t"
-        ".reg .b32 sh, inc;\n\t"
-        "setp.ne.b32 pin, %7, 0;\n\t"
+        ".reg .b32 inc;\n\t"
+        "setp.lt.u32 pin, %7, %8;\n\t"
         "setp.eq.and.b32 pa, %6, 0, pin;\n\t"
-        "setp.eq.and.b32 pc, %6, 1, pin;\n\t"
-        "setp.eq.and.b32 pg, %6, 2, pin;\n\t"
-        "setp.eq.and.b32 pt, %6, 3, pin;\n\t"
+        "setp.eq.and.b32 pc, %6, 8, pin;\n\t"
+        "setp.eq.and.b32 pg, %6, 16, pin;\n\t"
+        "setp.eq.and.b32 pt, %6, 24, pin;\n\t"
         "@pa add.rn.f32 %0, %0, %5;\n\t"
         "@pc add.rn.f32 %1, %1, %5;\n\t"
         "@pg add.rn.f32 %2, %2, %5;\n\t"
         "@pt add.rn.f32 %3, %3, %5;\n\t"
-        "shl.b32 sh, %6, 3;\n\t"
-        "shl.b32 inc, %8, sh;\n\t"
+        "shl.b32 inc, %9, %6;\n\t"
         "@pin add.u32 %4, %4, inc;\n\t"
         "}"
         : "+f"(wA), "+f"(wC), "+f"(wG), "+f"(wT), "+r"(c8)
-        : "f"(w), "r"(b), "r"((uint32_t)in), "r"(1u));
+        : "f"(w), "r"(b8), "r"(p), "r"(len), "r"(1u));
 }
 
 // The whole MSA stage of one anchor (local index ai) for one CTA. Every
@@ -826,7 +884,11 @@ msa_anchor(const DevOptions& o, const DevReads& r, uint32_t first, uint32_t ai, 
     const int MAXCOLS = 32 * jb * NWARP;
     extern __shared__ __align__(16) unsigned char dsm[];
     __shared__ float s_qw[256];
-    __shared__ uint2 s_hits[NWARP][36];      // per warp: the staged rows meeting its column block
+    // per warp: the staged rows meeting its column block, {row grid offset,
+    // first position - lane, length, weights}, and for 1- and 8-bit qualities
+    // the row's quality grid offset
+    __shared__ uint4 s_hits[NWARP][36];
+    __shared__ int s_hq[(QB == 1 || QB == 8) ? NWARP : 1][36];
     __shared__ int s_blk;                    // next column block (persistent rows: warps take blocks in turn)
     __shared__ float s_qwc[4];               // weight of a 1- or 2-bit quality code
     __shared__ int s_beg[kStageMax], s_len[kStageMax];
@@ -847,14 +909,15 @@ msa_anchor(const DevOptions& o, const DevReads& r, uint32_t first, uint32_t ai, 
     const int mlen = r.max_len;
     constexpr bool useQ = QB != 0;
     char* aout = out.seq + (size_t)ai * mlen;
-    const int nstage = msa_stage_rows(r.seq_pitch, r.qual_pitch);
-    const int rw = r.seq_pitch + r.qual_pitch;               // words per staged row
+    const int nstage = msa_stage_rows(r.seq_pitch, r.qual_pitch, QB);
+    const int rw = msa_slot_words(r.seq_pitch, r.qual_pitch, QB);   // words per staged row
     // dynamic shared memory, each part 16-byte aligned (msa_smem_bytes)
     uint16_t* s_aelem = (uint16_t*)dsm;                      // anchor row: base | quality char << 2
-    uint32_t* s_raw = (uint32_t*)(dsm + msa_round16((size_t)mlen * 2));   // [nstage][rw]
+    unsigned char* s_rawg = dsm + msa_round16((size_t)mlen * 2);
+    uint32_t* s_raw = (uint32_t*)(s_rawg + kStageGuard);     // [nstage][rw]
     // per anchor column: column weight sum, consensus weight, weight of the
     // anchor's base (EMIT only)
-    float* s_fw = (float*)((unsigned char*)s_raw + msa_round16((size_t)nstage * rw * 4));
+    float* s_fw = (float*)(s_rawg + msa_raw_bytes(r.seq_pitch, r.qual_pitch, QB));
     // per MSA column: counts of A C G T, support, coverage, consensus
     ushort4* s_cnt4 = (ushort4*)((unsigned char*)s_fw + (EMIT ? msa_round16((size_t)3 * mlen * 4) : 0));
     float* s_support = (float*)(s_cnt4 + MAXCOLS);
@@ -869,10 +932,6 @@ msa_anchor(const DevOptions& o, const DevReads& r, uint32_t first, uint32_t ai, 
         if (tid == 0) { out.status[ai] = 0; out.nedits[ai] = 0; }
         return;
     }
-
-    // the padding entries of the hit lists stay zero: a group of four rows
-    // reads them, with its element adds switched off, past a list's end
-    for (int i = tid; i < NWARP * 36; i += BLOCK) (&s_hits[0][0])[i] = make_uint2(0u, 0u);
 
     auto block_sum4 = [&](int v0, int v1, int v2, int v3, int* res) {
 #pragma unroll
@@ -1031,13 +1090,20 @@ msa_anchor(const DevOptions& o, const DevReads& r, uint32_t first, uint32_t ai, 
         }
     }
 
-    // stage candidate rows [c, c+n) of recs into slots 0..n-1: their packed
-    // sequence and quality words, eight rows in flight per lane; reverse-
-    // complement rows are then turned into the alignment's orientation in
-    // place (bases reversed and complemented, qualities reversed over the
-    // whole quality pitch: reverseQualitiesOfRCAlignments, corrector.hpp:
-    // 1227-1239), so the column sums read every row forward
-    auto stage = [&](int c, int n, bool fill) {
+    // stage candidate rows [c, c+n) of recs into slots 0..n-1, realigned to
+    // the anchor's grid: the code at row position p of a row with shift s
+    // moves to anchor-relative position s + p, which lies in word
+    // (s + p) / 16 - s / 16 of the row's bases (floor divisions; 32 and 4
+    // codes per word for 1- and 8-bit qualities). Reverse-complement rows are
+    // turned into the alignment's orientation on the way (bases reversed and
+    // complemented, qualities reversed over the whole quality pitch:
+    // reverseQualitiesOfRCAlignments, corrector.hpp:1227-1239), so the column
+    // sums read every row forward, and a lane finds its column's code at the
+    // same bits of every row. A warp per row: lane j loads word j of the
+    // row's packed bases and of its quality words (RR rows of a warp in
+    // flight), then builds output word j from a window of them.
+    auto stage = [&](int c, int n, bool fill, auto RR) {
+        constexpr int R = decltype(RR)::value;
         __syncthreads();
         if (fill) {
             for (int k = tid; k < n; k += BLOCK) {
@@ -1053,97 +1119,69 @@ msa_anchor(const DevOptions& o, const DevReads& r, uint32_t first, uint32_t ai, 
             }
             __syncthreads();
         }
-        // word idx = k * rw + w of the staged rows, eight words in flight per
-        // thread; k = floor(idx / rw) by a multiply-high (exact: idx * rw < 2^32)
-        const int nw = n * rw;
-        const unsigned long long mrw = ((1ull << 32) + (unsigned)rw - 1) / (unsigned)rw;
-        for (int b0 = 0; b0 < nw; b0 += 8 * BLOCK) {
-            uint32_t v[8];
+        for (int k0 = warp * R; k0 < n; k0 += NWARP * R) {
+            uint32_t ms[R], mq0[R], mq1[R];
 #pragma unroll
-            for (int u = 0; u < 8; ++u) {
-                const int idx = b0 + u * BLOCK + tid;
-                v[u] = 0u;
-                if (idx < nw) {
-                    const int k = (int)(((unsigned long long)idx * mrw) >> 32);
-                    const int w = idx - k * rw;
-                    const size_t id = s_id[k];
-                    v[u] = w < sp ? __ldg(r.seq + id * sp + w) : __ldg(r.qual + id * qp + (w - sp));
-                }
-            }
-#pragma unroll
-            for (int u = 0; u < 8; ++u) {
-                const int idx = b0 + u * BLOCK + tid;
-                if (idx < nw) s_raw[idx] = v[u];
-            }
-        }
-        __syncthreads();
-        // reverse-complement rows: a warp per row, each lane one output word
-        // built from a window of the source words (fetched by shuffle)
-        for (int k = warp; k < n; k += NWARP) {
-            if (s_fwd[k]) continue;                      // warp-uniform
-            uint32_t* row = s_raw + k * rw;
-            {   // bases: 16 per word, MSB first; output base p = complement of source base L-1-p
-                const int L = s_len[k];
-                const uint32_t mine = lane < sp ? row[lane] : 0u;
-                const int s0 = L - 16 - 16 * lane;       // first source base of this lane's word
-                const int wi = s0 >= 0 ? (s0 >> 4) : 0;
-                const uint32_t a = __shfl_sync(0xffffffffu, mine, wi & 31);
-                const uint32_t b = __shfl_sync(0xffffffffu, mine, (wi + 1) & 31);
-                uint32_t win;
-                if (s0 >= 0) win = (s0 & 15) ? __funnelshift_l(b, a, 2 * (s0 & 15)) : a;
-                else win = s0 > -16 ? a >> (-2 * s0) : 0u;
-                win = __brev(win);                           // reverse the 16 codes ...
-                win = ((win >> 1) & 0x55555555u) | ((win & 0x55555555u) << 1);   // ... keeping each code's bits
-                if (lane < sp) row[lane] = ~win;             // complement: A<->T, C<->G
-            }
-            if (useQ) {  // qualities reversed over the quality pitch (mlen characters)
-                uint32_t* qrow = row + sp;
-                if (qbits == 8) {        // 4 per word, little-endian bytes
-                    const uint32_t m0 = lane < qp ? qrow[lane] : 0u;
-                    const uint32_t m1 = lane + 32 < qp ? qrow[lane + 32] : 0u;
-                    __syncwarp();
-                    for (int h = 0; h < 2; ++h) {
-                        const int t = lane + 32 * h;
-                        const int s0 = mlen - 4 - 4 * t;
-                        const int wi = s0 >= 0 ? (s0 >> 2) : 0;
-                        const uint32_t a0 = __shfl_sync(0xffffffffu, m0, wi & 31);
-                        const uint32_t a1 = __shfl_sync(0xffffffffu, m1, wi & 31);
-                        const uint32_t b0 = __shfl_sync(0xffffffffu, m0, (wi + 1) & 31);
-                        const uint32_t b1 = __shfl_sync(0xffffffffu, m1, (wi + 1) & 31);
-                        const uint32_t a = wi < 32 ? a0 : a1, b = wi + 1 < 32 ? b0 : b1;
-                        uint32_t win;
-                        if (s0 >= 0) win = (s0 & 3) ? __funnelshift_r(a, b, 8 * (s0 & 3)) : a;
-                        else win = s0 > -4 ? a << (-8 * s0) : 0u;
-                        if (t < qp) qrow[t] = __byte_perm(win, 0u, 0x0123);
+            for (int t = 0; t < R; ++t) {
+                ms[t] = mq0[t] = mq1[t] = 0u;
+                if (k0 + t < n) {
+                    const size_t id = s_id[k0 + t];
+                    if (lane < sp) ms[t] = __ldg(r.seq + id * sp + lane);
+                    if constexpr (useQ) {
+                        const uint32_t* qrow = r.qual + id * qp;
+                        if (lane < qp) mq0[t] = __ldg(qrow + lane);
+                        if constexpr (QB == 8) if (lane + 32 < qp) mq1[t] = __ldg(qrow + lane + 32);
                     }
-                } else {
-                    const int per = qbits == 2 ? 16 : 32;    // codes per word, MSB first
-                    const uint32_t mine = lane < qp ? qrow[lane] : 0u;
-                    __syncwarp();
-                    const int s0 = mlen - per - per * lane;
-                    const int wi = s0 >= 0 ? s0 / per : 0;
-                    const uint32_t a = __shfl_sync(0xffffffffu, mine, wi & 31);
-                    const uint32_t b = __shfl_sync(0xffffffffu, mine, (wi + 1) & 31);
-                    const int sh = s0 >= 0 ? (s0 % per) * (32 / per) : 0;
-                    uint32_t win;
-                    if (s0 >= 0) win = sh ? __funnelshift_l(b, a, sh) : a;
-                    else win = s0 > -per ? a >> (-s0 * (32 / per)) : 0u;
-                    win = __brev(win);
-                    if (per == 16) win = ((win >> 1) & 0x55555555u) | ((win & 0x55555555u) << 1);
-                    if (lane < qp) qrow[lane] = win;
                 }
             }
-            __syncwarp();
+#pragma unroll
+            for (int t = 0; t < R; ++t) {
+                const int k = k0 + t;
+                if (k >= n) break;                           // warp-uniform
+                uint32_t* row = s_raw + k * rw;
+                const bool rev = !s_fwd[k];                  // warp-uniform
+                const int L = s_len[k], sft = s_beg[k];
+                const int o16 = sft & 15;
+                uint32_t ws = window2(ms[t], rev ? L - 16 - 16 * lane + o16 : 16 * lane - o16);
+                if (rev) ws = ~rev2(ws);                     // reversed, complemented: A<->T, C<->G
+                if constexpr (QB == 2) {
+                    uint32_t wq = window2(mq0[t], rev ? mlen - 16 - 16 * lane + o16 : 16 * lane - o16);
+                    if (rev) wq = rev2(wq);
+                    if (lane <= (sp > qp ? sp : qp)) reinterpret_cast<uint2*>(row)[lane] = make_uint2(ws, wq);
+                } else {
+                    if (lane <= sp) row[lane] = ws;
+                    if constexpr (QB == 1) {
+                        const int o32 = sft & 31;
+                        uint32_t wq = window1(mq0[t], rev ? mlen - 32 - 32 * lane + o32 : 32 * lane - o32);
+                        if (rev) wq = __brev(wq);
+                        if (lane <= qp) row[sp + 1 + lane] = wq;
+                    } else if constexpr (QB == 8) {
+                        const int o4 = sft & 3;
+#pragma unroll
+                        for (int h = 0; h < 3; ++h) {
+                            const int j = lane + 32 * h;
+                            uint32_t wq = window8(mq0[t], mq1[t], rev ? mlen - 4 - 4 * j + o4 : 4 * j - o4);
+                            if (rev) wq = __byte_perm(wq, 0u, 0x0123);
+                            if (j <= qp) row[sp + 1 + j] = wq;
+                        }
+                    }
+                }
+            }
         }
         __syncthreads();
     };
     // base (2-bit, in the candidate's aligned orientation) of staged row k at
     // position p < s_len[k]
-    auto cand_base = [&](int k, int p) -> uint32_t { return base_at(s_raw + k * rw, p); };
+    auto cand_base = [&](int k, int p) -> uint32_t {
+        const int sft = s_beg[k], q = sft + p;
+        const int wi = (q >> 4) - (sft >> 4);
+        const uint32_t w = s_raw[k * rw + (QB == 2 ? 2 * wi : wi)];
+        return (w >> (30 - 2 * (q & 15))) & 3u;
+    };
     const bool persistent = V <= nstage;      // all rows stay staged across rebuilds
     int nalive = V;
     if (persistent) {
-        stage(0, V, !direct);
+        stage(0, V, !direct, std::integral_constant<int, QB == 8 ? 2 : 4>{});
         for (int k = tid; k < V; k += BLOCK) s_alive[k] = (uint8_t)k;
     }
     __syncthreads();
@@ -1222,7 +1260,6 @@ msa_anchor(const DevOptions& o, const DevReads& r, uint32_t first, uint32_t ai, 
             uint32_t cAC = 0u, cGT = 0u;                     // 16-bit counts: A | C << 16, G | T << 16
             uint32_t c8 = 0u;           // the chunk's 8-bit counts A | C << 8 | G << 16 | T << 24
             float wA = 0.0f, wC = 0.0f, wG = 0.0f, wT = 0.0f;
-            auto add = [&](uint32_t b, float w, bool valid) { msa_add(wA, wC, wG, wT, c8, b, w, valid); };
             // a chunk adds at most 128 rows and the anchor: its 8-bit counts
             // cannot overflow before they are moved to the 16-bit ones
             auto flush = [&]() {
@@ -1234,54 +1271,96 @@ msa_anchor(const DevOptions& o, const DevReads& r, uint32_t first, uint32_t ai, 
                 const int p = col - abegin;
                 if (active && p >= 0 && p < La) {
                     const uint32_t e = s_aelem[p];
-                    add(e & 3u, useQ ? s_qw[e >> 2] : 1.0f, true);     // factor 1.0f
+                    msa_add8(wA, wC, wG, wT, c8, (e & 3u) << 3, useQ ? s_qw[e >> 2] : 1.0f, 0, 1);   // factor 1.0f
                 }
             }
             // staged rows (slot list[i], or slot i) meeting this block, in
             // list order: per chunk of 32 rows the warp lists the rows that
-            // meet the block (ballot, order kept) as {row word offset | slot
-            // << 16 | length << 23, first position - lane}; up to four listed
-            // rows load together, then add in order
+            // meet the block (ballot, order kept) as {grid origin of the row
+            // in bytes, first position - lane, length, weights}; up to four
+            // listed rows load together, then add in order. The last listed
+            // row is repeated three times past the list with length 0: a group
+            // of four reads it there, in bounds, and adds nothing.
             auto run_rows = [&](const uint8_t* list, int nrows) {
+                // this lane's column on the anchor's grid: the word of every
+                // staged row that holds it (byte offset, relative to the
+                // row's grid origin) and its bits there, as rotations that
+                // bring the base to bits 3-4 (base * 8) and the quality code
+                // to bits 2-3 (2-bit) or bit 2 (1-bit), i.e. the byte offset
+                // of its weight
+                const int q = col - abegin;
+                const int qsh = 30 - 2 * (q & 15);
+                const uint32_t rb8 = (uint32_t)(qsh + 29) & 31u;
+                const int loff = (q >> 4) * (QB == 2 ? 8 : 4);
+                uint32_t rq = 0u;
+                int qoff = 0;
+                if constexpr (QB == 2) rq = (uint32_t)(qsh + 30) & 31u;
+                if constexpr (QB == 1) { rq = (uint32_t)(31 - (q & 31) + 30) & 31u; qoff = (q >> 5) * 4; }
+                if constexpr (QB == 8) { rq = 8u * (uint32_t)(q & 3); qoff = (q >> 2) * 4; }
+                const unsigned char* rawb = reinterpret_cast<const unsigned char*>(s_raw);
+                const unsigned char* wqb = reinterpret_cast<const unsigned char*>(&s_wq[0][0]);
                 for (int i0 = 0; i0 < nrows; i0 += 32) {
                     bool hit = false;
-                    uint2 ent = make_uint2(0u, 0u);
+                    uint4 ent = make_uint4(0u, 0u, 0u, 0u);
+                    int hq = 0;
                     if (i0 + lane < nrows) {
                         const int k = list ? list[i0 + lane] : i0 + lane;
                         const int2 bl = s_bl[k];
                         const int cb = abegin + bl.x;
                         hit = cb < c0 + 32 && cb + bl.y > c0;
-                        ent = make_uint2((uint32_t)(k * rw) | ((uint32_t)k << 16) | ((uint32_t)bl.y << 23),
-                                         (uint32_t)(c0 - cb));
+                        ent.x = (uint32_t)(k * rw * 4 - (bl.x >> 4) * (QB == 2 ? 8 : 4));
+                        ent.y = (uint32_t)(c0 - cb);
+                        ent.z = (uint32_t)bl.y;
+                        ent.w = (QB == 1 || QB == 2) ? (uint32_t)k * 16u : __float_as_uint(s_w[k]);
+                        if constexpr (QB == 1) hq = (k * rw + sp + 1 - (bl.x >> 5)) * 4;
+                        if constexpr (QB == 8) hq = (k * rw + sp + 1 - (bl.x >> 2)) * 4;
                     }
                     const unsigned m = __ballot_sync(0xffffffffu, hit);
-                    if (hit) s_hits[warp][__popc(m & ((1u << lane) - 1u))] = ent;
-                    __syncwarp();
                     const int nh = __popc(m);
+                    if (hit) {
+                        const int pos = __popc(m & ((1u << lane) - 1u));
+                        s_hits[warp][pos] = ent;
+                        if constexpr (QB == 1 || QB == 8) s_hq[warp][pos] = hq;
+                        if (pos == nh - 1) {
+                            const uint4 pad = make_uint4(ent.x, ent.y, 0u, ent.w);
+#pragma unroll
+                            for (int u = 1; u <= 3; ++u) {
+                                s_hits[warp][pos + u] = pad;
+                                if constexpr (QB == 1 || QB == 8) s_hq[warp][pos + u] = hq;
+                            }
+                        }
+                    }
+                    __syncwarp();
                     for (int h0 = 0; h0 < nh; h0 += 4) {
-                        bool v[4];
                         uint32_t bb[4];
                         float ww[4];
-                        // branch free: entries past the list (zero, or an
-                        // earlier chunk's) load in bounds and add nothing
+                        int pp[4], ll[4];
 #pragma unroll
                         for (int u = 0; u < 4; ++u) {
-                            const uint2 e = s_hits[warp][h0 + u];
-                            const int p = lane + (int)e.y;
-                            const bool in = h0 + u < nh && (unsigned)p < (e.x >> 23);
-                            const int pc = in ? p : 0;          // loads stay inside the row
-                            const uint32_t* row = s_raw + (e.x & 0xFFFFu);
-                            const int k = (e.x >> 16) & 0x7F;
-                            const int wi = pc >> 4, sh = 30 - 2 * (pc & 15);
-                            bb[u] = (row[wi] >> sh) & 3u;
-                            if constexpr (QB == 0) ww[u] = s_w[k];
-                            else if constexpr (QB == 2) ww[u] = s_wq[k][(row[sp + wi] >> sh) & 3u];
-                            else if constexpr (QB == 1) ww[u] = s_wq[k][(row[sp + (pc >> 5)] >> (31 - (pc & 31))) & 1u];
-                            else ww[u] = fmul_rn(s_w[k], s_qw[(row[sp + (pc >> 2)] >> (8 * (pc & 3))) & 0xFFu]);
-                            v[u] = in;
+                            const uint4 e = s_hits[warp][h0 + u];
+                            const unsigned char* wp = rawb + ((int)e.x + loff);
+                            uint32_t sw, qv = 0u;
+                            if constexpr (QB == 2) {
+                                const uint2 t2 = *reinterpret_cast<const uint2*>(wp);
+                                sw = t2.x;
+                                qv = t2.y;
+                            } else {
+                                sw = *reinterpret_cast<const uint32_t*>(wp);
+                                if constexpr (QB == 1 || QB == 8)
+                                    qv = *reinterpret_cast<const uint32_t*>(rawb + (s_hq[warp][h0 + u] + qoff));
+                            }
+                            bb[u] = __funnelshift_r(sw, sw, rb8) & 24u;
+                            if constexpr (QB == 0) ww[u] = __uint_as_float(e.w);
+                            else if constexpr (QB == 2)
+                                ww[u] = *reinterpret_cast<const float*>(wqb + (e.w + (__funnelshift_r(qv, qv, rq) & 12u)));
+                            else if constexpr (QB == 1)
+                                ww[u] = *reinterpret_cast<const float*>(wqb + (e.w + (__funnelshift_r(qv, qv, rq) & 4u)));
+                            else ww[u] = fmul_rn(__uint_as_float(e.w), s_qw[(qv >> rq) & 0xFFu]);
+                            pp[u] = lane + (int)e.y;
+                            ll[u] = (int)e.z;
                         }
 #pragma unroll
-                        for (int u = 0; u < 4; ++u) add(bb[u], ww[u], v[u]);
+                        for (int u = 0; u < 4; ++u) msa_add8(wA, wC, wG, wT, c8, bb[u], ww[u], pp[u], ll[u]);
                     }
                     __syncwarp();
                 }
@@ -1293,7 +1372,7 @@ msa_anchor(const DevOptions& o, const DevReads& r, uint32_t first, uint32_t ai, 
                 int n = nalive;
                 if (!persistent) {
                     n = min(nstage, nalive - ch * nstage);
-                    stage(ch * nstage, n, true);
+                    stage(ch * nstage, n, true, std::integral_constant<int, 1>{});
                 }
                 if (active) run_rows(persistent ? s_alive : nullptr, n);
                 flush();

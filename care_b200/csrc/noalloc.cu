@@ -95,8 +95,10 @@ extern "C" int care_b200_correct_range_noalloc(const care_b200_options* opt, con
     if (num_anchors > kNoAllocMaxAnchors) return CARE_B200_ELIMIT;
     if (reads->max_length < 1 || reads->max_length > kMaxLen) return CARE_B200_ELIMIT;
     if ((size_t)(reads->max_length + 15) / 16 > reads->pitch_ints) return CARE_B200_EINVAL;
+    if (reads->pitch_ints > (size_t)kMaxLen / 16) return CARE_B200_EINVAL;
     if (opt->use_quality &&
-        (size_t)((int64_t)reads->max_length * opt->quality_bits + 31) / 32 > reads->qual_pitch_ints)
+        ((size_t)((int64_t)reads->max_length * opt->quality_bits + 31) / 32 > reads->qual_pitch_ints ||
+         reads->qual_pitch_ints > (size_t)kMaxLen * opt->quality_bits / 32))
         return CARE_B200_EINVAL;
     if (tables->threshold < 0 || tables->threshold > 65535) return CARE_B200_EINVAL;
 
@@ -212,7 +214,8 @@ extern "C" int care_b200_correct_range_noalloc(const care_b200_options* opt, con
         maxcols = c > maxcols ? c : maxcols;
     }
     const int jb = (maxcols + 127) / 128;
-    const size_t msmem = msa_smem_bytes(r.max_len, r.seq_pitch, r.qual_pitch, false, 128 * jb);
+    const int qb = !o.use_quality ? 0 : o.quality_bits == 1 ? 1 : o.quality_bits == 2 ? 2 : 8;
+    const size_t msmem = msa_smem_bytes(r.max_len, r.seq_pitch, r.qual_pitch, qb, false, 128 * jb);
 #define LAUNCH_MSA(QB)                                                                                   \
     do {                                                                                                  \
         if (cudaFuncSetAttribute(k_msa<128, QB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)msmem) \

@@ -94,7 +94,9 @@ const char* care_b200_last_error(const care_b200_ctx* ctx);
  * 152-187); enc_quals: num_reads rows of qual_pitch_ints uint32 in the
  * reference's qualityScoreBits encoding (qualityscorecompression.hpp:90-119),
  * or NULL; ambiguous_ids: reads that contained non-ACGT bases. Data is
- * copied into HBM once. Read length limit: 256 bases. Re-uploading the same
+ * copied into HBM once. Read length limit: 256 bases, so pitch_ints is at
+ * most 16 and qual_pitch_ints at most the words of 256 qualities (16, 8 or
+ * 64 for 2-, 1- and 8-bit codes; CARE_B200_EINVAL otherwise). Re-uploading the same
  * number of reads keeps the tables (they index reads by id); a different
  * number drops them. */
 int care_b200_upload_reads(care_b200_ctx* ctx, const uint32_t* packed, size_t pitch_ints,
