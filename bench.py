@@ -67,8 +67,9 @@ MLP_FILE_LARGE = os.path.join(ROOT, "care_b200", "data", "mlp_pe50x_h48.bin")
 METRIC = "reads corrected/s on 1 B200: plain vs MLP-classifier form at matched base F1"
 MLP_FILE = os.path.join(ROOT, "care_b200", "data", "mlp_pe30x.bin")
 # k_msa DRAM bytes per anchor: dram__bytes_read.sum + dram__bytes_write.sum of
-# one ncu capture of 100,000 anchors of this workload model (127.20 MB)
-MSA_DRAM_BYTES_PER_ANCHOR = 1272.0
+# one ncu capture of 100,000 anchors of this workload model (68.24 MB read +
+# 4.75 MB written)
+MSA_DRAM_BYTES_PER_ANCHOR = 730.0
 CARE_CPU = os.path.join(ROOT, "oracle", "_ref", "care-cpu")
 L2_BYTES = 126 * 1024 * 1024
 

