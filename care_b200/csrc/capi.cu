@@ -10,6 +10,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <condition_variable>
 #include <cstring>
 #include <functional>
 #include <memory>
@@ -60,6 +61,72 @@ struct HBuf {
         return e;
     }
     template <class T> T* as() const { return static_cast<T*>(p); }
+};
+
+// Host threads that copy one buffer in equal parts, kept for the context's
+// life: a copy of pageable caller memory into pinned staging runs at one
+// core's copy rate per thread, and starting threads per 16 MB chunk costs
+// as much as the copy.
+class CopyPool {
+public:
+    explicit CopyPool(unsigned n) : n_(std::max(1u, n)) {
+        for (unsigned i = 1; i < n_; ++i) th_.emplace_back([this, i] { run(i); });
+    }
+    ~CopyPool() {
+        {
+            std::lock_guard<std::mutex> g(m_);
+            quit_ = true;
+        }
+        go_.notify_all();
+        for (auto& t : th_) t.join();
+    }
+    CopyPool(const CopyPool&) = delete;
+    CopyPool& operator=(const CopyPool&) = delete;
+    // copies len bytes from src to dst; the calling thread takes part 0
+    void copy(void* dst, const void* src, size_t len) {
+        {
+            std::lock_guard<std::mutex> g(m_);
+            dst_ = static_cast<char*>(dst);
+            src_ = static_cast<const char*>(src);
+            len_ = len;
+            part_ = (len + n_ - 1) / n_;
+            pending_ = n_ - 1;
+            ++gen_;
+        }
+        go_.notify_all();
+        part(0);
+        std::unique_lock<std::mutex> lk(m_);
+        done_.wait(lk, [this] { return pending_ == 0; });
+    }
+
+private:
+    void part(unsigned i) {
+        const size_t a = (size_t)i * part_;
+        if (a < len_) std::memcpy(dst_ + a, src_ + a, std::min(part_, len_ - a));
+    }
+    void run(unsigned i) {
+        unsigned long long seen = 0;
+        std::unique_lock<std::mutex> lk(m_);
+        for (;;) {
+            go_.wait(lk, [&] { return quit_ || gen_ != seen; });
+            if (quit_) return;
+            seen = gen_;
+            lk.unlock();
+            part(i);
+            lk.lock();
+            if (--pending_ == 0) done_.notify_one();
+        }
+    }
+    unsigned n_;
+    std::vector<std::thread> th_;
+    std::mutex m_;
+    std::condition_variable go_, done_;
+    char* dst_ = nullptr;
+    const char* src_ = nullptr;
+    size_t len_ = 0, part_ = 0;
+    unsigned pending_ = 0;
+    unsigned long long gen_ = 0;
+    bool quit_ = false;
 };
 
 constexpr int kCandBlock = 128;
@@ -118,6 +185,7 @@ struct care_b200_ctx {
     HBuf h_text;                      // input files' bytes (records parsed on the device point into it)
     // host -> device staging of uploads: two pinned chunks per copy stream
     HBuf h_stage[2][2];
+    std::unique_ptr<CopyPool> copy_pool;          // host threads filling the staging chunks
     cudaEvent_t stage_ev[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
     cudaStream_t copy_stream = nullptr;
     cudaStream_t copy_stream2 = nullptr;          // quality words while the sequences upload
@@ -273,22 +341,14 @@ int staged_upload(care_b200_ctx* ctx, int slot, void* dst, const void* src, size
         return CARE_B200_OK;
     }
     for (auto& b : ctx->h_stage[slot]) CK(b.ensure(kChunk), "alloc staging");
-    const unsigned hw = std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
+    if (!ctx->copy_pool) ctx->copy_pool.reset(new CopyPool(std::min(16u, std::thread::hardware_concurrency())));
     size_t off = 0;
     for (int i = 0; off < bytes; ++i, off += kChunk) {
         const int b = i & 1;
         const size_t len = std::min(kChunk, bytes - off);
         CK(cudaEventSynchronize(ctx->stage_ev[slot][b]), "staging");   // the chunk's previous copy is done
         char* pin = ctx->h_stage[slot][b].as<char>();
-        const char* from = static_cast<const char*>(src) + off;
-        std::vector<std::thread> th;
-        const size_t part = (len + hw - 1) / hw;
-        for (unsigned t = 0; t < hw; ++t) {
-            const size_t a = t * part;
-            if (a >= len) break;
-            th.emplace_back([=] { std::memcpy(pin + a, from + a, std::min(part, len - a)); });
-        }
-        for (auto& x : th) x.join();
+        ctx->copy_pool->copy(pin, static_cast<const char*>(src) + off, len);
         CK(cudaMemcpyAsync(static_cast<char*>(dst) + off, pin, len, cudaMemcpyHostToDevice, st), "upload");
         CK(cudaEventRecord(ctx->stage_ev[slot][b], st), "staging");
         if (on_chunk) if (int rc = on_chunk(off + len, ctx->stage_ev[slot][b])) return rc;
