@@ -1927,6 +1927,7 @@ static __global__ void k_signatures(DevOptions o, DevReads r, uint32_t first, ui
     const int h = o.num_maps;
     const uint32_t* row = r.seq + (size_t)id * r.seq_pitch;
     unsigned long long mine[2] = {~0ull, ~0ull};  // maps lane and lane+32
+    unsigned long long alt[2] = {~0ull, ~0ull};
     if (L >= o.k) {
         const int npos = L - o.k + 1;
         const int rcshift = 64 - 2 * o.k;
@@ -1945,14 +1946,27 @@ static __global__ void k_signatures(DevOptions o, DevReads r, uint32_t first, ui
                 const unsigned long long rv = revcomp64(fw) >> rcshift;
                 cn = fw < rv ? fw : rv;
             }
+            // two k-mers per step into separate minima (the min chains of a
+            // lane overlap; an odd count hashes the last k-mer twice)
             const int nv = min(32, npos - p0);
-            for (int q = 0; q < nv; ++q) {
-                const unsigned long long km = __shfl_sync(0xffffffffu, cn, q);
-                if (lane < h) { const unsigned long long v = murmur64(km + lane); mine[0] = v < mine[0] ? v : mine[0]; }
-                if (lane + 32 < h) { const unsigned long long v = murmur64(km + lane + 32); mine[1] = v < mine[1] ? v : mine[1]; }
+            for (int q = 0; q < nv; q += 2) {
+                const unsigned long long k0 = __shfl_sync(0xffffffffu, cn, q);
+                const unsigned long long k1 = __shfl_sync(0xffffffffu, cn, q + 1 < nv ? q + 1 : q);
+                if (lane < h) {
+                    const unsigned long long v0 = murmur64(k0 + lane), v1 = murmur64(k1 + lane);
+                    mine[0] = v0 < mine[0] ? v0 : mine[0];
+                    alt[0] = v1 < alt[0] ? v1 : alt[0];
+                }
+                if (lane + 32 < h) {
+                    const unsigned long long v0 = murmur64(k0 + lane + 32), v1 = murmur64(k1 + lane + 32);
+                    mine[1] = v0 < mine[1] ? v0 : mine[1];
+                    alt[1] = v1 < alt[1] ? v1 : alt[1];
+                }
             }
         }
     }
+    mine[0] = alt[0] < mine[0] ? alt[0] : mine[0];
+    mine[1] = alt[1] < mine[1] ? alt[1] : mine[1];
     if (lane < h) sig[(size_t)ri * h + lane] = mine[0] & o.kmer_mask;
     if (lane + 32 < h) sig[(size_t)ri * h + lane + 32] = mine[1] & o.kmer_mask;
 }
