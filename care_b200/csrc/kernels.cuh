@@ -900,6 +900,7 @@ msa_anchor(const DevOptions& o, const DevReads& r, uint32_t first, uint32_t ai, 
     __shared__ uint8_t s_alive[kStageMax];
     __shared__ int s_red[NWARP][4];
     __shared__ int s_vals[12];
+    __shared__ uint16_t s_dec[EMIT ? kMaxLen : 1];   // decision positions of the anchor (EMIT)
     __shared__ __align__(16) float s_asup[kMaxLen];   // support of the anchor's columns, position order
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -1556,6 +1557,7 @@ msa_anchor(const DevOptions& o, const DevReads& r, uint32_t first, uint32_t ai, 
                 isHQ = fgeq((float)minCov, covThr) && fleq((float)smallest, fmul_rn((float)pct, 0.5f));
             }
             if (lane == 0) {
+                s_vals[10] = 0;                  // decision positions listed (EMIT)
                 s_vals[4] = good;
                 s_vals[5] = isHQ;
                 s_vals[6] = __float_as_int(avgSup);
@@ -1602,10 +1604,17 @@ msa_anchor(const DevOptions& o, const DevReads& r, uint32_t first, uint32_t ai, 
     // deciding, k_clf_apply overwrites it from the row's logit.
     if constexpr (EMIT) {
         if (!hq) {
+            // the decision positions are listed first (any order: rows are
+            // appended through a global counter), so that their features are
+            // computed by consecutive threads instead of by the warps that
+            // happen to hold one
             int nm = 0, mxc = 0;
             for (int p = tid; p < La; p += BLOCK) {
-                nm += (s_aelem[p] & 3u) != s_cons[abegin + p];
-                mxc = max(mxc, (int)s_cov[abegin + p]);
+                const int col = abegin + p;
+                const bool mis = (s_aelem[p] & 3u) != s_cons[col];
+                nm += mis;
+                mxc = max(mxc, (int)s_cov[col]);
+                if (mis && (int)s_cov[col] >= o.clf_min_coverage) s_dec[atomicAdd(&s_vals[10], 1)] = (uint16_t)p;
             }
 #pragma unroll
             for (int d = 16; d > 0; d >>= 1) {
@@ -1621,10 +1630,11 @@ msa_anchor(const DevOptions& o, const DevReads& r, uint32_t first, uint32_t ai, 
             const float avgSup = __int_as_float(s_vals[6]), minSup = __int_as_float(s_vals[7]);
             const int minCov = s_vals[8];
             const float E = o.estimated_coverage;
-            for (int p = tid; p < La; p += BLOCK) {
+            const int ndec = s_vals[10];
+            for (int i = tid; i < ndec; i += BLOCK) {
+                const int p = s_dec[i];
                 const int col = abegin + p;
                 const uint32_t ob = s_aelem[p] & 3u, cb = s_cons[col];
-                if (ob == cb || (int)s_cov[col] < o.clf_min_coverage) continue;
                 const float cov = (float)s_cov[col];
                 const int oc = cnt_of(col, ob), cc = cnt_of(col, cb);
                 const float wsum = s_fw[p], wc = s_fw[mlen + p], wo = s_fw[2 * mlen + p];
